@@ -1,0 +1,413 @@
+"""Benchmark: all-pairs self-gravity, mixed vs plain f64, on one B200.
+
+Workload (the configuration the headline metric is quoted on): 262,144
+equal-mass sources (total mass 1, G = 1) in the unit cube on a Zel'dovich-
+displaced 64^3 lattice (P(k) ~ k^-2, 1 % rms density contrast, cold start),
+plus 524,288 massless tracers from the same field; Plummer eps = 1e-3; 4th-
+order Yoshida, dt = 1e-3. A step is one Yoshida step over the whole state:
+3 force evaluations of 262,144 sources x 786,432 targets (6.18e11 pair
+interactions). Synthetic, seeded data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line on rank 0. `value` is whole-job G interactions/s of the
+chosen (mixed) path with the state resident in HBM; `e2e` the same metric
+through the public NBodySelfGrav API (state loaded from host arrays, host
+snapshots returned); f64 numbers, force error and energy drift beside it.
+Multi-GPU: the bodies do not partition without an all-gather of positions
+each force evaluation, so N > 1 runs N independent replicas ("replicas
+only"), each rank timing its own replica; value sums them.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SIDE = 64
+N_TRACER = 524_288
+EPS = 1e-3
+DT = 1e-3
+FLOP_PER_PAIR = 20          # the reference's own convention (TODO.md:73-74)
+METRIC = "G interactions/s (all-pairs self-gravity, mixed FP32-pair/FP64-accumulate, Yoshida-4)"
+UNIT = "G interactions/s"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def pairs_per_step(n_src, n_tgt, nsub=3):
+    return nsub * n_src * n_tgt
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            import tempfile
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------ CPU legs
+def cpu_sample(workload, seconds_target=12.0, threads=None):
+    """Time the oracle's f64 all-pairs force (the CPU restatement of the
+    reference's `beschleunigung`) on a bounded sample of targets against all
+    sources. Returns (pairs/s, cores, sample description)."""
+    from oracle import selfgrav as osg
+    threads = threads or os.cpu_count() or 1
+    src = workload["src4"]
+    tgt_all = workload["tgt4"]
+    n_src = len(src)
+    # probe a small sample, then scale to ~seconds_target of CPU work
+    probe = tgt_all[:: max(1, len(tgt_all) // 64)][:64]
+    t0 = time.perf_counter()
+    osg.accel(src, probe, EPS * EPS, dim=3, threads=threads)
+    dt_probe = time.perf_counter() - t0
+    rate = len(probe) * n_src / max(dt_probe, 1e-9)
+    n_t = int(min(len(tgt_all), max(64, rate * seconds_target / n_src)))
+    sample = tgt_all[:: max(1, len(tgt_all) // n_t)][:n_t]
+    t0 = time.perf_counter()
+    osg.accel(src, sample, EPS * EPS, dim=3, threads=threads)
+    dt = time.perf_counter() - t0
+    pairs = len(sample) * n_src
+    desc = (f"f64 oracle all-pairs force, {len(sample)} strided targets x {n_src} sources "
+            f"({pairs:.3e} pairs, {dt:.1f} s)")
+    return pairs / dt, threads, desc
+
+
+def build_workload():
+    from solarsystemsimulator_b200 import workloads
+    w = workloads.structure_formation(n_side=N_SIDE, n_tracer=N_TRACER)
+    n = len(w["pos"])
+    src4 = np.zeros((n, 4))
+    src4[:, :3] = w["pos"]
+    src4[:, 3] = 1.0 * w["mass"]          # G = 1
+    tgt4 = np.zeros((n + N_TRACER, 4))
+    tgt4[:n] = src4
+    tgt4[n:, :3] = w["tracer_pos"]
+    w["src4"], w["tgt4"] = src4, tgt4
+    return w
+
+
+def config_block(n_src, n_tgt):
+    return {"workload": "self-gravitating structure formation, 64^3 Zel'dovich lattice + "
+                        "524288 tracers, unit cube, eps=1e-3, Yoshida-4 dt=1e-3",
+            "n_sources": n_src, "n_targets": n_tgt, "dim": 3, "G": 1.0,
+            "pairs_per_step": pairs_per_step(n_src, n_tgt),
+            "l2": "L2 flushed (256 MiB write) before every timed step",
+            "parallelism": "1 GPU per replica (replicas only)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    w = build_workload()
+    n_src, n_tgt = len(w["src4"]), len(w["tgt4"])
+    rates = []
+    cores = os.cpu_count() or 1
+    desc = ""
+    for _ in range(max(1, args.warmup_cpu)):
+        pass
+    for _ in range(max(1, min(args.steps, 2))):
+        r, cores, desc = cpu_sample(w, seconds_target=args.cpu_seconds, threads=cores)
+        rates.append(r)
+    rate = statistics.median(rates)
+    value = rate / 1e9
+    sec_per_step = pairs_per_step(n_src, n_tgt) / rate
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": len(rates),
+            "warmup": 0, "ms_per_step": sec_per_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": config_block(n_src, n_tgt),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's CPU path of this force (its f64 NumPy formula) restated in C "
+                    "with OpenMP over targets (oracle/allpairs.c); steps/s extrapolated from the "
+                    "sampled pair rate"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from solarsystemsimulator_b200 import _lib
+    from solarsystemsimulator_b200 import selfgrav_kernel as sg
+
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    w = build_workload()
+    pos, mass, tpos = w["pos"], w["mass"], w["tracer_pos"]
+    n_src, n_tr = len(pos), len(tpos)
+    n_tgt = n_src + n_tr
+    zeros_s, zeros_t = np.zeros(n_src), np.zeros(n_tr)
+
+    def make(precision):
+        sim = sg.NBodySelfGrav(dev, softening_au=EPS, G=1.0, integrator="yoshida4",
+                               precision=precision)
+        st = sim.load_state(pos[:, 0], pos[:, 1], zeros_s, zeros_s, mass, z=pos[:, 2], vz=zeros_s,
+                            tracer=(tpos[:, 0], tpos[:, 1], zeros_t, zeros_t),
+                            tracer_z=(tpos[:, 2], zeros_t))
+        return sim, st
+
+    ctx = _lib.context(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed_steps(sim, st, k):
+        """k Yoshida steps, L2 flushed before each; returns device seconds."""
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        total = 0.0
+        for _ in range(k):
+            flush.fill_(1.0)
+            ev0.record(stream)
+            sim.step_batch_device(st, DT, 1, snapshots=True)
+            ev1.record(stream)
+            ev1.synchronize()
+            total += ev0.elapsed_time(ev1) * 1e-3
+        ctx.status(stream.cuda_stream)
+        return total
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- peaks measured in this run (the roofline denominators)
+    peak = {}
+    for kind, name in ((0, "fp64"), (1, "fp32"), (2, "fp32x2")):
+        v = ctypes_double()
+        ctx.check(ctx.lib.sss_probe_fma(ctx.ptr, kind, 4096, __import__("ctypes").byref(v)))
+        peak[name] = v.value
+
+    # ---- mixed: warm-up, then the timed region
+    sim_m, st_m = make("mixed")
+    for _ in range(max(args.warmup, 0)):
+        sim_m.step_batch_device(st_m, DT, 1, snapshots=True)
+    e_m0 = sim_m.energy(st_m)
+    barrier()
+    clocks = ClockSampler(gpu_smi_id(dev))
+    clocks.start()
+    t_mixed = timed_steps(sim_m, st_m, args.steps)
+    barrier()
+    clk = clocks.stop()
+    t_mixed = max_over_ranks(t_mixed)
+    e_m1 = sim_m.energy(st_m)
+
+    # ---- dominant kernel alone: the mixed force kernel, CUDA events
+    src_t = st_m["pos"][st_m["c"].cur][:n_src].contiguous()
+    tgt_t = st_m["pos"][st_m["c"].cur].contiguous()
+    acc_t = torch.empty_like(tgt_t)
+    sg.allpairs_accel(src_t, tgt_t, EPS * EPS, dim=3, precision="mixed", out=acc_t)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_k = 3
+    ev0.record(stream)
+    for _ in range(n_k):
+        sg.allpairs_accel(src_t, tgt_t, EPS * EPS, dim=3, precision="mixed", out=acc_t)
+    ev1.record(stream)
+    ev1.synchronize()
+    t_kernel_mixed = ev0.elapsed_time(ev1) * 1e-3 / n_k
+
+    # ---- force error of mixed vs f64 on the full state (f64 kernel is
+    #      pinned to the CPU oracle at 1e-12 by the tests) + CPU check
+    a64 = torch.empty_like(tgt_t)
+    ev0.record(stream)
+    sg.allpairs_accel(src_t, tgt_t, EPS * EPS, dim=3, precision="f64", out=a64)
+    ev1.record(stream)
+    ev1.synchronize()
+    t_kernel_f64 = ev0.elapsed_time(ev1) * 1e-3
+    am = acc_t[:, :3].double()
+    af = a64[:, :3]
+    rel = (torch.linalg.norm(am - af, dim=1) / torch.linalg.norm(af, dim=1)).cpu().numpy()
+    ferr = {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
+            "max": float(rel.max())}
+    from oracle import selfgrav as osg
+    samp = np.arange(0, n_tgt, n_tgt // 256)[:256]
+    tgt_h = tgt_t.cpu().numpy()
+    a_or = osg.accel(src_t.cpu().numpy(), tgt_h[samp], EPS * EPS, dim=3)[:, :3]
+    rel_or = np.linalg.norm(am.cpu().numpy()[samp] - a_or, axis=1) / np.linalg.norm(a_or, axis=1)
+    rel_f64_or = np.linalg.norm(af.cpu().numpy()[samp] - a_or, axis=1) / np.linalg.norm(a_or, axis=1)
+
+    # ---- plain f64 path, same workload
+    sim_f, st_f = make("f64")
+    sim_f.step_batch_device(st_f, DT, 1, snapshots=True)   # warm-up
+    e_f0 = sim_f.energy(st_f)
+    barrier()
+    k_f64 = max(1, args.steps // 2)
+    t_f64 = max_over_ranks(timed_steps(sim_f, st_f, k_f64))
+    e_f1 = sim_f.energy(st_f)
+    del sim_f, st_f
+
+    # ---- e2e through the public API: load_state from host arrays, K steps,
+    #      host snapshots back (every step's snapshot is D2H-copied)
+    del st_m
+    torch.cuda.empty_cache()
+    barrier()
+    ev0.record(stream)
+    sim_e, st_e = make("mixed")
+    out = sim_e.step_batch(st_e, DT, args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    t_e2e = max_over_ranks(ev0.elapsed_time(ev1) * 1e-3)
+    h2d = (n_tgt * 2 * 4 * 8) // max(args.steps, 1)
+    d2h = out.shape[1] * 4
+    del sim_e, st_e
+
+    pps = pairs_per_step(n_src, n_tgt)
+    value = world * pps * args.steps / t_mixed / 1e9
+    flops_kernel = n_src * n_tgt * FLOP_PER_PAIR
+    achieved = flops_kernel / t_kernel_mixed / 1e12
+    launches_per_step = 1 + 3 * 2        # open kernel + 3 x (tile prep + force)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r, cores, desc = cpu_sample(w, seconds_target=args.cpu_seconds)
+        cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_mixed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-pair/f64-accumulate",
+            "data": "synthetic (seeded Zel'dovich lattice)",
+            "config": config_block(n_src, n_tgt),
+            "steps_per_s": args.steps / t_mixed,
+            "f64": {"value": world * pps * k_f64 / t_f64 / 1e9, "unit": UNIT,
+                    "steps_per_s": k_f64 / t_f64, "steps": k_f64,
+                    "kernel_ms": t_kernel_f64 * 1e3,
+                    "fp64_frac": (n_src * n_tgt * FLOP_PER_PAIR / t_kernel_f64 / 1e12) / peak["fp64"],
+                    "energy_drift": abs((e_f1 - e_f0) / e_f0)},
+            "mixed_over_f64_steps": (args.steps / t_mixed) / (k_f64 / t_f64),
+            "force_error_vs_f64": ferr,
+            "force_error_vs_cpu_oracle_sample": {"median": float(np.median(rel_or)),
+                                                 "max": float(rel_or.max()),
+                                                 "f64_kernel_max": float(rel_f64_or.max()),
+                                                 "targets": len(samp)},
+            "energy_drift": abs((e_m1 - e_m0) / e_m0),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak["fp32"],
+                         "unit": "TFLOP/s", "frac": achieved / peak["fp32"], "traffic": None,
+                         "kernel": "k_force_mixed", "kernel_ms": t_kernel_mixed * 1e3,
+                         "flop_per_pair": FLOP_PER_PAIR,
+                         "peak_source": "FFMA-chain probe measured in this run (no FP32 "
+                                        "SIMT peak in MEASURED_PEAKS.json)"},
+            "peaks_measured_tflops": peak,
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * pps * args.steps / t_e2e / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def gpu_smi_id(dev: int) -> str:
+    """nvidia-smi --id for torch device `dev` (UUID when torch exposes it)."""
+    import torch
+    props = torch.cuda.get_device_properties(dev)
+    u = getattr(props, "uuid", None)
+    if u is not None:
+        s = str(u)
+        return s if s.startswith("GPU-") else "GPU-" + s
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        return vis.split(",")[dev]
+    return str(dev)
+
+
+def ctypes_double():
+    import ctypes
+    return ctypes.c_double()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--warmup-cpu", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

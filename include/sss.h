@@ -1,0 +1,145 @@
+/*
+ * sss.h — C ABI of libsss.so, the B200 (sm_100a) N-body physics library.
+ *
+ * Every entry point takes plain pointers and sizes. Unless stated otherwise a
+ * pointer argument is a DEVICE pointer owned by the caller (for example the
+ * data_ptr() of a torch tensor); the library owns only the scratch memory that
+ * lives inside an sss_ctx. Calls are asynchronous on the caller's stream
+ * (`stream` is a cudaStream_t passed as void*, NULL = legacy default stream)
+ * unless their comment says they synchronise.
+ *
+ * Errors: every int-returning call returns SSS_OK (0) or one of the SSS_ERR_*
+ * codes; sss_last_error() gives the message of the last failing call on that
+ * context. Kernels whose waits are bounded record SSS_ERR_TIMEOUT in a device
+ * status word that sss_device_status() reads back.
+ *
+ * Threading: one sss_ctx per session; a context is not thread-safe.
+ *
+ * Reference interfaces each group replaces are cited as file:line within the
+ * reference project (Peuqui/SolarSystemSimulator, directory backend/).
+ */
+#ifndef SSS_H
+#define SSS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SSS_ABI_VERSION 1
+
+/* status codes */
+#define SSS_OK                    0
+#define SSS_ERR_ARG               1  /* bad argument (shape, range, NULL)        */
+#define SSS_ERR_TOO_MANY_MASSIVE  2  /* more than SSS_M_MAX massive bodies       */
+#define SSS_ERR_GUARD             3  /* a step-count guard ran out               */
+#define SSS_ERR_TIMEOUT           4  /* a bounded device wait gave up            */
+#define SSS_ERR_CUDA              5  /* a CUDA runtime / cuFFT call failed       */
+#define SSS_ERR_CAPACITY          6  /* an output buffer was too small           */
+
+/* precision of the pair interaction in the all-pairs kernels */
+#define SSS_PREC_F64    0   /* every operation in f64 (the drop-in path)          */
+#define SSS_PREC_MIXED  1   /* f32 pair arithmetic on f64-differenced positions,
+                               f32 partial sums folded into f64 accumulators      */
+
+/* integrators of sss_selfgrav_step_batch */
+#define SSS_INT_KDK       0 /* kick-drift-kick leapfrog (selfgrav_kernel.py:333-386) */
+#define SSS_INT_YOSHIDA4  1 /* 4th-order Yoshida: KDK substeps w1, w0, w1           */
+
+typedef struct sss_ctx sss_ctx;
+
+/* ---------------------------------------------------------------- context */
+
+/* ABI version of the loaded library (== SSS_ABI_VERSION of its header). */
+int sss_abi_version(void);
+
+/* Create a context bound to CUDA device `device`. */
+int sss_create(int device, sss_ctx** out);
+
+/* Free the context and its scratch. NULL is accepted. */
+void sss_destroy(sss_ctx* ctx);
+
+/* Message of the last failing call on ctx (never NULL). */
+const char* sss_last_error(const sss_ctx* ctx);
+
+/* Synchronise `stream`, then read and clear the device status word that
+ * bounded waits write. Returns SSS_OK or the recorded SSS_ERR_* code. */
+int sss_device_status(sss_ctx* ctx, void* stream);
+
+/* Number of streaming multiprocessors of the context's device. */
+int sss_num_sms(const sss_ctx* ctx);
+
+/* ------------------------------------------------- all-pairs self-gravity
+ *
+ * Replaces `beschleunigung` (selfgrav_kernel.py:222-260):
+ *   a_t = sum_s Gm_s (r_s - r_t) / (|r_s - r_t|^2 + eps2)^(3/2)
+ * Body records are double4 {x, y, z, Gm} (z ignored when dim == 2; Gm is the
+ * source's G*mass and is ignored for targets). Output acc4 is double4
+ * {ax, ay, az, 0}. The self term contributes exactly 0 (zero offset).
+ * Sources are summed in ascending index order inside each source chunk; the
+ * chunk partials are added in ascending chunk order, so a result depends only
+ * on the inputs and on (n_src, n_tgt, number of SMs), never on scheduling.
+ * All pointers are device pointers with 16-byte alignment.
+ */
+int sss_allpairs_accel(sss_ctx* ctx, int dim, int precision,
+                       const double* src4, int64_t n_src,
+                       const double* tgt4, int64_t n_tgt,
+                       double* acc4, double eps2, void* stream);
+
+/* Plummer potential at the targets, phi_t = -sum_s Gm_s / sqrt(|d|^2+eps2),
+ * in f64; the self term (zero offset) IS included (-Gm_t/eps), as in the
+ * reference energy (test_selfgrav.py:54-63) before its diagonal correction.
+ * Output phi is double [n_tgt]. */
+int sss_allpairs_potential(sss_ctx* ctx, int dim,
+                           const double* src4, int64_t n_src,
+                           const double* tgt4, int64_t n_tgt,
+                           double* phi, double eps2, void* stream);
+
+/* Resident self-gravity state (caller-owned device buffers). Bodies
+ * [0, n_src) are the massive sources, [n_src, n_src + n_tracer) massless
+ * tracers (Kernel B, selfgrav_kernel.py:262-420). pos4[cur] holds the current
+ * positions; the other buffer is the ping-pong target of each drift, and
+ * `cur` is updated by every call that moves the bodies. acc4 holds the
+ * accelerations at pos4[cur] once sss_selfgrav_init_accel has run. */
+typedef struct sss_selfgrav_state {
+    int      dim;         /* 2 or 3                                        */
+    int      precision;   /* SSS_PREC_F64 or SSS_PREC_MIXED                */
+    int64_t  n_src;       /* massive bodies (sources and targets)          */
+    int64_t  n_tracer;    /* massless tracers (targets only)               */
+    double*  pos4[2];     /* [n_src + n_tracer] {x, y, z, Gm}              */
+    double*  vel4;        /* [n_src + n_tracer] {vx, vy, vz, 0}            */
+    double*  acc4;        /* [n_src + n_tracer] {ax, ay, az, 0}            */
+    int      cur;         /* 0 or 1: which pos4 buffer is current          */
+    double   eps2;        /* Plummer softening squared, > 0                */
+} sss_selfgrav_state;
+
+/* Accelerations of all bodies at pos4[cur] into acc4. */
+int sss_selfgrav_init_accel(sss_ctx* ctx, sss_selfgrav_state* st, void* stream);
+
+/* `steps` integrator steps over the whole state (one launch sequence on
+ * `stream`). Replaces the step loop of selfgrav_kernel (selfgrav_kernel.py:
+ * 333-419) and NBodySelfGrav.step_batch (:558-627). Each force evaluation is
+ * one kernel whose epilogue applies the closing half kick, writes the
+ * snapshot and applies the next opening half kick and drift. If `snap` is
+ * not NULL it is a device float buffer of steps rows; row s is
+ * [x|y|(z)|vx|vy|(vz)] over the n_src sources followed by [x|y|(z)] over the
+ * tracers, i.e. 2*dim*n_src + dim*n_tracer floats per row (the layout of
+ * selfgrav_kernel.py:600-627 for dim == 2). Requires acc4 to be valid. */
+int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st,
+                            int integrator, double dt, int steps,
+                            float* snap, void* stream);
+
+/* ------------------------------------------------------------ diagnostics */
+
+/* Measured FMA throughput of the device in TFLOP/s (2 flops per FMA lane):
+ * kind 0 = f64 DFMA, 1 = f32 FFMA, 2 = packed f32x2 FMA. Synchronous; the
+ * roofline denominator of the all-pairs kernels. No reference counterpart. */
+int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSS_H */

@@ -1,0 +1,155 @@
+"""ctypes binding of libsss.so (the C ABI declared in include/sss.h).
+
+The library is the only compute path: if it is missing or no CUDA device is
+present, every entry point raises — there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsss.so")
+
+SSS_OK = 0
+SSS_ERR_ARG = 1
+SSS_ERR_TOO_MANY_MASSIVE = 2
+SSS_ERR_GUARD = 3
+SSS_ERR_TIMEOUT = 4
+SSS_ERR_CUDA = 5
+SSS_ERR_CAPACITY = 6
+
+PREC_F64 = 0
+PREC_MIXED = 1
+INT_KDK = 0
+INT_YOSHIDA4 = 1
+
+_c_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+_dp = ctypes.c_void_p   # device pointers travel as integers
+
+
+class SelfGravState(ctypes.Structure):
+    """Mirror of sss_selfgrav_state."""
+    _fields_ = [
+        ("dim", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("n_src", _c_i64),
+        ("n_tracer", _c_i64),
+        ("pos4", _dp * 2),
+        ("vel4", _dp),
+        ("acc4", _dp),
+        ("cur", ctypes.c_int),
+        ("eps2", ctypes.c_double),
+    ]
+
+
+# name -> (restype, argtypes); every symbol include/sss.h declares
+SIGNATURES = {
+    "sss_abi_version": (ctypes.c_int, []),
+    "sss_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    "sss_destroy": (None, [_vp]),
+    "sss_last_error": (ctypes.c_char_p, [_vp]),
+    "sss_device_status": (ctypes.c_int, [_vp, _vp]),
+    "sss_num_sms": (ctypes.c_int, [_vp]),
+    "sss_allpairs_accel": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, _c_i64, _dp, _c_i64,
+                                          _dp, ctypes.c_double, _vp]),
+    "sss_allpairs_potential": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _c_i64, _dp, _c_i64, _dp,
+                                              ctypes.c_double, _vp]),
+    "sss_selfgrav_init_accel": (ctypes.c_int, [_vp, ctypes.POINTER(SelfGravState), _vp]),
+    "sss_selfgrav_step_batch": (ctypes.c_int, [_vp, ctypes.POINTER(SelfGravState), ctypes.c_int,
+                                               ctypes.c_double, ctypes.c_int, _dp, _vp]),
+    "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class SSSError(RuntimeError):
+    """A libsss call failed (status code in .code)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libsss error {code}: {msg}")
+        self.code = code
+
+
+def load() -> ctypes.CDLL:
+    """Load libsss.so once and declare its signatures."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is not built; run `python -m solarsystemsimulator_b200.build` "
+                "(nvcc, sm_100a). There is no CPU fallback.")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+class Context:
+    """One sss_ctx on one CUDA device."""
+
+    def __init__(self, device: int):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device: the B200 kernels have no CPU fallback")
+        self.lib = load()
+        self.device = int(device)
+        ptr = _vp()
+        rc = self.lib.sss_create(self.device, ctypes.byref(ptr))
+        if rc != SSS_OK:
+            raise SSSError(rc, f"sss_create(device={device}) failed")
+        self.ptr = ptr
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None):
+                self.lib.sss_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        return self.lib.sss_last_error(self.ptr).decode(errors="replace")
+
+    def check(self, rc: int) -> None:
+        if rc == SSS_OK:
+            return
+        msg = self.last_error()
+        if rc == SSS_ERR_ARG:
+            raise ValueError(msg)
+        raise SSSError(rc, msg)
+
+    def status(self, stream: int) -> None:
+        self.check(self.lib.sss_device_status(self.ptr, _vp(stream)))
+
+    @property
+    def num_sms(self) -> int:
+        return int(self.lib.sss_num_sms(self.ptr))
+
+
+_contexts: dict[int, Context] = {}
+
+
+def context(device: int) -> Context:
+    """Process-wide context per device (created on first use)."""
+    with _lock:
+        c = _contexts.get(int(device))
+    if c is None:
+        c = Context(device)
+        with _lock:
+            _contexts[int(device)] = c
+    return c
+
+
+def stream_handle(device: int) -> int:
+    import torch
+    return int(torch.cuda.current_stream(device).cuda_stream)

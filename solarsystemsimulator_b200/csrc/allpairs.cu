@@ -1,0 +1,723 @@
+// All-pairs Plummer self-gravity for sm_100a.
+//
+// Replaces the tiled force loop `beschleunigung` and the KDK step loop of
+// `selfgrav_kernel` (reference backend/selfgrav_kernel.py:222-420).
+//
+// Work decomposition: a CTA owns a block of NT*R targets (R per thread, in
+// registers) and one CHUNK of the source list. Source tiles are staged in
+// shared memory by 1-D bulk async copies (cp.async.bulk + mbarrier, double
+// buffered) and read back as broadcast loads. Chunks split the source sum so
+// the grid has enough CTAs for an even load on 148 SMs; the chunk partials
+// are added in ascending chunk order by the last CTA of each target block to
+// arrive (arrival counted by one atomic per target block, no spinning), and
+// that CTA runs the integrator epilogue: closing half kick, snapshot, next
+// opening half kick and drift (the Yoshida / KDK sequence fused into the
+// force kernel). Within a chunk each target sums its sources in ascending
+// index order, as the reference does (selfgrav_kernel.py:235-256).
+//
+// f64 path: every operation in f64; r^-3 from an f32 seed refined in f64
+// (sss_gm_rinv3_f64). Mixed path: sources are pre-shifted per tile to the
+// tile's bounding-box centre and rounded to f32; each target's offset to the
+// centre is formed in f64 and rounded once per tile, so the f32 pair
+// difference is a difference of small numbers. Pair terms are summed in f32
+// over sub-tiles of MIX_SUB sources and folded into f64 accumulators.
+
+#include "sss_internal.cuh"
+
+namespace {
+
+constexpr int F64_NT = 256;   // threads per CTA, f64 path
+constexpr int F64_R = 4;      // targets per thread, f64 path
+constexpr int F64_TS = 512;   // sources per shared-memory tile (16 KiB)
+
+constexpr int MIX_NT = 256;
+constexpr int MIX_R = 4;
+constexpr int MIX_TS = 1024;  // sources per tile (float4: 16 KiB)
+constexpr int MIX_SUB = 128;  // f32 partial-sum length before the f64 fold
+
+constexpr int WAVES = 16;     // target number of CTA waves per evaluation
+
+struct Epi {
+    int mode;            // 0: write accelerations only; 1: integrator step
+    int last;            // mode 1: no opening kick / drift after this force
+    double4* acc;        // out: accelerations (both modes)
+    double4* vel;        // mode 1
+    double4* pos_nxt;    // mode 1: drifted positions
+    float* snap;         // mode 1: snapshot row or nullptr
+    double kc, ko, kd;   // closing kick, opening kick, drift factors
+    int64_t n_src, n_tr; // snapshot layout
+};
+
+struct ForceArgs {
+    const double4* src;      // f64 path: sources
+    const float4* srcf;      // mixed path: tile-shifted f32 sources
+    const double4* centers;  // mixed path: tile centres
+    int64_t n_src;
+    const double4* tgt;
+    int64_t n_tgt;
+    double eps2;
+    int n_tiles;
+    int n_chunks;
+    int tiles_per_chunk;
+    double4* part;           // [n_chunks][n_tgt] partial sums (n_chunks > 1)
+    unsigned* counters;      // [n_target_blocks]
+    int* status;
+    Epi epi;
+};
+
+template <int D>
+__device__ __forceinline__ void epilogue(const Epi& e, int64_t i, double ax, double ay,
+                                         double az, const double4& p) {
+    e.acc[i] = make_double4(ax, ay, az, 0.0);
+    if (e.mode == 0) return;
+    double4 v = e.vel[i];
+    // closing half kick, as `vx[i] += a0 * (0.5 * dt)` (selfgrav_kernel.py:366-367)
+    v.x += ax * e.kc;
+    v.y += ay * e.kc;
+    if (D == 3) v.z += az * e.kc;
+    if (e.snap != nullptr) {
+        if (i < e.n_src) {
+            const int64_t n = e.n_src;
+            e.snap[i] = (float)p.x;
+            e.snap[n + i] = (float)p.y;
+            if (D == 3) e.snap[2 * n + i] = (float)p.z;
+            float* sv = e.snap + D * n;
+            sv[i] = (float)v.x;
+            sv[n + i] = (float)v.y;
+            if (D == 3) sv[2 * n + i] = (float)v.z;
+        } else {
+            const int64_t t = i - e.n_src, m = e.n_tr;
+            float* st = e.snap + 2 * D * e.n_src;
+            st[t] = (float)p.x;
+            st[m + t] = (float)p.y;
+            if (D == 3) st[2 * m + t] = (float)p.z;
+        }
+    }
+    double4 q = p;
+    if (!e.last) {
+        // next opening half kick + drift (selfgrav_kernel.py:335-346)
+        v.x += ax * e.ko;
+        v.y += ay * e.ko;
+        if (D == 3) v.z += az * e.ko;
+        q.x = p.x + v.x * e.kd;
+        q.y = p.y + v.y * e.kd;
+        if (D == 3) q.z = p.z + v.z * e.kd;
+    }
+    e.vel[i] = v;
+    e.pos_nxt[i] = q;
+}
+
+// Chunk partial -> (last arriving CTA) fixed-order sum -> epilogue.
+// Returns after all work of this CTA is done.
+template <int D, int R, int NT>
+__device__ __forceinline__ void finish_block(const ForceArgs& a, int tb, int ch,
+                                             const double (&ax)[R], const double (&ay)[R],
+                                             const double (&az)[R]) {
+    __shared__ unsigned s_last;
+    const int tid = threadIdx.x;
+    const int64_t tbase = (int64_t)tb * (NT * R);
+    if (a.n_chunks == 1) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int64_t i = tbase + r * NT + tid;
+            if (i < a.n_tgt) epilogue<D>(a.epi, i, ax[r], ay[r], az[r], a.tgt[i]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t i = tbase + r * NT + tid;
+        if (i < a.n_tgt) {
+            double2* q = reinterpret_cast<double2*>(a.part + (int64_t)ch * a.n_tgt + i);
+            __stcg(q, make_double2(ax[r], ay[r]));
+            __stcg(q + 1, make_double2(az[r], 0.0));
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        const unsigned prev = atomicAdd(&a.counters[tb], 1u);
+        s_last = (prev == (unsigned)(a.n_chunks - 1)) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t i = tbase + r * NT + tid;
+        if (i >= a.n_tgt) continue;
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int c = 0; c < a.n_chunks; ++c) {
+            const double2* q = reinterpret_cast<const double2*>(a.part + (int64_t)c * a.n_tgt + i);
+            const double2 q0 = __ldcg(q), q1 = __ldcg(q + 1);
+            sx += q0.x;
+            sy += q0.y;
+            sz += q1.x;
+        }
+        epilogue<D>(a.epi, i, sx, sy, sz, a.tgt[i]);
+    }
+    if (tid == 0) a.counters[tb] = 0u;  // ready for the next launch
+}
+
+// Wait (bounded) for copies still in flight after an abort, so the CTA does
+// not exit while the async proxy writes its shared memory.
+__device__ __noinline__ void drain_after_abort(uint64_t* bar, int issued, int consumed, int* status) {
+    for (int k = consumed; k < issued; ++k) sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, status);
+}
+
+// ------------------------------------------------------------------ f64
+
+template <int D, int VAR>
+__device__ __forceinline__ double gm_rinv3(double gm, double r2) {
+    if (VAR == 0) return sss_gm_rinv3_f64(gm, r2);
+    return sss_gm_rinv3_cuda(gm, r2);
+}
+
+template <int D, int R, int NT, int TS, int VAR>
+__global__ void __launch_bounds__(NT, 2) k_force_f64(const ForceArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    double4* tiles = reinterpret_cast<double4*>(smem);
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_abort;
+
+    const int S = a.n_chunks;
+    const int tb = blockIdx.x / S;
+    const int ch = blockIdx.x - tb * S;
+    const int tid = threadIdx.x;
+    const int64_t tbase = (int64_t)tb * (NT * R);
+
+    double px[R], py[R], pz[R], ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t i = tbase + r * NT + tid;
+        const double4 p = (i < a.n_tgt) ? a.tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        px[r] = p.x; py[r] = p.y; pz[r] = p.z;
+        ax[r] = 0.0; ay[r] = 0.0; az[r] = 0.0;
+    }
+
+    const int t_begin = ch * a.tiles_per_chunk;
+    const int t_end = min(t_begin + a.tiles_per_chunk, a.n_tiles);
+    const int nt = t_end - t_begin;
+
+    if (tid == 0) {
+        s_abort = 0;
+        sss_mbar_init(&bar[0], 1);
+        sss_mbar_init(&bar[1], 1);
+        sss_fence_mbar_init();
+    }
+    __syncthreads();
+
+    int issued = 0;
+    auto issue = [&](int k) {
+        const int64_t j0 = (int64_t)(t_begin + k) * TS;
+        const int cnt = (int)min((int64_t)TS, a.n_src - j0);
+        const unsigned bytes = (unsigned)cnt * (unsigned)sizeof(double4);
+        sss_mbar_arrive_expect_tx(&bar[k & 1], bytes);
+        sss_bulk_g2s(tiles + (k & 1) * TS, a.src + j0, bytes, &bar[k & 1]);
+    };
+    if (tid == 0) {
+        issue(0);
+        issued = 1;
+        if (nt > 1) { issue(1); issued = 2; }
+    }
+
+    const double eps2 = a.eps2;
+    int k = 0;
+    for (; k < nt; ++k) {
+        const int64_t j0 = (int64_t)(t_begin + k) * TS;
+        const int cnt = (int)min((int64_t)TS, a.n_src - j0);
+        if (!sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status)) s_abort = 1;
+        __syncthreads();
+        if (s_abort) break;
+        const double4* s = tiles + (k & 1) * TS;
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) {
+            const double4 sj = s[j];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const double dx = sj.x - px[r];
+                const double dy = sj.y - py[r];
+                double r2;
+                double dz = 0.0;
+                if (D == 3) {
+                    dz = sj.z - pz[r];
+                    r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+                } else {
+                    r2 = fma(dx, dx, fma(dy, dy, eps2));
+                }
+                const double f = gm_rinv3<D, VAR>(sj.w, r2);
+                ax[r] = fma(f, dx, ax[r]);
+                ay[r] = fma(f, dy, ay[r]);
+                if (D == 3) az[r] = fma(f, dz, az[r]);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + 2 < nt) { issue(k + 2); issued = k + 3; }
+    }
+    if (k < nt) {  // aborted on a timed-out wait
+        if (tid == 0) drain_after_abort(bar, issued, k, a.status);
+        return;
+    }
+    finish_block<D, R, NT>(a, tb, ch, ax, ay, az);
+}
+
+// ---------------------------------------------------------------- mixed
+
+// One CTA per tile of MIX_TS sources: bounding-box centre (f64) and the
+// f32 offsets of every source from it (padding entries get Gm = 0).
+template <int D>
+__global__ void __launch_bounds__(256) k_prep_mixed(const double4* __restrict__ src, int64_t n_src,
+                                                    float4* __restrict__ out,
+                                                    double4* __restrict__ centers) {
+    __shared__ double red[6][8];
+    const int tile = blockIdx.x;
+    const int64_t j0 = (int64_t)tile * MIX_TS;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int j = threadIdx.x; j < MIX_TS; j += blockDim.x) {
+        const int64_t g = j0 + j;
+        if (g < n_src) {
+            const double4 s = src[g];
+            lo[0] = fmin(lo[0], s.x); hi[0] = fmax(hi[0], s.x);
+            lo[1] = fmin(lo[1], s.y); hi[1] = fmax(hi[1], s.y);
+            lo[2] = fmin(lo[2], s.z); hi[2] = fmax(hi[2], s.z);
+        }
+    }
+    for (int c = 0; c < 3; ++c) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        for (int c = 0; c < 3; ++c) { red[c][w] = lo[c]; red[3 + c][w] = hi[c]; }
+    }
+    __syncthreads();
+    double cen[3];
+    for (int c = 0; c < 3; ++c) {
+        double a = red[c][0], b = red[3 + c][0];
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) { a = fmin(a, red[c][q]); b = fmax(b, red[3 + c][q]); }
+        cen[c] = (a <= b) ? 0.5 * (a + b) : 0.0;
+    }
+    if (D == 2) cen[2] = 0.0;
+    if (threadIdx.x == 0) centers[tile] = make_double4(cen[0], cen[1], cen[2], 0.0);
+    for (int j = threadIdx.x; j < MIX_TS; j += blockDim.x) {
+        const int64_t g = j0 + j;
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (g < n_src) {
+            const double4 s = src[g];
+            o.x = __double2float_rn(s.x - cen[0]);
+            o.y = __double2float_rn(s.y - cen[1]);
+            o.z = (D == 3) ? __double2float_rn(s.z - cen[2]) : 0.f;
+            o.w = __double2float_rn(s.w);
+        }
+        out[j0 + j] = o;
+    }
+}
+
+template <int D, int R, int NT, int TS, int SUB>
+__global__ void __launch_bounds__(NT, 2) k_force_mixed(const ForceArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* tiles = reinterpret_cast<float4*>(smem);
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_abort;
+
+    const int S = a.n_chunks;
+    const int tb = blockIdx.x / S;
+    const int ch = blockIdx.x - tb * S;
+    const int tid = threadIdx.x;
+    const int64_t tbase = (int64_t)tb * (NT * R);
+
+    double px[R], py[R], pz[R], ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t i = tbase + r * NT + tid;
+        const double4 p = (i < a.n_tgt) ? a.tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        px[r] = p.x; py[r] = p.y; pz[r] = p.z;
+        ax[r] = 0.0; ay[r] = 0.0; az[r] = 0.0;
+    }
+
+    const int t_begin = ch * a.tiles_per_chunk;
+    const int t_end = min(t_begin + a.tiles_per_chunk, a.n_tiles);
+    const int nt = t_end - t_begin;
+
+    if (tid == 0) {
+        s_abort = 0;
+        sss_mbar_init(&bar[0], 1);
+        sss_mbar_init(&bar[1], 1);
+        sss_fence_mbar_init();
+    }
+    __syncthreads();
+
+    int issued = 0;
+    constexpr unsigned kTileBytes = TS * sizeof(float4);
+    auto issue = [&](int k) {
+        sss_mbar_arrive_expect_tx(&bar[k & 1], kTileBytes);
+        sss_bulk_g2s(tiles + (k & 1) * TS, a.srcf + (int64_t)(t_begin + k) * TS, kTileBytes, &bar[k & 1]);
+    };
+    if (tid == 0) {
+        issue(0);
+        issued = 1;
+        if (nt > 1) { issue(1); issued = 2; }
+    }
+
+    const float eps2f = (float)a.eps2;
+    int k = 0;
+    for (; k < nt; ++k) {
+        const int tile = t_begin + k;
+        const int64_t j0 = (int64_t)tile * TS;
+        const int cnt = (int)min((int64_t)TS, a.n_src - j0);
+        const double4 c = a.centers[tile];
+        float ox[R], oy[R], oz[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            ox[r] = __double2float_rn(c.x - px[r]);
+            oy[r] = __double2float_rn(c.y - py[r]);
+            oz[r] = (D == 3) ? __double2float_rn(c.z - pz[r]) : 0.f;
+        }
+        if (!sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status)) s_abort = 1;
+        __syncthreads();
+        if (s_abort) break;
+        const float4* s = tiles + (k & 1) * TS;
+        for (int js = 0; js < cnt; js += SUB) {
+            const int je = min(js + SUB, cnt);
+            float fx[R], fy[R], fz[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) { fx[r] = 0.f; fy[r] = 0.f; fz[r] = 0.f; }
+#pragma unroll 4
+            for (int j = js; j < je; ++j) {
+                const float4 sj = s[j];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const float dx = sj.x + ox[r];
+                    const float dy = sj.y + oy[r];
+                    float r2, dz = 0.f;
+                    if (D == 3) {
+                        dz = sj.z + oz[r];
+                        r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2f)));
+                    } else {
+                        r2 = fmaf(dx, dx, fmaf(dy, dy, eps2f));
+                    }
+                    const float inv = sss_rsqrt_approx_f32(r2);
+                    const float inv2 = inv * inv;
+                    const float f = (sj.w * inv) * inv2;
+                    fx[r] = fmaf(f, dx, fx[r]);
+                    fy[r] = fmaf(f, dy, fy[r]);
+                    if (D == 3) fz[r] = fmaf(f, dz, fz[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                ax[r] += (double)fx[r];
+                ay[r] += (double)fy[r];
+                if (D == 3) az[r] += (double)fz[r];
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + 2 < nt) { issue(k + 2); issued = k + 3; }
+    }
+    if (k < nt) {
+        if (tid == 0) drain_after_abort(bar, issued, k, a.status);
+        return;
+    }
+    finish_block<D, R, NT>(a, tb, ch, ax, ay, az);
+}
+
+// ------------------------------------------------------------- potential
+
+// phi_t = -sum_s Gm_s / sqrt(|d|^2 + eps2), f64, one target per thread,
+// sources through shared memory in ascending order (diagnostic path).
+template <int D>
+__global__ void __launch_bounds__(256) k_potential(const double4* __restrict__ src, int64_t n_src,
+                                                   const double4* __restrict__ tgt, int64_t n_tgt,
+                                                   double* __restrict__ phi, double eps2) {
+    __shared__ double4 sh[256];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const double4 p = (i < n_tgt) ? tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    double acc = 0.0;
+    for (int64_t j0 = 0; j0 < n_src; j0 += 256) {
+        const int64_t g = j0 + threadIdx.x;
+        sh[threadIdx.x] = (g < n_src) ? src[g] : make_double4(0.0, 0.0, 0.0, 0.0);
+        __syncthreads();
+        const int cnt = (int)min((int64_t)256, n_src - j0);
+        for (int j = 0; j < cnt; ++j) {
+            const double4 s = sh[j];
+            const double dx = s.x - p.x, dy = s.y - p.y;
+            double r2 = dx * dx + dy * dy + eps2;
+            if (D == 3) { const double dz = s.z - p.z; r2 += dz * dz; }
+            acc += s.w * rsqrt(r2);
+        }
+        __syncthreads();
+    }
+    if (i < n_tgt) phi[i] = -acc;
+}
+
+// -------------------------------------------------------------- integrate
+
+// Opening half kick + drift of the first substep of a batch.
+template <int D>
+__global__ void k_open(const double4* __restrict__ pos, double4* __restrict__ pos_nxt,
+                       double4* __restrict__ vel, const double4* __restrict__ acc, int64_t n,
+                       double ko, double kd) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 a = acc[i];
+    double4 v = vel[i];
+    const double4 p = pos[i];
+    v.x += a.x * ko;
+    v.y += a.y * ko;
+    if (D == 3) v.z += a.z * ko;
+    double4 q = p;
+    q.x = p.x + v.x * kd;
+    q.y = p.y + v.y * kd;
+    if (D == 3) q.z = p.z + v.z * kd;
+    vel[i] = v;
+    pos_nxt[i] = q;
+}
+
+// ---------------------------------------------------------------- host side
+
+struct Plan {
+    int n_tblocks, n_tiles, n_chunks, tiles_per_chunk;
+};
+
+Plan make_plan(int64_t n_src, int64_t n_tgt, int targets_per_block, int ts, int slots) {
+    Plan p;
+    p.n_tblocks = (int)((n_tgt + targets_per_block - 1) / targets_per_block);
+    p.n_tiles = (int)((n_src + ts - 1) / ts);
+    const int64_t want = (int64_t)WAVES * slots;
+    int64_t s = (want + p.n_tblocks - 1) / p.n_tblocks;
+    if (s < 1) s = 1;
+    if (s > p.n_tiles) s = p.n_tiles;
+    p.tiles_per_chunk = (int)((p.n_tiles + s - 1) / s);
+    p.n_chunks = (p.n_tiles + p.tiles_per_chunk - 1) / p.tiles_per_chunk;
+    return p;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+int force_eval(sss_ctx* ctx, int dim, int precision, const double4* src, int64_t n_src,
+               const double4* tgt, int64_t n_tgt, double eps2, const Epi& epi, cudaStream_t stream) {
+    if (n_tgt <= 0) return SSS_OK;
+    if (n_src <= 0) {
+        // no sources: zero accelerations, the epilogue still integrates
+        return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: n_src must be >= 1");
+    }
+    if (n_src > ((int64_t)1 << 40) || n_tgt > ((int64_t)1 << 40))
+        return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: size out of range");
+    ForceArgs a;
+    memset(&a, 0, sizeof(a));
+    a.src = src;
+    a.n_src = n_src;
+    a.tgt = tgt;
+    a.n_tgt = n_tgt;
+    a.eps2 = eps2;
+    a.status = ctx->d_status;
+    a.epi = epi;
+
+    const bool mixed = (precision == SSS_PREC_MIXED);
+    const int nt = mixed ? MIX_NT : F64_NT;
+    const int tpb = mixed ? MIX_NT * MIX_R : F64_NT * F64_R;
+    const int ts = mixed ? MIX_TS : F64_TS;
+    const size_t smem = mixed ? 2 * MIX_TS * sizeof(float4) : 2 * F64_TS * sizeof(double4);
+
+    void* kfn;
+    if (mixed) kfn = (dim == 3) ? (void*)k_force_mixed<3, MIX_R, MIX_NT, MIX_TS, MIX_SUB>
+                                : (void*)k_force_mixed<2, MIX_R, MIX_NT, MIX_TS, MIX_SUB>;
+    else kfn = (dim == 3) ? (void*)k_force_f64<3, F64_R, F64_NT, F64_TS, 0>
+                          : (void*)k_force_f64<2, F64_R, F64_NT, F64_TS, 0>;
+    const int key = (mixed ? 2 : 0) + (dim == 3 ? 1 : 0);
+    if (ctx->occ[key] == 0) {
+        SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        ctx->occ[key] = per_sm;
+    }
+    const int per_sm = ctx->occ[key];
+    const Plan pl = make_plan(n_src, n_tgt, tpb, ts, per_sm * ctx->num_sms);
+    a.n_tiles = pl.n_tiles;
+    a.n_chunks = pl.n_chunks;
+    a.tiles_per_chunk = pl.tiles_per_chunk;
+
+    // scratch: [mixed tiles][centres][partials]
+    size_t off = 0;
+    size_t bytes_tiles = 0, bytes_cent = 0, bytes_part = 0;
+    if (mixed) {
+        bytes_tiles = (size_t)pl.n_tiles * MIX_TS * sizeof(float4);
+        bytes_cent = ((size_t)pl.n_tiles * sizeof(double4) + 255) & ~(size_t)255;
+    }
+    if (pl.n_chunks > 1) bytes_part = (size_t)pl.n_chunks * (size_t)n_tgt * sizeof(double4);
+    void* scr = nullptr;
+    const size_t total = bytes_tiles + bytes_cent + bytes_part;
+    if (total > 0) {
+        int rc = sss_scratch(ctx, total, &scr);
+        if (rc) return rc;
+    }
+    if (mixed) {
+        a.srcf = (const float4*)((char*)scr + off);
+        off += bytes_tiles;
+        a.centers = (const double4*)((char*)scr + off);
+        off += bytes_cent;
+    }
+    if (pl.n_chunks > 1) a.part = (double4*)((char*)scr + off);
+    if (pl.n_chunks > 1) {
+        int rc = sss_counters(ctx, (size_t)pl.n_tblocks, &a.counters);
+        if (rc) return rc;
+    }
+
+    if (mixed) {
+        if (dim == 3)
+            k_prep_mixed<3><<<pl.n_tiles, 256, 0, stream>>>(src, n_src, (float4*)a.srcf, (double4*)a.centers);
+        else
+            k_prep_mixed<2><<<pl.n_tiles, 256, 0, stream>>>(src, n_src, (float4*)a.srcf, (double4*)a.centers);
+        SSS_LAUNCH_CHECK(ctx, "k_prep_mixed launch");
+    }
+    const unsigned grid = (unsigned)pl.n_tblocks * (unsigned)pl.n_chunks;
+    void* args[] = {&a};
+    SSS_CUDA_TRY(ctx, cudaLaunchKernel(kfn, dim3(grid), dim3(nt), args, smem, stream));
+    return SSS_OK;
+}
+
+int check_common(sss_ctx* ctx, int dim, int precision) {
+    if (!ctx) return SSS_ERR_ARG;
+    if (dim != 2 && dim != 3) return sss_set_err(ctx, SSS_ERR_ARG, "dim must be 2 or 3 (got %d)", dim);
+    if (precision != SSS_PREC_F64 && precision != SSS_PREC_MIXED)
+        return sss_set_err(ctx, SSS_ERR_ARG, "precision must be SSS_PREC_F64 or SSS_PREC_MIXED (got %d)", precision);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return sss_set_err(ctx, SSS_ERR_CUDA, "cudaSetDevice failed");
+    return SSS_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" int sss_allpairs_accel(sss_ctx* ctx, int dim, int precision, const double* src4, int64_t n_src,
+                                  const double* tgt4, int64_t n_tgt, double* acc4, double eps2,
+                                  void* stream) {
+    int rc = check_common(ctx, dim, precision);
+    if (rc) return rc;
+    if (n_tgt < 0 || n_src < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
+    if (n_tgt == 0) return SSS_OK;
+    if (!src4 || !tgt4 || !acc4) return sss_set_err(ctx, SSS_ERR_ARG, "NULL pointer");
+    if (!aligned16(src4) || !aligned16(tgt4) || !aligned16(acc4))
+        return sss_set_err(ctx, SSS_ERR_ARG, "pointers must be 16-byte aligned");
+    if (!(eps2 >= 0.0)) return sss_set_err(ctx, SSS_ERR_ARG, "eps2 must be >= 0");
+    Epi e;
+    memset(&e, 0, sizeof(e));
+    e.mode = 0;
+    e.acc = (double4*)acc4;
+    return force_eval(ctx, dim, precision, (const double4*)src4, n_src, (const double4*)tgt4, n_tgt, eps2, e,
+                      (cudaStream_t)stream);
+}
+
+extern "C" int sss_allpairs_potential(sss_ctx* ctx, int dim, const double* src4, int64_t n_src,
+                                      const double* tgt4, int64_t n_tgt, double* phi, double eps2,
+                                      void* stream) {
+    int rc = check_common(ctx, dim, SSS_PREC_F64);
+    if (rc) return rc;
+    if (n_tgt < 0 || n_src < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
+    if (n_tgt == 0) return SSS_OK;
+    if (!src4 || !tgt4 || !phi) return sss_set_err(ctx, SSS_ERR_ARG, "NULL pointer");
+    const unsigned grid = (unsigned)((n_tgt + 255) / 256);
+    if (dim == 3)
+        k_potential<3><<<grid, 256, 0, (cudaStream_t)stream>>>((const double4*)src4, n_src, (const double4*)tgt4,
+                                                                n_tgt, phi, eps2);
+    else
+        k_potential<2><<<grid, 256, 0, (cudaStream_t)stream>>>((const double4*)src4, n_src, (const double4*)tgt4,
+                                                                n_tgt, phi, eps2);
+    SSS_LAUNCH_CHECK(ctx, "k_potential launch");
+    return SSS_OK;
+}
+
+static int check_state(sss_ctx* ctx, const sss_selfgrav_state* st) {
+    if (!st) return sss_set_err(ctx, SSS_ERR_ARG, "NULL state");
+    int rc = check_common(ctx, st->dim, st->precision);
+    if (rc) return rc;
+    if (st->n_src < 1) return sss_set_err(ctx, SSS_ERR_ARG, "state needs at least one massive body");
+    if (st->n_tracer < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative tracer count");
+    if (st->cur != 0 && st->cur != 1) return sss_set_err(ctx, SSS_ERR_ARG, "cur must be 0 or 1");
+    if (!st->pos4[0] || !st->pos4[1] || !st->vel4 || !st->acc4) return sss_set_err(ctx, SSS_ERR_ARG, "NULL buffer");
+    if (!aligned16(st->pos4[0]) || !aligned16(st->pos4[1]) || !aligned16(st->vel4) || !aligned16(st->acc4))
+        return sss_set_err(ctx, SSS_ERR_ARG, "buffers must be 16-byte aligned");
+    if (!(st->eps2 > 0.0)) return sss_set_err(ctx, SSS_ERR_ARG, "softening must be positive");
+    return SSS_OK;
+}
+
+extern "C" int sss_selfgrav_init_accel(sss_ctx* ctx, sss_selfgrav_state* st, void* stream) {
+    int rc = check_state(ctx, st);
+    if (rc) return rc;
+    const int64_t n_all = st->n_src + st->n_tracer;
+    const double4* pos = (const double4*)st->pos4[st->cur];
+    Epi e;
+    memset(&e, 0, sizeof(e));
+    e.mode = 0;
+    e.acc = (double4*)st->acc4;
+    return force_eval(ctx, st->dim, st->precision, pos, st->n_src, pos, n_all, st->eps2, e, (cudaStream_t)stream);
+}
+
+extern "C" int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st, int integrator, double dt,
+                                       int steps, float* snap, void* stream) {
+    int rc = check_state(ctx, st);
+    if (rc) return rc;
+    if (steps < 1) return sss_set_err(ctx, SSS_ERR_ARG, "steps must be >= 1 (got %d)", steps);
+    if (integrator != SSS_INT_KDK && integrator != SSS_INT_YOSHIDA4)
+        return sss_set_err(ctx, SSS_ERR_ARG, "unknown integrator %d", integrator);
+    if (!(dt == dt)) return sss_set_err(ctx, SSS_ERR_ARG, "dt is NaN");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int D = st->dim;
+    const int64_t n_all = st->n_src + st->n_tracer;
+    const int64_t row = 2 * (int64_t)D * st->n_src + (int64_t)D * st->n_tracer;
+
+    // substep weights (Yoshida 1990 fourth-order triple-jump composition)
+    double w[3];
+    int nsub;
+    if (integrator == SSS_INT_KDK) {
+        nsub = 1;
+        w[0] = 1.0;
+    } else {
+        const double cbrt2 = cbrt(2.0);
+        nsub = 3;
+        w[0] = 1.0 / (2.0 - cbrt2);
+        w[1] = -cbrt2 / (2.0 - cbrt2);
+        w[2] = w[0];
+    }
+
+    // opening half kick + drift of the first substep
+    {
+        const double4* p = (const double4*)st->pos4[st->cur];
+        double4* q = (double4*)st->pos4[1 - st->cur];
+        const unsigned grid = (unsigned)((n_all + 255) / 256);
+        if (D == 3)
+            k_open<3><<<grid, 256, 0, s>>>(p, q, (double4*)st->vel4, (const double4*)st->acc4, n_all,
+                                          0.5 * w[0] * dt, w[0] * dt);
+        else
+            k_open<2><<<grid, 256, 0, s>>>(p, q, (double4*)st->vel4, (const double4*)st->acc4, n_all,
+                                          0.5 * w[0] * dt, w[0] * dt);
+        SSS_LAUNCH_CHECK(ctx, "k_open launch");
+        st->cur = 1 - st->cur;
+    }
+    for (int step = 0; step < steps; ++step) {
+        for (int k = 0; k < nsub; ++k) {
+            Epi e;
+            memset(&e, 0, sizeof(e));
+            e.mode = 1;
+            e.last = (step == steps - 1 && k == nsub - 1) ? 1 : 0;
+            e.acc = (double4*)st->acc4;
+            e.vel = (double4*)st->vel4;
+            e.pos_nxt = (double4*)st->pos4[1 - st->cur];
+            e.snap = (snap && k == nsub - 1) ? snap + (int64_t)step * row : nullptr;
+            e.kc = 0.5 * w[k] * dt;
+            const int kn = (k + 1) % nsub;
+            e.ko = 0.5 * w[kn] * dt;
+            e.kd = w[kn] * dt;
+            e.n_src = st->n_src;
+            e.n_tr = st->n_tracer;
+            const double4* pos = (const double4*)st->pos4[st->cur];
+            rc = force_eval(ctx, D, st->precision, pos, st->n_src, pos, n_all, st->eps2, e, s);
+            if (rc) return rc;
+            st->cur = 1 - st->cur;
+        }
+    }
+    return SSS_OK;
+}

@@ -1,0 +1,84 @@
+// FMA-throughput probe: the FP64 / FP32 SIMT peaks the all-pairs kernels
+// are measured against (the driver-measured peaks cover only HBM copy and
+// bf16 tensor GEMM). Diagnostic entry point, no reference counterpart.
+#include "sss_internal.cuh"
+
+namespace {
+
+constexpr int CHAINS = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_chain(T* out, int iters, T a, T b) {
+    T x[CHAINS];
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) x[c] = (T)(threadIdx.x + c) * (T)1e-3;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < CHAINS; ++c) x[c] = fma(x[c], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) s += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// packed f32x2 FMA (sm_100a): two f32 lanes per thread per instruction
+__global__ void __launch_bounds__(256) k_fma_chain_x2(float* out, int iters, float a, float b) {
+    unsigned long long x[CHAINS];
+    unsigned long long av, bv;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(av) : "f"(a));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(bv) : "f"(b));
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) {
+        const float v0 = (float)(threadIdx.x + c) * 1e-3f, v1 = v0 + 0.5f;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(x[c]) : "f"(v0), "f"(v1));
+    }
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < CHAINS; ++c)
+            asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(x[c]) : "l"(av), "l"(bv));
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) {
+        float lo, hi;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x[c]));
+        s += lo + hi;
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+extern "C" int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops) {
+    if (!ctx || !tflops) return SSS_ERR_ARG;
+    if (kind < 0 || kind > 2) return sss_set_err(ctx, SSS_ERR_ARG, "kind must be 0 (f64), 1 (f32), 2 (f32x2)");
+    if (iters < 1) return sss_set_err(ctx, SSS_ERR_ARG, "iters must be >= 1");
+    SSS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    const int blocks = ctx->num_sms * 8, threads = 256;
+    void* out = nullptr;
+    int rc = sss_scratch(ctx, (size_t)blocks * threads * sizeof(double), &out);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    SSS_CUDA_TRY(ctx, cudaEventCreate(&e0));
+    SSS_CUDA_TRY(ctx, cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {  // first launch is a warm-up
+        cudaEventRecord(e0);
+        if (kind == 0) k_fma_chain<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+        else if (kind == 1) k_fma_chain<float><<<blocks, threads>>>((float*)out, iters, 0.9999f, 1e-4f);
+        else k_fma_chain_x2<<<blocks, threads>>>((float*)out, iters, 0.9999f, 1e-4f);
+        cudaEventRecord(e1);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return sss_cuda_err(ctx, e, "probe kernel");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best_ms) best_ms = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double lanes_per_fma = (kind == 2) ? 2.0 : 1.0;
+    const double flops = 2.0 * lanes_per_fma * CHAINS * (double)iters * blocks * threads;
+    *tflops = flops / (best_ms * 1e-3) / 1e12;
+    return SSS_OK;
+}
