@@ -170,11 +170,12 @@ __device__ __noinline__ void drain_after_abort(uint64_t* bar, int issued, int co
 template <int D, int VAR>
 __device__ __forceinline__ double gm_rinv3(double gm, double r2) {
     if (VAR == 0) return sss_gm_rinv3_f64(gm, r2);
+    if (VAR == 2) return sss_gm_rinv3_f64_iseed(gm, r2);
     return sss_gm_rinv3_cuda(gm, r2);
 }
 
-template <int D, int R, int NT, int TS, int VAR>
-__global__ void __launch_bounds__(NT, 2) k_force_f64(const ForceArgs a) {
+template <int D, int R, int NT, int TS, int VAR, int MINB = 2, int UNROLL = 2>
+__global__ void __launch_bounds__(NT, MINB) k_force_f64(const ForceArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     double4* tiles = reinterpret_cast<double4*>(smem);
     __shared__ __align__(8) uint64_t bar[2];
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(NT, 2) k_force_f64(const ForceArgs a) {
         __syncthreads();
         if (s_abort) break;
         const double4* s = tiles + (k & 1) * TS;
-#pragma unroll 2
+#pragma unroll UNROLL
         for (int j = 0; j < cnt; ++j) {
             const double4 sj = s[j];
 #pragma unroll
@@ -411,6 +412,214 @@ __global__ void __launch_bounds__(NT, 2) k_force_mixed(const ForceArgs a) {
                 ax[r] += (double)fx[r];
                 ay[r] += (double)fy[r];
                 if (D == 3) az[r] += (double)fz[r];
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && k + 2 < nt) { issue(k + 2); issued = k + 3; }
+    }
+    if (k < nt) {
+        if (tid == 0) drain_after_abort(bar, issued, k, a.status);
+        return;
+    }
+    finish_block<D, R, NT>(a, tb, ch, ax, ay, az);
+}
+
+// -------------------------------------------------------- mixed, packed
+//
+// Same arithmetic as k_force_mixed, issued as packed f32x2 instructions
+// (sm_100a add/mul/fma .f32x2): two targets of a thread share one
+// instruction. The FP32 lanes do the same work; the packed form halves the
+// issue slots per pair, which is what bounds the scalar loop. Tiles hold
+// each source duplicated, {x,x,y,y},{z,z,Gm,Gm}, so one shared-memory load
+// yields the packed operands directly.
+
+typedef unsigned long long f2x;
+
+__device__ __forceinline__ f2x pk2(float lo, float hi) {
+    f2x r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(f2x v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b) {
+    f2x d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
+    f2x d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
+    f2x d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+constexpr int MX2_NT = 256;
+constexpr int MX2_R = 4;      // targets per thread (2 packed pairs)
+constexpr int MX2_TS = 512;   // sources per tile (32 B each: 16 KiB)
+constexpr int MX2_SUB = 128;
+
+template <int D, int TS>
+__global__ void __launch_bounds__(256) k_prep_mixed2(const double4* __restrict__ src, int64_t n_src,
+                                                     float4* __restrict__ out,
+                                                     double4* __restrict__ centers) {
+    __shared__ double red[6][8];
+    const int tile = blockIdx.x;
+    const int64_t j0 = (int64_t)tile * TS;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int j = threadIdx.x; j < TS; j += blockDim.x) {
+        const int64_t g = j0 + j;
+        if (g < n_src) {
+            const double4 s = src[g];
+            lo[0] = fmin(lo[0], s.x); hi[0] = fmax(hi[0], s.x);
+            lo[1] = fmin(lo[1], s.y); hi[1] = fmax(hi[1], s.y);
+            lo[2] = fmin(lo[2], s.z); hi[2] = fmax(hi[2], s.z);
+        }
+    }
+    for (int c = 0; c < 3; ++c) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        for (int c = 0; c < 3; ++c) { red[c][w] = lo[c]; red[3 + c][w] = hi[c]; }
+    }
+    __syncthreads();
+    double cen[3];
+    for (int c = 0; c < 3; ++c) {
+        double a = red[c][0], b = red[3 + c][0];
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) { a = fmin(a, red[c][q]); b = fmax(b, red[3 + c][q]); }
+        cen[c] = (a <= b) ? 0.5 * (a + b) : 0.0;
+    }
+    if (D == 2) cen[2] = 0.0;
+    if (threadIdx.x == 0) centers[tile] = make_double4(cen[0], cen[1], cen[2], 0.0);
+    for (int j = threadIdx.x; j < TS; j += blockDim.x) {
+        const int64_t g = j0 + j;
+        float x = 0.f, y = 0.f, z = 0.f, m = 0.f;
+        if (g < n_src) {
+            const double4 s = src[g];
+            x = __double2float_rn(s.x - cen[0]);
+            y = __double2float_rn(s.y - cen[1]);
+            z = (D == 3) ? __double2float_rn(s.z - cen[2]) : 0.f;
+            m = __double2float_rn(s.w);
+        }
+        out[2 * (j0 + j)] = make_float4(x, x, y, y);
+        out[2 * (j0 + j) + 1] = make_float4(z, z, m, m);
+    }
+}
+
+template <int D, int R, int NT, int TS, int SUB, int MINB = 2>
+__global__ void __launch_bounds__(NT, MINB) k_force_mixed2(const ForceArgs a) {
+    static_assert(R % 2 == 0, "packed kernel needs an even target count");
+    constexpr int P = R / 2;
+    extern __shared__ __align__(128) unsigned char smem[];
+    ulonglong2* tiles = reinterpret_cast<ulonglong2*>(smem);   // [2][TS][2]
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_abort;
+
+    const int S = a.n_chunks;
+    const int tb = blockIdx.x / S;
+    const int ch = blockIdx.x - tb * S;
+    const int tid = threadIdx.x;
+    const int64_t tbase = (int64_t)tb * (NT * R);
+
+    double px[R], py[R], pz[R], ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t i = tbase + r * NT + tid;
+        const double4 p = (i < a.n_tgt) ? a.tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        px[r] = p.x; py[r] = p.y; pz[r] = p.z;
+        ax[r] = 0.0; ay[r] = 0.0; az[r] = 0.0;
+    }
+
+    const int t_begin = ch * a.tiles_per_chunk;
+    const int t_end = min(t_begin + a.tiles_per_chunk, a.n_tiles);
+    const int nt = t_end - t_begin;
+
+    if (tid == 0) {
+        s_abort = 0;
+        sss_mbar_init(&bar[0], 1);
+        sss_mbar_init(&bar[1], 1);
+        sss_fence_mbar_init();
+    }
+    __syncthreads();
+
+    int issued = 0;
+    constexpr unsigned kTileBytes = TS * 2 * sizeof(float4);
+    const float4* srcf = a.srcf;
+    auto issue = [&](int k) {
+        sss_mbar_arrive_expect_tx(&bar[k & 1], kTileBytes);
+        sss_bulk_g2s(tiles + (k & 1) * TS * 2, srcf + (int64_t)(t_begin + k) * TS * 2, kTileBytes, &bar[k & 1]);
+    };
+    if (tid == 0) {
+        issue(0);
+        issued = 1;
+        if (nt > 1) { issue(1); issued = 2; }
+    }
+
+    const float eps2f = (float)a.eps2;
+    const f2x eps2x = pk2(eps2f, eps2f);
+    int k = 0;
+    for (; k < nt; ++k) {
+        const int tile = t_begin + k;
+        const int64_t j0 = (int64_t)tile * TS;
+        const int cnt = (int)min((int64_t)TS, a.n_src - j0);
+        const double4 c = a.centers[tile];
+        f2x ox[P], oy[P], oz[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            ox[q] = pk2(__double2float_rn(c.x - px[2 * q]), __double2float_rn(c.x - px[2 * q + 1]));
+            oy[q] = pk2(__double2float_rn(c.y - py[2 * q]), __double2float_rn(c.y - py[2 * q + 1]));
+            oz[q] = (D == 3) ? pk2(__double2float_rn(c.z - pz[2 * q]), __double2float_rn(c.z - pz[2 * q + 1]))
+                             : pk2(0.f, 0.f);
+        }
+        if (!sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status)) s_abort = 1;
+        __syncthreads();
+        if (s_abort) break;
+        const ulonglong2* s = tiles + (k & 1) * TS * 2;
+        for (int js = 0; js < cnt; js += SUB) {
+            const int je = min(js + SUB, cnt);
+            f2x fx[P], fy[P], fz[P];
+#pragma unroll
+            for (int q = 0; q < P; ++q) { fx[q] = 0ull; fy[q] = 0ull; fz[q] = 0ull; }
+#pragma unroll 4
+            for (int j = js; j < je; ++j) {
+                const ulonglong2 xy = s[2 * j];
+                const ulonglong2 zw = s[2 * j + 1];
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    const f2x dx = add2(xy.x, ox[q]);
+                    const f2x dy = add2(xy.y, oy[q]);
+                    f2x r2;
+                    f2x dz = 0ull;
+                    if (D == 3) {
+                        dz = add2(zw.x, oz[q]);
+                        r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, eps2x)));
+                    } else {
+                        r2 = fma2(dx, dx, fma2(dy, dy, eps2x));
+                    }
+                    float r0, r1;
+                    upk2(r2, r0, r1);
+                    const f2x inv = pk2(sss_rsqrt_approx_f32(r0), sss_rsqrt_approx_f32(r1));
+                    const f2x f = mul2(mul2(zw.y, inv), mul2(inv, inv));
+                    fx[q] = fma2(f, dx, fx[q]);
+                    fy[q] = fma2(f, dy, fy[q]);
+                    if (D == 3) fz[q] = fma2(f, dz, fz[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                float l0, l1;
+                upk2(fx[q], l0, l1); ax[2 * q] += (double)l0; ax[2 * q + 1] += (double)l1;
+                upk2(fy[q], l0, l1); ay[2 * q] += (double)l0; ay[2 * q + 1] += (double)l1;
+                if (D == 3) { upk2(fz[q], l0, l1); az[2 * q] += (double)l0; az[2 * q + 1] += (double)l1; }
             }
         }
         __syncthreads();
@@ -721,3 +930,4 @@ extern "C" int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st, int
     }
     return SSS_OK;
 }
+

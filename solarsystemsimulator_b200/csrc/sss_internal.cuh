@@ -143,6 +143,25 @@ __device__ __forceinline__ double sss_gm_rinv3_f64(double gm, double r2) {
     return fma(g3, e * p, g3);                  // Gm c^3 (1 + e p)
 }
 
+// Same series with the seed's argument formed by integer operations instead
+// of an f64->f32 conversion: the high word of r2 (sign, 11-bit exponent, 20
+// mantissa bits) re-biased to an f32 bit pattern (mantissa truncated, |rel.
+// error| < 2^-20), and the f32 result widened to f64 bit by bit. Valid for
+// 2^-126 <= r2 < 2^128 (|e| < 1.3e-6, cubic remainder < 5e-18).
+__device__ __forceinline__ double sss_gm_rinv3_f64_iseed(double gm, double r2) {
+    const unsigned hi = (unsigned)__double2hiint(r2);
+    const unsigned fb = (hi << 3) + 0x40000000u;          // exponent 1023 -> 127 bias
+    const float yf = sss_rsqrt_approx_f32(__uint_as_float(fb));
+    const unsigned yb = __float_as_uint(yf);
+    const double c = __hiloint2double((int)((yb >> 3) + 0x38000000u), (int)(yb << 29));
+    const double c2 = c * c;
+    const double e = fma(-r2, c2, 1.0);
+    const double p = fma(e, 1.875, 1.5);
+    const double g = gm * c;
+    const double g3 = g * c2;
+    return fma(g3, e * p, g3);
+}
+
 // Same value from CUDA's own f64 rsqrt (kept as a selectable variant so the
 // faster form can be chosen by measurement).
 __device__ __forceinline__ double sss_gm_rinv3_cuda(double gm, double r2) {
