@@ -131,6 +131,45 @@ int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st,
                             int integrator, double dt, int steps,
                             float* snap, void* stream);
 
+/* ----------------------------------------------- no-allocation variant
+ *
+ * sss_allpairs_accel_noalloc computes exactly what sss_allpairs_accel
+ * computes, for callers that may not allocate device memory: a host
+ * application that owns the whole device-memory budget and hands libraries
+ * only the buffers it sized in advance (an engine with its own arena
+ * allocator, a plugin host that forbids library allocations), or a
+ * latency-critical loop that cannot afford cudaMalloc/cudaFree, which block
+ * and synchronise the device. It needs no sss_ctx and calls no cudaMalloc,
+ * cudaFree or allocating library routine.
+ *
+ * Its scratch is one file-scope device array of SSS_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading libsss holds until the process exits. Limits: in
+ * mixed precision n_src <= SSS_NOALLOC_MAX_MIXED_SOURCES (the f32 source
+ * tiles must fit), SSS_ERR_CAPACITY otherwise; f64 has no source limit.
+ * When the chunk partial sums of the source split do not fit, the split is
+ * narrowed (down to a single chunk), which changes only the order in which
+ * chunk partials are added (rounding-level differences).
+ *
+ * The first call on a device does a one-time set-up with that device
+ * current (it resolves the array's device address with
+ * cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the array and finds the previous call's contents in it;
+ * the call clears what must start at zero. Calls whose work overlaps on the
+ * GPU (different streams, or devices sharing no order) race on the array:
+ * order them on one stream.
+ *
+ * device: CUDA device of all pointers (made current). d_status: optional
+ * device int that a timed-out bounded wait sets to SSS_ERR_TIMEOUT (NULL =
+ * an internal word). errbuf/errbuf_len: optional host buffer for a message.
+ * No reference counterpart. */
+#define SSS_NOALLOC_SCRATCH_BYTES     (32u << 20)
+#define SSS_NOALLOC_MAX_MIXED_SOURCES 2088960
+int sss_allpairs_accel_noalloc(int device, int dim, int precision,
+                               const double* src4, int64_t n_src,
+                               const double* tgt4, int64_t n_tgt,
+                               double* acc4, double eps2, int* d_status,
+                               void* stream, char* errbuf, size_t errbuf_len);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /* Measured FMA throughput of the device in TFLOP/s (2 flops per FMA lane):

@@ -61,6 +61,9 @@ SIGNATURES = {
     "sss_selfgrav_step_batch": (ctypes.c_int, [_vp, ctypes.POINTER(SelfGravState), ctypes.c_int,
                                                ctypes.c_double, ctypes.c_int, _dp, _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
+                                                  _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,
+                                                  ctypes.c_char_p, ctypes.c_size_t]),
 }
 
 _lib = None

@@ -24,6 +24,8 @@
 
 #include "sss_internal.cuh"
 
+#include <pthread.h>
+
 namespace {
 
 constexpr int F64_NT = 256;   // threads per CTA, f64 path
@@ -931,3 +933,198 @@ extern "C" int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st, int
     return SSS_OK;
 }
 
+// ------------------------------------------------ no-allocation variant
+//
+// sss_allpairs_accel_noalloc: the all-pairs force of sss_allpairs_accel for
+// callers that must not allocate device memory (see include/sss.h). Its
+// scratch (status word, chunk-arrival counters, mixed-precision tiles and
+// chunk partial sums) lives in the file-scope array below, which every GPU
+// that loads libsss holds until the process exits. Host code reaches the
+// array only through the device address cudaGetSymbolAddress returns; the
+// symbol itself names a host-side stand-in.
+
+#define SSS_NOALLOC_STATUS_BYTES 256u
+#define SSS_NOALLOC_COUNTERS 16384u
+
+static __device__ __align__(256) unsigned char g_sss_noalloc_scratch[SSS_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+struct NoAllocDevice {
+    int ready;
+    unsigned char* base;  // device address of g_sss_noalloc_scratch on this device
+    int num_sms;
+    int occ[4];           // CTAs per SM of the four force kernels
+};
+
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+pthread_mutex_t g_noalloc_mu = PTHREAD_MUTEX_INITIALIZER;
+
+int noalloc_err(char* buf, size_t len, int code, const char* fmt, ...) {
+    if (buf && len) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, len, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+void* force_kernel_fn(bool mixed, int dim) {
+    if (mixed) return (dim == 3) ? (void*)k_force_mixed<3, MIX_R, MIX_NT, MIX_TS, MIX_SUB>
+                                 : (void*)k_force_mixed<2, MIX_R, MIX_NT, MIX_TS, MIX_SUB>;
+    return (dim == 3) ? (void*)k_force_f64<3, F64_R, F64_NT, F64_TS, 0>
+                      : (void*)k_force_f64<2, F64_R, F64_NT, F64_TS, 0>;
+}
+
+// Once per device, with that device current: resolve the scratch array's
+// device address and the launch parameters of the force kernels.
+int noalloc_setup(int device, NoAllocDevice** out, char* eb, size_t el) {
+    pthread_mutex_lock(&g_noalloc_mu);
+    NoAllocDevice* d = &g_noalloc_dev[device];
+    int rc = SSS_OK;
+    if (!d->ready) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_sss_noalloc_scratch);
+        if (e != cudaSuccess) {
+            rc = noalloc_err(eb, el, SSS_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        } else if (((uintptr_t)p & 255u) != 0) {
+            rc = noalloc_err(eb, el, SSS_ERR_CUDA, "static scratch is not 256-byte aligned");
+        } else {
+            d->base = (unsigned char*)p;
+            e = cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, device);
+            for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+                const bool mixed = (k & 2) != 0;
+                const int dim = (k & 1) ? 3 : 2;
+                void* fn = force_kernel_fn(mixed, dim);
+                const int nt = mixed ? MIX_NT : F64_NT;
+                const size_t smem = mixed ? 2 * MIX_TS * sizeof(float4) : 2 * F64_TS * sizeof(double4);
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                int per_sm = 0;
+                if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem);
+                d->occ[k] = per_sm < 1 ? 1 : per_sm;
+            }
+            if (e != cudaSuccess)
+                rc = noalloc_err(eb, el, SSS_ERR_CUDA, "no-alloc setup: %s", cudaGetErrorString(e));
+            else
+                d->ready = 1;
+        }
+    }
+    pthread_mutex_unlock(&g_noalloc_mu);
+    *out = d;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int sss_allpairs_accel_noalloc(int device, int dim, int precision, const double* src4, int64_t n_src,
+                                          const double* tgt4, int64_t n_tgt, double* acc4, double eps2,
+                                          int* d_status, void* stream, char* errbuf, size_t errbuf_len) {
+    char* eb = errbuf;
+    const size_t el = errbuf_len;
+    if (dim != 2 && dim != 3) return noalloc_err(eb, el, SSS_ERR_ARG, "dim must be 2 or 3 (got %d)", dim);
+    if (precision != SSS_PREC_F64 && precision != SSS_PREC_MIXED)
+        return noalloc_err(eb, el, SSS_ERR_ARG, "unknown precision %d", precision);
+    if (n_src < 0 || n_tgt < 0) return noalloc_err(eb, el, SSS_ERR_ARG, "negative size");
+    if (n_tgt == 0) return SSS_OK;
+    if (n_src < 1) return noalloc_err(eb, el, SSS_ERR_ARG, "n_src must be >= 1");
+    if (n_src > ((int64_t)1 << 40) || n_tgt > ((int64_t)1 << 40))
+        return noalloc_err(eb, el, SSS_ERR_ARG, "size out of range");
+    if (!src4 || !tgt4 || !acc4) return noalloc_err(eb, el, SSS_ERR_ARG, "NULL pointer");
+    if (!aligned16(src4) || !aligned16(tgt4) || !aligned16(acc4) || ((uintptr_t)d_status & 3u))
+        return noalloc_err(eb, el, SSS_ERR_ARG, "pointers must be 16-byte aligned (status 4-byte)");
+    if (!(eps2 >= 0.0)) return noalloc_err(eb, el, SSS_ERR_ARG, "eps2 must be >= 0");
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev || device >= kNoAllocMaxDevices)
+        return noalloc_err(eb, el, SSS_ERR_ARG, "bad device %d", device);
+    if (cudaSetDevice(device) != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "cudaSetDevice failed");
+    NoAllocDevice* d = nullptr;
+    int rc = noalloc_setup(device, &d, eb, el);
+    if (rc) return rc;
+
+    const bool mixed = (precision == SSS_PREC_MIXED);
+    const int key = (mixed ? 2 : 0) + (dim == 3 ? 1 : 0);
+    const int nt = mixed ? MIX_NT : F64_NT;
+    const int tpb = mixed ? MIX_NT * MIX_R : F64_NT * F64_R;
+    const int ts = mixed ? MIX_TS : F64_TS;
+    const size_t smem = mixed ? 2 * MIX_TS * sizeof(float4) : 2 * F64_TS * sizeof(double4);
+    Plan pl = make_plan(n_src, n_tgt, tpb, ts, d->occ[key] * d->num_sms);
+
+    // scratch layout: [status 256 B][counters 64 KiB][tiles][centres][partials]
+    const size_t data_off = SSS_NOALLOC_STATUS_BYTES + SSS_NOALLOC_COUNTERS * sizeof(unsigned);
+    const size_t avail = (size_t)SSS_NOALLOC_SCRATCH_BYTES - data_off;
+    size_t bytes_tiles = 0, bytes_cent = 0;
+    if (mixed) {
+        bytes_tiles = (size_t)pl.n_tiles * MIX_TS * sizeof(float4);
+        bytes_cent = ((size_t)pl.n_tiles * sizeof(double4) + 255) & ~(size_t)255;
+    }
+    const size_t fixed = bytes_tiles + bytes_cent;
+    if (fixed > avail)
+        return noalloc_err(eb, el, SSS_ERR_CAPACITY,
+                           "n_src = %lld needs %zu bytes of mixed-precision tiles; the no-allocation "
+                           "scratch holds %zu (at most %d sources)", (long long)n_src, fixed, avail,
+                           SSS_NOALLOC_MAX_MIXED_SOURCES);
+    // narrow the source split until its partial sums fit (1 chunk needs none)
+    if (pl.n_chunks > 1) {
+        const size_t per_chunk = (size_t)n_tgt * sizeof(double4);
+        size_t s_fit = (avail - fixed) / per_chunk;
+        if (pl.n_tblocks > (int)SSS_NOALLOC_COUNTERS) s_fit = 1;
+        if (s_fit < (size_t)pl.n_chunks) {
+            if (s_fit <= 1) {
+                pl.tiles_per_chunk = pl.n_tiles;
+                pl.n_chunks = 1;
+            } else {
+                pl.tiles_per_chunk = (int)((pl.n_tiles + s_fit - 1) / s_fit);
+                pl.n_chunks = (pl.n_tiles + pl.tiles_per_chunk - 1) / pl.tiles_per_chunk;
+            }
+        }
+    }
+    unsigned char* base = d->base;
+    cudaStream_t s = (cudaStream_t)stream;
+    int* status = d_status ? d_status : (int*)base;
+    unsigned* counters = (unsigned*)(base + SSS_NOALLOC_STATUS_BYTES);
+    unsigned char* data = base + data_off;
+
+    ForceArgs a;
+    memset(&a, 0, sizeof(a));
+    a.src = (const double4*)src4;
+    a.n_src = n_src;
+    a.tgt = (const double4*)tgt4;
+    a.n_tgt = n_tgt;
+    a.eps2 = eps2;
+    a.n_tiles = pl.n_tiles;
+    a.n_chunks = pl.n_chunks;
+    a.tiles_per_chunk = pl.tiles_per_chunk;
+    a.status = status;
+    a.epi.mode = 0;
+    a.epi.acc = (double4*)acc4;
+    if (mixed) {
+        a.srcf = (const float4*)data;
+        a.centers = (const double4*)(data + bytes_tiles);
+    }
+    if (pl.n_chunks > 1) {
+        a.part = (double4*)(data + fixed);
+        a.counters = counters;
+    }
+
+    // the array keeps the previous call's contents: zero what must start at 0
+    cudaError_t e = cudaSuccess;
+    if (!d_status) e = cudaMemsetAsync(status, 0, sizeof(int), s);
+    if (e == cudaSuccess && pl.n_chunks > 1)
+        e = cudaMemsetAsync(counters, 0, (size_t)pl.n_tblocks * sizeof(unsigned), s);
+    if (e != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+    if (mixed) {
+        if (dim == 3)
+            k_prep_mixed<3><<<pl.n_tiles, 256, 0, s>>>(a.src, n_src, (float4*)a.srcf, (double4*)a.centers);
+        else
+            k_prep_mixed<2><<<pl.n_tiles, 256, 0, s>>>(a.src, n_src, (float4*)a.srcf, (double4*)a.centers);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "k_prep_mixed: %s", cudaGetErrorString(e));
+    }
+    const unsigned grid = (unsigned)pl.n_tblocks * (unsigned)pl.n_chunks;
+    void* args[] = {&a};
+    e = cudaLaunchKernel(force_kernel_fn(mixed, dim), dim3(grid), dim3(nt), args, smem, s);
+    if (e != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "force kernel: %s", cudaGetErrorString(e));
+    return SSS_OK;
+}
