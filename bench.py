@@ -129,14 +129,14 @@ def cpu_sample(workload, seconds_target=12.0, threads=None):
     return pairs / dt, threads, desc
 
 
-def build_workload():
+def build_workload(n_side=N_SIDE, n_tracer=N_TRACER):
     from solarsystemsimulator_b200 import workloads
-    w = workloads.structure_formation(n_side=N_SIDE, n_tracer=N_TRACER)
+    w = workloads.structure_formation(n_side=n_side, n_tracer=n_tracer)
     n = len(w["pos"])
     src4 = np.zeros((n, 4))
     src4[:, :3] = w["pos"]
     src4[:, 3] = 1.0 * w["mass"]          # G = 1
-    tgt4 = np.zeros((n + N_TRACER, 4))
+    tgt4 = np.zeros((n + n_tracer, 4))
     tgt4[:n] = src4
     tgt4[n:, :3] = w["tracer_pos"]
     w["src4"], w["tgt4"] = src4, tgt4
@@ -144,8 +144,9 @@ def build_workload():
 
 
 def config_block(n_src, n_tgt):
-    return {"workload": "self-gravitating structure formation, 64^3 Zel'dovich lattice + "
-                        "524288 tracers, unit cube, eps=1e-3, Yoshida-4 dt=1e-3",
+    side = round(n_src ** (1 / 3))
+    return {"workload": f"self-gravitating structure formation, {side}^3 Zel'dovich lattice + "
+                        f"{n_tgt - n_src} tracers, unit cube, eps=1e-3, Yoshida-4 dt=1e-3",
             "n_sources": n_src, "n_targets": n_tgt, "dim": 3, "G": 1.0,
             "pairs_per_step": pairs_per_step(n_src, n_tgt),
             "l2": "L2 flushed (256 MiB write) before every timed step",
@@ -155,7 +156,7 @@ def config_block(n_src, n_tgt):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    w = build_workload()
+    w = build_workload(args.n_side, args.n_tracer)
     n_src, n_tgt = len(w["src4"]), len(w["tgt4"])
     rates = []
     cores = os.cpu_count() or 1
@@ -193,7 +194,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
 
-    w = build_workload()
+    w = build_workload(args.n_side, args.n_tracer)
     pos, mass, tpos = w["pos"], w["mass"], w["tracer_pos"]
     n_src, n_tr = len(pos), len(tpos)
     n_tgt = n_src + n_tr
@@ -398,6 +399,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--warmup-cpu", type=int, default=0)
+    ap.add_argument("--n-side", type=int, default=N_SIDE,
+                    help="sources = n_side^3 (64 is the configuration; smaller only for profiling)")
+    ap.add_argument("--n-tracer", type=int, default=N_TRACER)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

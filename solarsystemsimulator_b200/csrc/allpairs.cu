@@ -12,15 +12,21 @@
 // arrive (arrival counted by one atomic per target block, no spinning), and
 // that CTA runs the integrator epilogue: closing half kick, snapshot, next
 // opening half kick and drift (the Yoshida / KDK sequence fused into the
-// force kernel). Within a chunk each target sums its sources in ascending
-// index order, as the reference does (selfgrav_kernel.py:235-256).
+// force kernel). Within a tile each target sums its sources in ascending
+// index order, tiles in ascending order, as the reference does
+// (selfgrav_kernel.py:235-256).
 //
-// f64 path: every operation in f64; r^-3 from an f32 seed refined in f64
-// (sss_gm_rinv3_f64). Mixed path: sources are pre-shifted per tile to the
-// tile's bounding-box centre and rounded to f32; each target's offset to the
-// centre is formed in f64 and rounded once per tile, so the f32 pair
-// difference is a difference of small numbers. Pair terms are summed in f32
-// over sub-tiles of MIX_SUB sources and folded into f64 accumulators.
+// Equal-mass tiles: when every source of a tile has the same Gm, the pair
+// loop drops the mass multiply and the tile's sum is scaled by Gm once when
+// it is folded into the accumulator (detected per tile, automatically).
+//
+// f64 path: every operation in f64; r^-3 from an f32 seed refined in f64.
+// Mixed path: sources are pre-shifted per tile to the tile's bounding-box
+// centre and rounded to f32; each target's offset to the centre is formed
+// in f64 and rounded once per tile, so the f32 pair difference is a
+// difference of small numbers. f32 pair terms are summed over sub-tiles of
+// MIX_SUB sources and folded into f64 accumulators. The f32 arithmetic is
+// issued as packed f32x2 instructions (two targets per instruction).
 
 #include "sss_internal.cuh"
 
@@ -28,16 +34,24 @@
 
 namespace {
 
-constexpr int F64_NT = 256;   // threads per CTA, f64 path
-constexpr int F64_R = 4;      // targets per thread, f64 path
-constexpr int F64_TS = 512;   // sources per shared-memory tile (16 KiB)
+// f64 kernel: 2 targets per thread, 64 registers, 4 CTAs (32 warps) per SM
+constexpr int F64_NT = 256;
+constexpr int F64_R = 2;
+constexpr int F64_TS = 512;     // sources per shared-memory tile (16 KiB)
+constexpr int F64_MINB = 4;
+constexpr int F64_UNROLL = 4;
 
-constexpr int MIX_NT = 256;
-constexpr int MIX_R = 4;
-constexpr int MIX_TS = 1024;  // sources per tile (float4: 16 KiB)
-constexpr int MIX_SUB = 128;  // f32 partial-sum length before the f64 fold
+// mixed kernel: 8 targets per thread (4 packed pairs), 2 CTAs per SM
+constexpr int MIX_NT = 128;
+constexpr int MIX_R = 8;
+constexpr int MIX_TS = 512;     // sources per tile (32 B each, duplicated: 16 KiB)
+constexpr int MIX_SUB = 128;    // f32 partial-sum length before the f64 fold
+constexpr int MIX_MINB = 2;
 
-constexpr int WAVES = 16;     // target number of CTA waves per evaluation
+constexpr int WAVES = 16;       // target number of CTA waves per evaluation
+
+// r2 below this is outside the integer-seeded rsqrt's range (2^-126)
+constexpr double kIseedMinR2 = 1.1754943508222875e-38;
 
 struct Epi {
     int mode;            // 0: write accelerations only; 1: integrator step
@@ -52,8 +66,8 @@ struct Epi {
 
 struct ForceArgs {
     const double4* src;      // f64 path: sources
-    const float4* srcf;      // mixed path: tile-shifted f32 sources
-    const double4* centers;  // mixed path: tile centres
+    const float4* srcf;      // mixed path: tile-shifted, duplicated f32 sources
+    const double4* centers;  // mixed path: tile centres, .w = common Gm or NaN
     int64_t n_src;
     const double4* tgt;
     int64_t n_tgt;
@@ -110,7 +124,6 @@ __device__ __forceinline__ void epilogue(const Epi& e, int64_t i, double ax, dou
 }
 
 // Chunk partial -> (last arriving CTA) fixed-order sum -> epilogue.
-// Returns after all work of this CTA is done.
 template <int D, int R, int NT>
 __device__ __forceinline__ void finish_block(const ForceArgs& a, int tb, int ch,
                                              const double (&ax)[R], const double (&ay)[R],
@@ -169,19 +182,68 @@ __device__ __noinline__ void drain_after_abort(uint64_t* bar, int issued, int co
 
 // ------------------------------------------------------------------ f64
 
-template <int D, int VAR>
-__device__ __forceinline__ double gm_rinv3(double gm, double r2) {
-    if (VAR == 0) return sss_gm_rinv3_f64(gm, r2);
-    if (VAR == 2) return sss_gm_rinv3_f64_iseed(gm, r2);
-    return sss_gm_rinv3_cuda(gm, r2);
+// r2^(-3/2), times gm unless UNIT (the equal-mass tile loop scales later).
+template <int VAR, bool UNIT>
+__device__ __forceinline__ double rinv3(double gm, double r2) {
+    if (VAR == 1) {
+        const double inv = rsqrt(r2);
+        return UNIT ? (inv * inv) * inv : ((gm * inv) * inv) * inv;
+    }
+    double c;
+    if (VAR == 2) {
+        // seed argument by integer re-biasing of r2's high word (valid for
+        // 2^-126 <= r2 < 2^128), widened back bit by bit
+        const unsigned hi = (unsigned)__double2hiint(r2);
+        const float yf = sss_rsqrt_approx_f32(__uint_as_float((hi << 3) + 0x40000000u));
+        const unsigned yb = __float_as_uint(yf);
+        c = __hiloint2double((int)((yb >> 3) + 0x38000000u), (int)(yb << 29));
+    } else {
+        c = (double)sss_rsqrt_approx_f32(__double2float_rn(r2));
+    }
+    // c^3 (1 + 3/2 e + 15/8 e^2), e = 1 - r2 c^2 (see sss_gm_rinv3_f64)
+    const double c2 = c * c;
+    const double e = fma(-r2, c2, 1.0);
+    const double p = fma(e, 1.875, 1.5);
+    const double g3 = UNIT ? c * c2 : (gm * c) * c2;
+    return fma(g3, e * p, g3);
 }
 
-template <int D, int R, int NT, int TS, int VAR, int MINB = 2, int UNROLL = 2>
+template <int D, int R, int VAR, bool UNIT, int UNROLL>
+__device__ __forceinline__ void tile_f64(const double4* __restrict__ s, int cnt, double eps2,
+                                         const double (&px)[R], const double (&py)[R],
+                                         const double (&pz)[R], double (&tx)[R], double (&ty)[R],
+                                         double (&tz)[R]) {
+#pragma unroll UNROLL
+    for (int j = 0; j < cnt; ++j) {
+        const double4 sj = s[j];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double dx = sj.x - px[r];
+            const double dy = sj.y - py[r];
+            double r2;
+            double dz = 0.0;
+            if (D == 3) {
+                dz = sj.z - pz[r];
+                r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+            } else {
+                r2 = fma(dx, dx, fma(dy, dy, eps2));
+            }
+            const double f = rinv3<VAR, UNIT>(sj.w, r2);
+            tx[r] = fma(f, dx, tx[r]);
+            ty[r] = fma(f, dy, ty[r]);
+            if (D == 3) tz[r] = fma(f, dz, tz[r]);
+        }
+    }
+}
+
+template <int D, int R, int NT, int TS, int VAR, int MINB, int UNROLL>
 __global__ void __launch_bounds__(NT, MINB) k_force_f64(const ForceArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     double4* tiles = reinterpret_cast<double4*>(smem);
     __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_abort;
+    // chunk accumulators live in shared memory (touched once per tile), which
+    // leaves the registers to the pair loop
+    __shared__ double s_acc[3 * R][NT];
 
     const int S = a.n_chunks;
     const int tb = blockIdx.x / S;
@@ -189,13 +251,15 @@ __global__ void __launch_bounds__(NT, MINB) k_force_f64(const ForceArgs a) {
     const int tid = threadIdx.x;
     const int64_t tbase = (int64_t)tb * (NT * R);
 
-    double px[R], py[R], pz[R], ax[R], ay[R], az[R];
+    double px[R], py[R], pz[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int64_t i = tbase + r * NT + tid;
         const double4 p = (i < a.n_tgt) ? a.tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
         px[r] = p.x; py[r] = p.y; pz[r] = p.z;
-        ax[r] = 0.0; ay[r] = 0.0; az[r] = 0.0;
+        s_acc[r][tid] = 0.0;
+        s_acc[R + r][tid] = 0.0;
+        s_acc[2 * R + r][tid] = 0.0;
     }
 
     const int t_begin = ch * a.tiles_per_chunk;
@@ -203,7 +267,6 @@ __global__ void __launch_bounds__(NT, MINB) k_force_f64(const ForceArgs a) {
     const int nt = t_end - t_begin;
 
     if (tid == 0) {
-        s_abort = 0;
         sss_mbar_init(&bar[0], 1);
         sss_mbar_init(&bar[1], 1);
         sss_fence_mbar_init();
@@ -229,30 +292,24 @@ __global__ void __launch_bounds__(NT, MINB) k_force_f64(const ForceArgs a) {
     for (; k < nt; ++k) {
         const int64_t j0 = (int64_t)(t_begin + k) * TS;
         const int cnt = (int)min((int64_t)TS, a.n_src - j0);
-        if (!sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status)) s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
+        const bool waited = sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status);
+        if (__syncthreads_or(!waited)) break;
         const double4* s = tiles + (k & 1) * TS;
-#pragma unroll UNROLL
-        for (int j = 0; j < cnt; ++j) {
-            const double4 sj = s[j];
+        const double w0 = s[0].w;
+        bool same = true;
+        for (int j = tid; j < cnt; j += NT) same &= (s[j].w == w0);
+        const bool uni = __syncthreads_and(same) != 0;
+        double tx[R], ty[R], tz[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const double dx = sj.x - px[r];
-                const double dy = sj.y - py[r];
-                double r2;
-                double dz = 0.0;
-                if (D == 3) {
-                    dz = sj.z - pz[r];
-                    r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-                } else {
-                    r2 = fma(dx, dx, fma(dy, dy, eps2));
-                }
-                const double f = gm_rinv3<D, VAR>(sj.w, r2);
-                ax[r] = fma(f, dx, ax[r]);
-                ay[r] = fma(f, dy, ay[r]);
-                if (D == 3) az[r] = fma(f, dz, az[r]);
-            }
+        for (int r = 0; r < R; ++r) { tx[r] = 0.0; ty[r] = 0.0; tz[r] = 0.0; }
+        if (uni) tile_f64<D, R, VAR, true, UNROLL>(s, cnt, eps2, px, py, pz, tx, ty, tz);
+        else tile_f64<D, R, VAR, false, UNROLL>(s, cnt, eps2, px, py, pz, tx, ty, tz);
+        const double wt = uni ? w0 : 1.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            s_acc[r][tid] = fma(wt, tx[r], s_acc[r][tid]);
+            s_acc[R + r][tid] = fma(wt, ty[r], s_acc[R + r][tid]);
+            s_acc[2 * R + r][tid] = fma(wt, tz[r], s_acc[2 * R + r][tid]);
         }
         __syncthreads();
         if (tid == 0 && k + 2 < nt) { issue(k + 2); issued = k + 3; }
@@ -261,181 +318,19 @@ __global__ void __launch_bounds__(NT, MINB) k_force_f64(const ForceArgs a) {
         if (tid == 0) drain_after_abort(bar, issued, k, a.status);
         return;
     }
+    double ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        ax[r] = s_acc[r][tid];
+        ay[r] = s_acc[R + r][tid];
+        az[r] = s_acc[2 * R + r][tid];
+    }
     finish_block<D, R, NT>(a, tb, ch, ax, ay, az);
 }
 
 // ---------------------------------------------------------------- mixed
 
-// One CTA per tile of MIX_TS sources: bounding-box centre (f64) and the
-// f32 offsets of every source from it (padding entries get Gm = 0).
-template <int D>
-__global__ void __launch_bounds__(256) k_prep_mixed(const double4* __restrict__ src, int64_t n_src,
-                                                    float4* __restrict__ out,
-                                                    double4* __restrict__ centers) {
-    __shared__ double red[6][8];
-    const int tile = blockIdx.x;
-    const int64_t j0 = (int64_t)tile * MIX_TS;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int j = threadIdx.x; j < MIX_TS; j += blockDim.x) {
-        const int64_t g = j0 + j;
-        if (g < n_src) {
-            const double4 s = src[g];
-            lo[0] = fmin(lo[0], s.x); hi[0] = fmax(hi[0], s.x);
-            lo[1] = fmin(lo[1], s.y); hi[1] = fmax(hi[1], s.y);
-            lo[2] = fmin(lo[2], s.z); hi[2] = fmax(hi[2], s.z);
-        }
-    }
-    for (int c = 0; c < 3; ++c) {
-        for (int o = 16; o > 0; o >>= 1) {
-            lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
-            hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
-        }
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        for (int c = 0; c < 3; ++c) { red[c][w] = lo[c]; red[3 + c][w] = hi[c]; }
-    }
-    __syncthreads();
-    double cen[3];
-    for (int c = 0; c < 3; ++c) {
-        double a = red[c][0], b = red[3 + c][0];
-        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) { a = fmin(a, red[c][q]); b = fmax(b, red[3 + c][q]); }
-        cen[c] = (a <= b) ? 0.5 * (a + b) : 0.0;
-    }
-    if (D == 2) cen[2] = 0.0;
-    if (threadIdx.x == 0) centers[tile] = make_double4(cen[0], cen[1], cen[2], 0.0);
-    for (int j = threadIdx.x; j < MIX_TS; j += blockDim.x) {
-        const int64_t g = j0 + j;
-        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (g < n_src) {
-            const double4 s = src[g];
-            o.x = __double2float_rn(s.x - cen[0]);
-            o.y = __double2float_rn(s.y - cen[1]);
-            o.z = (D == 3) ? __double2float_rn(s.z - cen[2]) : 0.f;
-            o.w = __double2float_rn(s.w);
-        }
-        out[j0 + j] = o;
-    }
-}
-
-template <int D, int R, int NT, int TS, int SUB>
-__global__ void __launch_bounds__(NT, 2) k_force_mixed(const ForceArgs a) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    float4* tiles = reinterpret_cast<float4*>(smem);
-    __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_abort;
-
-    const int S = a.n_chunks;
-    const int tb = blockIdx.x / S;
-    const int ch = blockIdx.x - tb * S;
-    const int tid = threadIdx.x;
-    const int64_t tbase = (int64_t)tb * (NT * R);
-
-    double px[R], py[R], pz[R], ax[R], ay[R], az[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int64_t i = tbase + r * NT + tid;
-        const double4 p = (i < a.n_tgt) ? a.tgt[i] : make_double4(0.0, 0.0, 0.0, 0.0);
-        px[r] = p.x; py[r] = p.y; pz[r] = p.z;
-        ax[r] = 0.0; ay[r] = 0.0; az[r] = 0.0;
-    }
-
-    const int t_begin = ch * a.tiles_per_chunk;
-    const int t_end = min(t_begin + a.tiles_per_chunk, a.n_tiles);
-    const int nt = t_end - t_begin;
-
-    if (tid == 0) {
-        s_abort = 0;
-        sss_mbar_init(&bar[0], 1);
-        sss_mbar_init(&bar[1], 1);
-        sss_fence_mbar_init();
-    }
-    __syncthreads();
-
-    int issued = 0;
-    constexpr unsigned kTileBytes = TS * sizeof(float4);
-    auto issue = [&](int k) {
-        sss_mbar_arrive_expect_tx(&bar[k & 1], kTileBytes);
-        sss_bulk_g2s(tiles + (k & 1) * TS, a.srcf + (int64_t)(t_begin + k) * TS, kTileBytes, &bar[k & 1]);
-    };
-    if (tid == 0) {
-        issue(0);
-        issued = 1;
-        if (nt > 1) { issue(1); issued = 2; }
-    }
-
-    const float eps2f = (float)a.eps2;
-    int k = 0;
-    for (; k < nt; ++k) {
-        const int tile = t_begin + k;
-        const int64_t j0 = (int64_t)tile * TS;
-        const int cnt = (int)min((int64_t)TS, a.n_src - j0);
-        const double4 c = a.centers[tile];
-        float ox[R], oy[R], oz[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            ox[r] = __double2float_rn(c.x - px[r]);
-            oy[r] = __double2float_rn(c.y - py[r]);
-            oz[r] = (D == 3) ? __double2float_rn(c.z - pz[r]) : 0.f;
-        }
-        if (!sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status)) s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
-        const float4* s = tiles + (k & 1) * TS;
-        for (int js = 0; js < cnt; js += SUB) {
-            const int je = min(js + SUB, cnt);
-            float fx[R], fy[R], fz[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) { fx[r] = 0.f; fy[r] = 0.f; fz[r] = 0.f; }
-#pragma unroll 4
-            for (int j = js; j < je; ++j) {
-                const float4 sj = s[j];
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const float dx = sj.x + ox[r];
-                    const float dy = sj.y + oy[r];
-                    float r2, dz = 0.f;
-                    if (D == 3) {
-                        dz = sj.z + oz[r];
-                        r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2f)));
-                    } else {
-                        r2 = fmaf(dx, dx, fmaf(dy, dy, eps2f));
-                    }
-                    const float inv = sss_rsqrt_approx_f32(r2);
-                    const float inv2 = inv * inv;
-                    const float f = (sj.w * inv) * inv2;
-                    fx[r] = fmaf(f, dx, fx[r]);
-                    fy[r] = fmaf(f, dy, fy[r]);
-                    if (D == 3) fz[r] = fmaf(f, dz, fz[r]);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                ax[r] += (double)fx[r];
-                ay[r] += (double)fy[r];
-                if (D == 3) az[r] += (double)fz[r];
-            }
-        }
-        __syncthreads();
-        if (tid == 0 && k + 2 < nt) { issue(k + 2); issued = k + 3; }
-    }
-    if (k < nt) {
-        if (tid == 0) drain_after_abort(bar, issued, k, a.status);
-        return;
-    }
-    finish_block<D, R, NT>(a, tb, ch, ax, ay, az);
-}
-
-// -------------------------------------------------------- mixed, packed
-//
-// Same arithmetic as k_force_mixed, issued as packed f32x2 instructions
-// (sm_100a add/mul/fma .f32x2): two targets of a thread share one
-// instruction. The FP32 lanes do the same work; the packed form halves the
-// issue slots per pair, which is what bounds the scalar loop. Tiles hold
-// each source duplicated, {x,x,y,y},{z,z,Gm,Gm}, so one shared-memory load
-// yields the packed operands directly.
-
-typedef unsigned long long f2x;
+typedef unsigned long long f2x;   // two packed f32
 
 __device__ __forceinline__ f2x pk2(float lo, float hi) {
     f2x r;
@@ -461,19 +356,22 @@ __device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
     return d;
 }
 
-constexpr int MX2_NT = 256;
-constexpr int MX2_R = 4;      // targets per thread (2 packed pairs)
-constexpr int MX2_TS = 512;   // sources per tile (32 B each: 16 KiB)
-constexpr int MX2_SUB = 128;
-
+// One CTA per tile of TS sources: bounding-box centre (f64), common Gm of
+// the tile (NaN if the masses differ), and every source's f32 offset from
+// the centre, duplicated {x,x,y,y},{z,z,Gm,Gm} for the packed loop
+// (padding entries get Gm = 0).
 template <int D, int TS>
-__global__ void __launch_bounds__(256) k_prep_mixed2(const double4* __restrict__ src, int64_t n_src,
-                                                     float4* __restrict__ out,
-                                                     double4* __restrict__ centers) {
+__global__ void __launch_bounds__(256) k_prep_mixed(const double4* __restrict__ src, int64_t n_src,
+                                                    float4* __restrict__ out,
+                                                    double4* __restrict__ centers) {
     __shared__ double red[6][8];
+    __shared__ int s_diff;
     const int tile = blockIdx.x;
     const int64_t j0 = (int64_t)tile * TS;
+    if (threadIdx.x == 0) s_diff = 0;
+    const double w0 = src[j0].w;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    bool diff = false;
     for (int j = threadIdx.x; j < TS; j += blockDim.x) {
         const int64_t g = j0 + j;
         if (g < n_src) {
@@ -481,6 +379,7 @@ __global__ void __launch_bounds__(256) k_prep_mixed2(const double4* __restrict__
             lo[0] = fmin(lo[0], s.x); hi[0] = fmax(hi[0], s.x);
             lo[1] = fmin(lo[1], s.y); hi[1] = fmax(hi[1], s.y);
             lo[2] = fmin(lo[2], s.z); hi[2] = fmax(hi[2], s.z);
+            diff |= (s.w != w0);
         }
     }
     for (int c = 0; c < 3; ++c) {
@@ -490,6 +389,8 @@ __global__ void __launch_bounds__(256) k_prep_mixed2(const double4* __restrict__
         }
     }
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (diff) s_diff = 1;
     if (l == 0) {
         for (int c = 0; c < 3; ++c) { red[c][w] = lo[c]; red[3 + c][w] = hi[c]; }
     }
@@ -501,7 +402,8 @@ __global__ void __launch_bounds__(256) k_prep_mixed2(const double4* __restrict__
         cen[c] = (a <= b) ? 0.5 * (a + b) : 0.0;
     }
     if (D == 2) cen[2] = 0.0;
-    if (threadIdx.x == 0) centers[tile] = make_double4(cen[0], cen[1], cen[2], 0.0);
+    if (threadIdx.x == 0)
+        centers[tile] = make_double4(cen[0], cen[1], cen[2], s_diff ? __longlong_as_double(0x7ff8000000000000ll) : w0);
     for (int j = threadIdx.x; j < TS; j += blockDim.x) {
         const int64_t g = j0 + j;
         float x = 0.f, y = 0.f, z = 0.f, m = 0.f;
@@ -517,14 +419,44 @@ __global__ void __launch_bounds__(256) k_prep_mixed2(const double4* __restrict__
     }
 }
 
-template <int D, int R, int NT, int TS, int SUB, int MINB = 2>
-__global__ void __launch_bounds__(NT, MINB) k_force_mixed2(const ForceArgs a) {
+template <int D, int P, bool UNIT>
+__device__ __forceinline__ void subtile_mixed(const ulonglong2* __restrict__ s, int js, int je, f2x eps2x,
+                                              const f2x (&ox)[P], const f2x (&oy)[P], const f2x (&oz)[P],
+                                              f2x (&fx)[P], f2x (&fy)[P], f2x (&fz)[P]) {
+#pragma unroll 4
+    for (int j = js; j < je; ++j) {
+        const ulonglong2 xy = s[2 * j];
+        const ulonglong2 zw = s[2 * j + 1];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const f2x dx = add2(xy.x, ox[q]);
+            const f2x dy = add2(xy.y, oy[q]);
+            f2x r2;
+            f2x dz = 0ull;
+            if (D == 3) {
+                dz = add2(zw.x, oz[q]);
+                r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, eps2x)));
+            } else {
+                r2 = fma2(dx, dx, fma2(dy, dy, eps2x));
+            }
+            float r0, r1;
+            upk2(r2, r0, r1);
+            const f2x inv = pk2(sss_rsqrt_approx_f32(r0), sss_rsqrt_approx_f32(r1));
+            const f2x f = UNIT ? mul2(inv, mul2(inv, inv)) : mul2(mul2(zw.y, inv), mul2(inv, inv));
+            fx[q] = fma2(f, dx, fx[q]);
+            fy[q] = fma2(f, dy, fy[q]);
+            if (D == 3) fz[q] = fma2(f, dz, fz[q]);
+        }
+    }
+}
+
+template <int D, int R, int NT, int TS, int SUB, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_force_mixed(const ForceArgs a) {
     static_assert(R % 2 == 0, "packed kernel needs an even target count");
     constexpr int P = R / 2;
     extern __shared__ __align__(128) unsigned char smem[];
     ulonglong2* tiles = reinterpret_cast<ulonglong2*>(smem);   // [2][TS][2]
     __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int s_abort;
 
     const int S = a.n_chunks;
     const int tb = blockIdx.x / S;
@@ -546,7 +478,6 @@ __global__ void __launch_bounds__(NT, MINB) k_force_mixed2(const ForceArgs a) {
     const int nt = t_end - t_begin;
 
     if (tid == 0) {
-        s_abort = 0;
         sss_mbar_init(&bar[0], 1);
         sss_mbar_init(&bar[1], 1);
         sss_fence_mbar_init();
@@ -574,6 +505,7 @@ __global__ void __launch_bounds__(NT, MINB) k_force_mixed2(const ForceArgs a) {
         const int64_t j0 = (int64_t)tile * TS;
         const int cnt = (int)min((int64_t)TS, a.n_src - j0);
         const double4 c = a.centers[tile];
+        const bool uni = (c.w == c.w);   // the tile's common Gm, NaN if masses differ
         f2x ox[P], oy[P], oz[P];
 #pragma unroll
         for (int q = 0; q < P; ++q) {
@@ -582,46 +514,31 @@ __global__ void __launch_bounds__(NT, MINB) k_force_mixed2(const ForceArgs a) {
             oz[q] = (D == 3) ? pk2(__double2float_rn(c.z - pz[2 * q]), __double2float_rn(c.z - pz[2 * q + 1]))
                              : pk2(0.f, 0.f);
         }
-        if (!sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status)) s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
+        const bool waited = sss_mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1, a.status);
+        if (__syncthreads_or(!waited)) break;
         const ulonglong2* s = tiles + (k & 1) * TS * 2;
+        const double wt = uni ? c.w : 1.0;
         for (int js = 0; js < cnt; js += SUB) {
             const int je = min(js + SUB, cnt);
             f2x fx[P], fy[P], fz[P];
 #pragma unroll
             for (int q = 0; q < P; ++q) { fx[q] = 0ull; fy[q] = 0ull; fz[q] = 0ull; }
-#pragma unroll 4
-            for (int j = js; j < je; ++j) {
-                const ulonglong2 xy = s[2 * j];
-                const ulonglong2 zw = s[2 * j + 1];
-#pragma unroll
-                for (int q = 0; q < P; ++q) {
-                    const f2x dx = add2(xy.x, ox[q]);
-                    const f2x dy = add2(xy.y, oy[q]);
-                    f2x r2;
-                    f2x dz = 0ull;
-                    if (D == 3) {
-                        dz = add2(zw.x, oz[q]);
-                        r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, eps2x)));
-                    } else {
-                        r2 = fma2(dx, dx, fma2(dy, dy, eps2x));
-                    }
-                    float r0, r1;
-                    upk2(r2, r0, r1);
-                    const f2x inv = pk2(sss_rsqrt_approx_f32(r0), sss_rsqrt_approx_f32(r1));
-                    const f2x f = mul2(mul2(zw.y, inv), mul2(inv, inv));
-                    fx[q] = fma2(f, dx, fx[q]);
-                    fy[q] = fma2(f, dy, fy[q]);
-                    if (D == 3) fz[q] = fma2(f, dz, fz[q]);
-                }
-            }
+            if (uni) subtile_mixed<D, P, true>(s, js, je, eps2x, ox, oy, oz, fx, fy, fz);
+            else subtile_mixed<D, P, false>(s, js, je, eps2x, ox, oy, oz, fx, fy, fz);
 #pragma unroll
             for (int q = 0; q < P; ++q) {
                 float l0, l1;
-                upk2(fx[q], l0, l1); ax[2 * q] += (double)l0; ax[2 * q + 1] += (double)l1;
-                upk2(fy[q], l0, l1); ay[2 * q] += (double)l0; ay[2 * q + 1] += (double)l1;
-                if (D == 3) { upk2(fz[q], l0, l1); az[2 * q] += (double)l0; az[2 * q + 1] += (double)l1; }
+                upk2(fx[q], l0, l1);
+                ax[2 * q] = fma(wt, (double)l0, ax[2 * q]);
+                ax[2 * q + 1] = fma(wt, (double)l1, ax[2 * q + 1]);
+                upk2(fy[q], l0, l1);
+                ay[2 * q] = fma(wt, (double)l0, ay[2 * q]);
+                ay[2 * q + 1] = fma(wt, (double)l1, ay[2 * q + 1]);
+                if (D == 3) {
+                    upk2(fz[q], l0, l1);
+                    az[2 * q] = fma(wt, (double)l0, az[2 * q]);
+                    az[2 * q + 1] = fma(wt, (double)l1, az[2 * q + 1]);
+                }
             }
         }
         __syncthreads();
@@ -705,17 +622,81 @@ Plan make_plan(int64_t n_src, int64_t n_tgt, int targets_per_block, int ts, int 
     return p;
 }
 
+// The force kernel a launch uses and its launch shape.
+struct KSel {
+    void* fn;
+    int nt, tpb, ts;
+    size_t smem;       // dynamic shared memory
+    int key;           // index of its cached occupancy (0..5)
+    bool mixed;
+};
+
+KSel select_kernel(int dim, int precision, double eps2) {
+    KSel k;
+    k.mixed = (precision == SSS_PREC_MIXED);
+    if (k.mixed) {
+        k.fn = (dim == 3) ? (void*)k_force_mixed<3, MIX_R, MIX_NT, MIX_TS, MIX_SUB, MIX_MINB>
+                          : (void*)k_force_mixed<2, MIX_R, MIX_NT, MIX_TS, MIX_SUB, MIX_MINB>;
+        k.nt = MIX_NT;
+        k.tpb = MIX_NT * MIX_R;
+        k.ts = MIX_TS;
+        k.smem = 2 * (size_t)MIX_TS * 2 * sizeof(float4);
+        k.key = 4 + (dim == 3);
+        return k;
+    }
+    // the integer-seeded series needs r2 >= 2^-126; smaller softening takes CUDA's rsqrt
+    const bool iseed = eps2 >= kIseedMinR2;
+    if (iseed)
+        k.fn = (dim == 3) ? (void*)k_force_f64<3, F64_R, F64_NT, F64_TS, 2, F64_MINB, F64_UNROLL>
+                          : (void*)k_force_f64<2, F64_R, F64_NT, F64_TS, 2, F64_MINB, F64_UNROLL>;
+    else
+        k.fn = (dim == 3) ? (void*)k_force_f64<3, F64_R, F64_NT, F64_TS, 1, F64_MINB, F64_UNROLL>
+                          : (void*)k_force_f64<2, F64_R, F64_NT, F64_TS, 1, F64_MINB, F64_UNROLL>;
+    k.nt = F64_NT;
+    k.tpb = F64_NT * F64_R;
+    k.ts = F64_TS;
+    k.smem = 2 * (size_t)F64_TS * sizeof(double4);
+    k.key = (iseed ? 0 : 2) + (dim == 3);
+    return k;
+}
+
+// Bytes of mixed-precision tile copies and tile centres for n_tiles tiles.
+size_t mixed_tile_bytes(int n_tiles) { return (size_t)n_tiles * MIX_TS * 2 * sizeof(float4); }
+size_t mixed_centre_bytes(int n_tiles) { return ((size_t)n_tiles * sizeof(double4) + 255) & ~(size_t)255; }
+
+cudaError_t launch_prep(int dim, const double4* src, int64_t n_src, int n_tiles, float4* tiles,
+                        double4* centres, cudaStream_t s) {
+    if (dim == 3) k_prep_mixed<3, MIX_TS><<<n_tiles, 256, 0, s>>>(src, n_src, tiles, centres);
+    else k_prep_mixed<2, MIX_TS><<<n_tiles, 256, 0, s>>>(src, n_src, tiles, centres);
+    return cudaGetLastError();
+}
+
+// CTAs per SM of a force kernel (sets its shared-memory attribute first).
+cudaError_t query_occupancy(const KSel& k, int* per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k.fn, k.nt, k.smem);
+    *per_sm = n < 1 ? 1 : n;
+    return e;
+}
+
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 int force_eval(sss_ctx* ctx, int dim, int precision, const double4* src, int64_t n_src,
                const double4* tgt, int64_t n_tgt, double eps2, const Epi& epi, cudaStream_t stream) {
     if (n_tgt <= 0) return SSS_OK;
-    if (n_src <= 0) {
-        // no sources: zero accelerations, the epilogue still integrates
-        return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: n_src must be >= 1");
-    }
+    if (n_src <= 0) return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: n_src must be >= 1");
     if (n_src > ((int64_t)1 << 40) || n_tgt > ((int64_t)1 << 40))
         return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: size out of range");
+    const KSel ks = select_kernel(dim, precision, eps2);
+    if (ctx->occ[ks.key] == 0) {
+        int per_sm = 0;
+        SSS_CUDA_TRY(ctx, query_occupancy(ks, &per_sm));
+        ctx->occ[ks.key] = per_sm;
+    }
+    const Plan pl = make_plan(n_src, n_tgt, ks.tpb, ks.ts, ctx->occ[ks.key] * ctx->num_sms);
+
     ForceArgs a;
     memset(&a, 0, sizeof(a));
     a.src = src;
@@ -725,68 +706,36 @@ int force_eval(sss_ctx* ctx, int dim, int precision, const double4* src, int64_t
     a.eps2 = eps2;
     a.status = ctx->d_status;
     a.epi = epi;
-
-    const bool mixed = (precision == SSS_PREC_MIXED);
-    const int nt = mixed ? MIX_NT : F64_NT;
-    const int tpb = mixed ? MIX_NT * MIX_R : F64_NT * F64_R;
-    const int ts = mixed ? MIX_TS : F64_TS;
-    const size_t smem = mixed ? 2 * MIX_TS * sizeof(float4) : 2 * F64_TS * sizeof(double4);
-
-    void* kfn;
-    if (mixed) kfn = (dim == 3) ? (void*)k_force_mixed<3, MIX_R, MIX_NT, MIX_TS, MIX_SUB>
-                                : (void*)k_force_mixed<2, MIX_R, MIX_NT, MIX_TS, MIX_SUB>;
-    else kfn = (dim == 3) ? (void*)k_force_f64<3, F64_R, F64_NT, F64_TS, 0>
-                          : (void*)k_force_f64<2, F64_R, F64_NT, F64_TS, 0>;
-    const int key = (mixed ? 2 : 0) + (dim == 3 ? 1 : 0);
-    if (ctx->occ[key] == 0) {
-        SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, smem) != cudaSuccess || per_sm < 1)
-            per_sm = 1;
-        ctx->occ[key] = per_sm;
-    }
-    const int per_sm = ctx->occ[key];
-    const Plan pl = make_plan(n_src, n_tgt, tpb, ts, per_sm * ctx->num_sms);
     a.n_tiles = pl.n_tiles;
     a.n_chunks = pl.n_chunks;
     a.tiles_per_chunk = pl.tiles_per_chunk;
 
     // scratch: [mixed tiles][centres][partials]
-    size_t off = 0;
-    size_t bytes_tiles = 0, bytes_cent = 0, bytes_part = 0;
-    if (mixed) {
-        bytes_tiles = (size_t)pl.n_tiles * MIX_TS * sizeof(float4);
-        bytes_cent = ((size_t)pl.n_tiles * sizeof(double4) + 255) & ~(size_t)255;
-    }
-    if (pl.n_chunks > 1) bytes_part = (size_t)pl.n_chunks * (size_t)n_tgt * sizeof(double4);
+    const size_t bytes_tiles = ks.mixed ? mixed_tile_bytes(pl.n_tiles) : 0;
+    const size_t bytes_cent = ks.mixed ? mixed_centre_bytes(pl.n_tiles) : 0;
+    const size_t bytes_part = pl.n_chunks > 1 ? (size_t)pl.n_chunks * (size_t)n_tgt * sizeof(double4) : 0;
     void* scr = nullptr;
     const size_t total = bytes_tiles + bytes_cent + bytes_part;
     if (total > 0) {
         int rc = sss_scratch(ctx, total, &scr);
         if (rc) return rc;
     }
-    if (mixed) {
-        a.srcf = (const float4*)((char*)scr + off);
-        off += bytes_tiles;
-        a.centers = (const double4*)((char*)scr + off);
-        off += bytes_cent;
+    if (ks.mixed) {
+        a.srcf = (const float4*)scr;
+        a.centers = (const double4*)((char*)scr + bytes_tiles);
     }
-    if (pl.n_chunks > 1) a.part = (double4*)((char*)scr + off);
     if (pl.n_chunks > 1) {
+        a.part = (double4*)((char*)scr + bytes_tiles + bytes_cent);
         int rc = sss_counters(ctx, (size_t)pl.n_tblocks, &a.counters);
         if (rc) return rc;
     }
-
-    if (mixed) {
-        if (dim == 3)
-            k_prep_mixed<3><<<pl.n_tiles, 256, 0, stream>>>(src, n_src, (float4*)a.srcf, (double4*)a.centers);
-        else
-            k_prep_mixed<2><<<pl.n_tiles, 256, 0, stream>>>(src, n_src, (float4*)a.srcf, (double4*)a.centers);
-        SSS_LAUNCH_CHECK(ctx, "k_prep_mixed launch");
+    if (ks.mixed) {
+        cudaError_t e = launch_prep(dim, src, n_src, pl.n_tiles, (float4*)a.srcf, (double4*)a.centers, stream);
+        if (e != cudaSuccess) return sss_cuda_err(ctx, e, "k_prep_mixed launch");
     }
     const unsigned grid = (unsigned)pl.n_tblocks * (unsigned)pl.n_chunks;
     void* args[] = {&a};
-    SSS_CUDA_TRY(ctx, cudaLaunchKernel(kfn, dim3(grid), dim3(nt), args, smem, stream));
+    SSS_CUDA_TRY(ctx, cudaLaunchKernel(ks.fn, dim3(grid), dim3(ks.nt), args, ks.smem, stream));
     return SSS_OK;
 }
 
@@ -954,7 +903,7 @@ struct NoAllocDevice {
     int ready;
     unsigned char* base;  // device address of g_sss_noalloc_scratch on this device
     int num_sms;
-    int occ[4];           // CTAs per SM of the four force kernels
+    int occ[6];           // CTAs per SM of the force kernels (KSel::key)
 };
 
 constexpr int kNoAllocMaxDevices = 64;
@@ -969,13 +918,6 @@ int noalloc_err(char* buf, size_t len, int code, const char* fmt, ...) {
         va_end(ap);
     }
     return code;
-}
-
-void* force_kernel_fn(bool mixed, int dim) {
-    if (mixed) return (dim == 3) ? (void*)k_force_mixed<3, MIX_R, MIX_NT, MIX_TS, MIX_SUB>
-                                 : (void*)k_force_mixed<2, MIX_R, MIX_NT, MIX_TS, MIX_SUB>;
-    return (dim == 3) ? (void*)k_force_f64<3, F64_R, F64_NT, F64_TS, 0>
-                      : (void*)k_force_f64<2, F64_R, F64_NT, F64_TS, 0>;
 }
 
 // Once per device, with that device current: resolve the scratch array's
@@ -994,17 +936,14 @@ int noalloc_setup(int device, NoAllocDevice** out, char* eb, size_t el) {
         } else {
             d->base = (unsigned char*)p;
             e = cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, device);
-            for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
-                const bool mixed = (k & 2) != 0;
-                const int dim = (k & 1) ? 3 : 2;
-                void* fn = force_kernel_fn(mixed, dim);
-                const int nt = mixed ? MIX_NT : F64_NT;
-                const size_t smem = mixed ? 2 * MIX_TS * sizeof(float4) : 2 * F64_TS * sizeof(double4);
-                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                int per_sm = 0;
-                if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem);
-                d->occ[k] = per_sm < 1 ? 1 : per_sm;
-            }
+            // one representative eps2 per f64 seed variant selects each kernel once
+            const double probe_eps2[2] = {1.0, 0.0};
+            for (int prec = 0; prec < 2 && e == cudaSuccess; ++prec)
+                for (int dim = 2; dim <= 3 && e == cudaSuccess; ++dim)
+                    for (int v = 0; v < (prec ? 1 : 2) && e == cudaSuccess; ++v) {
+                        const KSel ks = select_kernel(dim, prec, probe_eps2[v]);
+                        e = query_occupancy(ks, &d->occ[ks.key]);
+                    }
             if (e != cudaSuccess)
                 rc = noalloc_err(eb, el, SSS_ERR_CUDA, "no-alloc setup: %s", cudaGetErrorString(e));
             else
@@ -1043,22 +982,14 @@ extern "C" int sss_allpairs_accel_noalloc(int device, int dim, int precision, co
     int rc = noalloc_setup(device, &d, eb, el);
     if (rc) return rc;
 
-    const bool mixed = (precision == SSS_PREC_MIXED);
-    const int key = (mixed ? 2 : 0) + (dim == 3 ? 1 : 0);
-    const int nt = mixed ? MIX_NT : F64_NT;
-    const int tpb = mixed ? MIX_NT * MIX_R : F64_NT * F64_R;
-    const int ts = mixed ? MIX_TS : F64_TS;
-    const size_t smem = mixed ? 2 * MIX_TS * sizeof(float4) : 2 * F64_TS * sizeof(double4);
-    Plan pl = make_plan(n_src, n_tgt, tpb, ts, d->occ[key] * d->num_sms);
+    const KSel ks = select_kernel(dim, precision, eps2);
+    Plan pl = make_plan(n_src, n_tgt, ks.tpb, ks.ts, d->occ[ks.key] * d->num_sms);
 
     // scratch layout: [status 256 B][counters 64 KiB][tiles][centres][partials]
     const size_t data_off = SSS_NOALLOC_STATUS_BYTES + SSS_NOALLOC_COUNTERS * sizeof(unsigned);
     const size_t avail = (size_t)SSS_NOALLOC_SCRATCH_BYTES - data_off;
-    size_t bytes_tiles = 0, bytes_cent = 0;
-    if (mixed) {
-        bytes_tiles = (size_t)pl.n_tiles * MIX_TS * sizeof(float4);
-        bytes_cent = ((size_t)pl.n_tiles * sizeof(double4) + 255) & ~(size_t)255;
-    }
+    const size_t bytes_tiles = ks.mixed ? mixed_tile_bytes(pl.n_tiles) : 0;
+    const size_t bytes_cent = ks.mixed ? mixed_centre_bytes(pl.n_tiles) : 0;
     const size_t fixed = bytes_tiles + bytes_cent;
     if (fixed > avail)
         return noalloc_err(eb, el, SSS_ERR_CAPACITY,
@@ -1099,7 +1030,7 @@ extern "C" int sss_allpairs_accel_noalloc(int device, int dim, int precision, co
     a.status = status;
     a.epi.mode = 0;
     a.epi.acc = (double4*)acc4;
-    if (mixed) {
+    if (ks.mixed) {
         a.srcf = (const float4*)data;
         a.centers = (const double4*)(data + bytes_tiles);
     }
@@ -1114,17 +1045,13 @@ extern "C" int sss_allpairs_accel_noalloc(int device, int dim, int precision, co
     if (e == cudaSuccess && pl.n_chunks > 1)
         e = cudaMemsetAsync(counters, 0, (size_t)pl.n_tblocks * sizeof(unsigned), s);
     if (e != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
-    if (mixed) {
-        if (dim == 3)
-            k_prep_mixed<3><<<pl.n_tiles, 256, 0, s>>>(a.src, n_src, (float4*)a.srcf, (double4*)a.centers);
-        else
-            k_prep_mixed<2><<<pl.n_tiles, 256, 0, s>>>(a.src, n_src, (float4*)a.srcf, (double4*)a.centers);
-        e = cudaGetLastError();
+    if (ks.mixed) {
+        e = launch_prep(dim, a.src, n_src, pl.n_tiles, (float4*)a.srcf, (double4*)a.centers, s);
         if (e != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "k_prep_mixed: %s", cudaGetErrorString(e));
     }
     const unsigned grid = (unsigned)pl.n_tblocks * (unsigned)pl.n_chunks;
     void* args[] = {&a};
-    e = cudaLaunchKernel(force_kernel_fn(mixed, dim), dim3(grid), dim3(nt), args, smem, s);
+    e = cudaLaunchKernel(ks.fn, dim3(grid), dim3(ks.nt), args, ks.smem, s);
     if (e != cudaSuccess) return noalloc_err(eb, el, SSS_ERR_CUDA, "force kernel: %s", cudaGetErrorString(e));
     return SSS_OK;
 }

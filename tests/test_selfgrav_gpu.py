@@ -74,6 +74,28 @@ def test_f64_accel_parity_with_oracle(dim, n_src, n_tgt):
     assert np.all(a[:, 3] == 0.0)
 
 
+@pytest.mark.parametrize("precision,tol", [("f64", None), ("mixed", 1e-5)])
+def test_equal_mass_tiles_and_mixed_tiles(precision, tol):
+    # equal-mass tiles take the mass-factored loop, others the general loop
+    sg = _sg()
+    rng = np.random.default_rng(21)
+    n = 9000
+    src = np.zeros((n, 4))
+    src[:, :3] = rng.uniform(-0.5, 0.5, (n, 3))
+    src[:, 3] = 1.0 / n
+    src[600:700, 3] *= rng.uniform(0.5, 2.0, 100)      # tile 1 (f64) / tile 1 (mixed)
+    src[5000, 3] = 3.0 / n                               # one odd mass in a later tile
+    ref = osg.accel(src, src, 1e-4, dim=3)
+    t = torch.from_numpy(src).cuda()
+    a = sg.allpairs_accel(t, t, 1e-4, dim=3, precision=precision).cpu().numpy()
+    if tol is None:
+        ok, worst = parity_ok(a, ref, 3)
+        assert ok, worst
+    else:
+        rel = np.linalg.norm(a[:, :3] - ref[:, :3], axis=1) / np.linalg.norm(ref[:, :3], axis=1)
+        assert np.median(rel) <= tol
+
+
 def test_f64_accel_is_deterministic():
     sg = _sg()
     src = torch.from_numpy(cloud(30000, 3, 5)).cuda()
