@@ -163,7 +163,7 @@ int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st,
  * an internal word). errbuf/errbuf_len: optional host buffer for a message.
  * No reference counterpart. */
 #define SSS_NOALLOC_SCRATCH_BYTES     (32u << 20)
-#define SSS_NOALLOC_MAX_MIXED_SOURCES 2088960
+#define SSS_NOALLOC_MAX_MIXED_SOURCES 1044480
 int sss_allpairs_accel_noalloc(int device, int dim, int precision,
                                const double* src4, int64_t n_src,
                                const double* tgt4, int64_t n_tgt,

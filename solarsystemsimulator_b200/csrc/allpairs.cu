@@ -183,6 +183,12 @@ __device__ __noinline__ void drain_after_abort(uint64_t* bar, int issued, int co
 // ------------------------------------------------------------------ f64
 
 // r2^(-3/2), times gm unless UNIT (the equal-mass tile loop scales later).
+//   VAR 1: CUDA's rsqrt(double) and three multiplies
+//   VAR 0: series refinement of an f32 seed formed by f64->f32 conversion
+//   VAR 2: the same with the seed argument formed by integer operations
+// (Measured on the benchmark shape: VAR 2 199.7 ms, VAR 0 198.8-202.6 ms,
+// VAR 1 245.6 ms per evaluation; evaluating the e^2 term in f32 to save one
+// f64 operation was slower, 215 ms, because of its two conversions.)
 template <int VAR, bool UNIT>
 __device__ __forceinline__ double rinv3(double gm, double r2) {
     if (VAR == 1) {
@@ -203,8 +209,8 @@ __device__ __forceinline__ double rinv3(double gm, double r2) {
     // c^3 (1 + 3/2 e + 15/8 e^2), e = 1 - r2 c^2 (see sss_gm_rinv3_f64)
     const double c2 = c * c;
     const double e = fma(-r2, c2, 1.0);
-    const double p = fma(e, 1.875, 1.5);
     const double g3 = UNIT ? c * c2 : (gm * c) * c2;
+    const double p = fma(e, 1.875, 1.5);
     return fma(g3, e * p, g3);
 }
 
@@ -896,6 +902,18 @@ extern "C" int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st, int
 #define SSS_NOALLOC_COUNTERS 16384u
 
 static __device__ __align__(256) unsigned char g_sss_noalloc_scratch[SSS_NOALLOC_SCRATCH_BYTES];
+
+// The stated mixed-precision source limit must be exactly what the scratch
+// layout holds: whole tiles plus their 256-byte-rounded centres.
+constexpr size_t noalloc_fixed_bytes(size_t n_src) {
+    return ((n_src + MIX_TS - 1) / MIX_TS) * MIX_TS * 2 * sizeof(float4) +
+           ((((n_src + MIX_TS - 1) / MIX_TS) * sizeof(double4) + 255) & ~(size_t)255);
+}
+constexpr size_t kNoAllocAvail =
+    (size_t)SSS_NOALLOC_SCRATCH_BYTES - SSS_NOALLOC_STATUS_BYTES - SSS_NOALLOC_COUNTERS * sizeof(unsigned);
+static_assert(noalloc_fixed_bytes(SSS_NOALLOC_MAX_MIXED_SOURCES) <= kNoAllocAvail &&
+                  noalloc_fixed_bytes(SSS_NOALLOC_MAX_MIXED_SOURCES + 1) > kNoAllocAvail,
+              "SSS_NOALLOC_MAX_MIXED_SOURCES does not match the no-allocation scratch layout");
 
 namespace {
 

@@ -74,7 +74,7 @@ def test_noalloc_matches_context_entry_point(precision, dim, n_src, n_tgt):
 def test_noalloc_rejects_sizes_beyond_maximum():
     from solarsystemsimulator_b200 import _lib
     lib = _lib.load()
-    n_max = 2088960   # SSS_NOALLOC_MAX_MIXED_SOURCES
+    n_max = 1044480   # SSS_NOALLOC_MAX_MIXED_SOURCES
     src = torch.zeros((n_max + 1, 4), dtype=torch.float64, device="cuda")
     tgt = torch.zeros((4, 4), dtype=torch.float64, device="cuda")
     out = torch.zeros((4, 4), dtype=torch.float64, device="cuda")
