@@ -131,6 +131,65 @@ int sss_selfgrav_step_batch(sss_ctx* ctx, sss_selfgrav_state* st,
                             int integrator, double dt, int steps,
                             float* snap, void* stream);
 
+/* ------------------------------------------ few massive + many asteroids
+ *
+ * Replaces `frame_kernel` and the device side of NBodyCuda
+ * (nbody_kernel.py:97-560, 617-1060): massive bodies (M <= SSS_M_MAX) act on
+ * each other and on the asteroids, asteroids act back on the massive bodies,
+ * asteroid x asteroid is ignored; 4th-order Yoshida with hierarchical
+ * substeps and a private adaptive loop for close-encounter ("hot")
+ * asteroids. All arrays are caller-owned device buffers: per dimension c the
+ * asteroid arrays have n_ast entries and the massive arrays M entries
+ * (dimension 2 needs only the first two pointers of each triple). */
+#define SSS_M_MAX            64   /* nbody_kernel.py:58 */
+#define SSS_K_MAX            16   /* nbody_kernel.py:59 */
+#define SSS_SUB_SAMPLES_MAX  32   /* nbody_kernel.py:71 */
+
+typedef struct sss_frame_state {
+    int      dim;                 /* 2 or 3 */
+    int64_t  n_ast;
+    int      M;
+    double*  ast_x[3];            /* positions  [n_ast] */
+    double*  ast_v[3];            /* velocities [n_ast] */
+    double*  ast_acc[3];          /* work: accelerations [n_ast] */
+    double*  ast_m;               /* masses [n_ast] (scatter mode 2 writes) */
+    unsigned char* ast_vis;       /* 0 = frozen and force-free */
+    double*  ast_r;               /* contact radii (0 = never touches) */
+    int64_t* ast_idx;             /* original body index of each asteroid */
+    unsigned char* ast_hot;       /* work [n_ast] */
+    double*  mas_x[3];            /* [M] */
+    double*  mas_v[3];
+    double*  mas_m;
+    unsigned char* mas_vis;
+    double*  mas_r;
+    int64_t* mas_idx;             /* original body index of each massive body */
+    double   G;                   /* G_AU = 4 pi^2 in AU/yr/Msun */
+    double   softening;           /* added to r^2 (SOFTENING = 1e-6 AU^2) */
+    double   max_sub_dt;          /* MAX_SUB_DT_YEARS */
+    int      max_sub_steps;       /* MAX_SUB_STEPS_PER_FRAME */
+    double   w1, w0;              /* Yoshida weights */
+    int      massless_asteroids;  /* 1: every asteroid mass is 0 (no back-reaction) */
+} sss_frame_state;
+
+/* One launch of k raster samples of length dt_raster (frame_kernel). snap is
+ * [k][2*dim][n_ast + M] floats in original body order ([x|y|(z)|vx|vy|(vz)],
+ * the layout NBodyCuda.step_batch returns); sub_pos [k][m_sub][dim][n_ast]
+ * and sub_n [k][n_ast] hold the hot asteroids' sub-samples (sub_n == m_sub:
+ * gap-free); hit_t/hit_m [n_ast] the first contact time since the launch
+ * start (< 0: none, the caller sets -1) and the compact massive index;
+ * guard_used (device int) the number of substeps taken. */
+int sss_frame_launch(sss_ctx* ctx, const sss_frame_state* st, double dt_raster, int k, int m_sub,
+                     float* snap, float* sub_pos, unsigned char* sub_n, float* hit_t, int* hit_m,
+                     int* guard_used, void* stream);
+
+/* Point updates at compact slots (>= 0: asteroid, < 0: massive -slot-1) —
+ * apply_updates (mode 0: set x,v), apply_deltas (mode 1: add to x,v; slots
+ * must be unique), apply_body_state (mode 2: set x,v and mass)
+ * (nbody_kernel.py:947-1010). vals is [m][2*dim] (mode 2: [m][2*dim+1]),
+ * device memory. */
+int sss_frame_scatter(sss_ctx* ctx, const sss_frame_state* st, const int64_t* slot,
+                      const double* vals, int m, int mode, void* stream);
+
 /* ----------------------------------------------- no-allocation variant
  *
  * sss_allpairs_accel_noalloc computes exactly what sss_allpairs_accel

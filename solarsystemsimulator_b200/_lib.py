@@ -45,6 +45,20 @@ class SelfGravState(ctypes.Structure):
     ]
 
 
+class FrameState(ctypes.Structure):
+    """Mirror of sss_frame_state."""
+    _fields_ = [
+        ("dim", ctypes.c_int), ("n_ast", _c_i64), ("M", ctypes.c_int),
+        ("ast_x", _dp * 3), ("ast_v", _dp * 3), ("ast_acc", _dp * 3),
+        ("ast_m", _dp), ("ast_vis", _dp), ("ast_r", _dp), ("ast_idx", _dp), ("ast_hot", _dp),
+        ("mas_x", _dp * 3), ("mas_v", _dp * 3),
+        ("mas_m", _dp), ("mas_vis", _dp), ("mas_r", _dp), ("mas_idx", _dp),
+        ("G", ctypes.c_double), ("softening", ctypes.c_double), ("max_sub_dt", ctypes.c_double),
+        ("max_sub_steps", ctypes.c_int), ("w1", ctypes.c_double), ("w0", ctypes.c_double),
+        ("massless_asteroids", ctypes.c_int),
+    ]
+
+
 # name -> (restype, argtypes); every symbol include/sss.h declares
 SIGNATURES = {
     "sss_abi_version": (ctypes.c_int, []),
@@ -60,6 +74,9 @@ SIGNATURES = {
     "sss_selfgrav_init_accel": (ctypes.c_int, [_vp, ctypes.POINTER(SelfGravState), _vp]),
     "sss_selfgrav_step_batch": (ctypes.c_int, [_vp, ctypes.POINTER(SelfGravState), ctypes.c_int,
                                                ctypes.c_double, ctypes.c_int, _dp, _vp]),
+    "sss_frame_launch": (ctypes.c_int, [_vp, ctypes.POINTER(FrameState), ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
+                                        _dp, _dp, _dp, _vp]),
+    "sss_frame_scatter": (ctypes.c_int, [_vp, ctypes.POINTER(FrameState), _dp, _dp, ctypes.c_int, ctypes.c_int, _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,
