@@ -190,6 +190,25 @@ int sss_frame_launch(sss_ctx* ctx, const sss_frame_state* st, double dt_raster, 
 int sss_frame_scatter(sss_ctx* ctx, const sss_frame_state* st, const int64_t* slot,
                       const double* vals, int m, int mode, void* stream);
 
+/* ------------------------------------------------------------ broadphase
+ *
+ * Asteroid x asteroid collision candidates on a uniform grid and their
+ * exact tests — replaces `Erkennungskarte._hits` and `_zellschluessel`
+ * (film_producer.py:223-321). Inputs are device arrays of n bodies (f32
+ * snapshot x, y, vx, vy; f32 contact radii rr; u8 asteroid and visibility
+ * flags); h is the cell size, halo the stripe halo, [lo, hi) the x stripe
+ * this call owns (-inf/+inf for one card). The hit list is bit-exact against
+ * the reference: out_hits receives up to `capacity` int32 triples
+ * (offset index 0..4, a, b) in no particular order — sorted by (offset, a, b)
+ * they are the reference's pairs (a, b) in its order. n_hits / n_cand (host)
+ * receive the number of hits and of candidate pairs (the reference's
+ * `kandidaten`). Synchronous. SSS_ERR_CAPACITY if more hits than capacity
+ * were found (n_hits tells how many). */
+int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, const float* vx, const float* vy,
+                   const float* rr, const unsigned char* is_ast, const unsigned char* vis, int64_t n,
+                   double dt_y, double h, double halo, float lo, float hi, int* out_hits,
+                   int64_t capacity, int64_t* n_hits, int64_t* n_cand, void* stream);
+
 /* ----------------------------------------------- no-allocation variant
  *
  * sss_allpairs_accel_noalloc computes exactly what sss_allpairs_accel

@@ -77,6 +77,9 @@ SIGNATURES = {
     "sss_frame_launch": (ctypes.c_int, [_vp, ctypes.POINTER(FrameState), ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp,
                                         _dp, _dp, _dp, _vp]),
     "sss_frame_scatter": (ctypes.c_int, [_vp, ctypes.POINTER(FrameState), _dp, _dp, ctypes.c_int, ctypes.c_int, _vp]),
+    "sss_broadphase": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_float, ctypes.c_float, _dp,
+                                      _c_i64, ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64), _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,

@@ -1,0 +1,126 @@
+"""GPU broadphase: the colliding-pair list must be bit-exact.
+
+Against the reference's own `_hits` outputs (golden fixtures: same pairs,
+same (i, j) orientation, same order, same candidate count) and against the
+CPU oracle on further seeded scenes (dense clumps, hidden bodies, stripes,
+degenerate inputs). Mirrors the reference's test_erkennung_streifen.py.
+"""
+import numpy as np
+import pytest
+
+from oracle import broadphase as obp
+
+pytestmark = pytest.mark.gpu
+
+SCENES = ["wolke", "klumpen", "zwei_wolken", "auf_der_grenze"]
+
+
+def _bp():
+    from solarsystemsimulator_b200 import broadphase as bp
+    return bp
+
+
+def _same(res, ref):
+    if ref is None or res is None:
+        return res is None and ref is None
+    return np.array_equal(res[0], ref[0]) and np.array_equal(res[1], ref[1])
+
+
+@pytest.mark.parametrize("scene", SCENES)
+def test_hits_bit_exact_against_reference_golden(load_golden, scene):
+    bp = _bp()
+    g = load_golden(f"broadphase_{scene}.npz")
+    karte = bp.Erkennungskarte(0, np.ones(len(g["x"]), bool), -np.inf, np.inf)
+    karte.stammdaten(np.ones(len(g["x"]), np.uint8), g["rr"])
+    res, cand = karte.bounce_hits(g["x"], g["y"], g["vx"], g["vy"], float(g["dt_y"]), float(g["h"]),
+                                  float(g["halo"]))
+    assert cand == int(g["n_cand"])
+    assert _same(res, (g["hit_i"], g["hit_j"]))
+
+
+@pytest.mark.parametrize("scene", SCENES)
+def test_stripe_union_equals_single_card(load_golden, scene):
+    # test_erkennung_streifen.py: the union of stripe hits is exactly the full set
+    bp = _bp()
+    g = load_golden(f"broadphase_{scene}.npz")
+    n = len(g["x"])
+    karte = bp.Erkennungskarte(0, np.ones(n, bool), -np.inf, np.inf)
+    karte.stammdaten(np.ones(n, np.uint8), g["rr"])
+    full = set(zip(g["hit_i"].tolist(), g["hit_j"].tolist()))
+    for k in (2, 3, 5):
+        got, count = set(), 0
+        for lo, hi in bp._streifengrenzen(g["x"], [1.0 / k] * k):
+            karte.streifen(lo, hi)
+            res, _ = karte.bounce_hits(g["x"], g["y"], g["vx"], g["vy"], float(g["dt_y"]), float(g["h"]),
+                                       float(g["halo"]))
+            if res is not None:
+                part = set(zip(res[0].tolist(), res[1].tolist()))
+                assert not (got & part)
+                got |= part
+                count += len(res[0])
+        assert got == full and count == int(g[f"stripes{k}_count"])
+
+
+def _scene(seed, n, kind):
+    rng = np.random.default_rng(seed)
+    if kind == "clumps":
+        cen = rng.uniform(1, 5, (8, 2))
+        which = rng.integers(0, 8, n)
+        x = cen[which, 0] + rng.normal(0, 0.01, n)
+        y = cen[which, 1] + rng.normal(0, 0.01, n)
+        vx = rng.normal(0, 2, n); vy = rng.normal(5, 2, n)
+        rr = 10 ** rng.uniform(-7, -4, n)
+    else:
+        x = rng.uniform(-5, 5, n); y = rng.uniform(-5, 5, n)
+        vx = rng.normal(0, 6, n); vy = rng.normal(0, 6, n)
+        rr = np.full(n, 2e-3)
+    return [a.astype(np.float32) for a in (x, y, vx, vy, rr)]
+
+
+@pytest.mark.parametrize("kind,n", [("clumps", 60000), ("uniform", 120000)])
+def test_hits_bit_exact_against_oracle(kind, n):
+    bp = _bp()
+    x, y, vx, vy, rr = _scene(5, n, kind)
+    rng = np.random.default_rng(6)
+    is_ast = rng.random(n) > 0.02
+    vis = (rng.random(n) > 0.02).astype(np.uint8)
+    dt = 0.5 / 365.25
+    v95 = float(np.percentile(np.hypot(vx, vy), 95))
+    h = max(1e-4, 2.0 * v95 * dt)
+    halo = 2.0 * h + 2.0 * float(rr.max())
+    ref, cand_ref = obp.hits(x, y, vx, vy, rr, dt, h, halo, is_ast=is_ast, vis=vis)
+    res, cand = bp.bounce_hits(x, y, vx, vy, dt, h, halo, rr=rr, is_ast=is_ast, vis=vis)
+    assert cand == cand_ref
+    assert _same(res, ref)
+    # a stripe with a finite window
+    lo, hi = np.percentile(x, [30, 60])
+    ref, cand_ref = obp.hits(x, y, vx, vy, rr, dt, h, halo, is_ast=is_ast, vis=vis, lo=lo, hi=hi)
+    res, cand = bp.bounce_hits(x, y, vx, vy, dt, h, halo, rr=rr, is_ast=is_ast, vis=vis, lo=lo, hi=hi)
+    assert cand == cand_ref and _same(res, ref)
+
+
+def test_degenerate_inputs():
+    bp = _bp()
+    one = np.ones(1, np.float32)
+    assert bp.bounce_hits(one, one, one, one, 0.01, 0.1, 0.2, rr=one) == (None, 0)
+    x = np.zeros(5, np.float32)
+    hidden = np.zeros(5, np.uint8)
+    assert bp.bounce_hits(x, x, x, x, 0.01, 0.1, 0.2, rr=x + 1e-3, vis=hidden) == (None, 0)
+    # all bodies in one cell: every pair is a candidate and touches
+    res, cand = bp.bounce_hits(x, x, x, x, 0.01, 0.1, 0.2, rr=x + 1e-3)
+    ref, cref = obp.hits(x, x, x, x, x + 1e-3, 0.01, 0.1, 0.2)
+    assert cand == cref and _same(res, ref) and len(res[0]) == 10
+
+
+def test_more_hits_than_the_first_buffer():
+    # a dense clump with far more hits than bodies exercises the capacity retry
+    bp = _bp()
+    rng = np.random.default_rng(8)
+    n = 3000
+    x = (2 + rng.normal(0, 1e-4, n)).astype(np.float32)
+    y = rng.normal(0, 1e-4, n).astype(np.float32)
+    v = rng.normal(0, 1, n).astype(np.float32)
+    rr = np.full(n, 1e-3, np.float32)
+    res, cand = bp.bounce_hits(x, y, v, v, 0.001, 1e-3, 4e-3, rr=rr)
+    ref, cref = obp.hits(x, y, v, v, rr, 0.001, 1e-3, 4e-3)
+    assert cand == cref and _same(res, ref) and len(res[0]) > 4096
