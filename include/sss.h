@@ -209,6 +209,36 @@ int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, const float* vx
                    double dt_y, double h, double halo, float lo, float hi, int* out_hits,
                    int64_t capacity, int64_t* n_hits, int64_t* n_cand, void* stream);
 
+/* ------------------------------------------------------ particle mesh, 2-D
+ *
+ * The reference's isolated 2-D PM (pm_kernel.py:34-293): Hockney-James zero
+ * padding to 2N x 2N, convolution with the transforms of the softened force
+ * kernels, cloud-in-cell deposit and gather, f64. A plan object holds the
+ * cuFFT plans and the grids of one grid size N. All pointers are device
+ * pointers. */
+typedef struct sss_pm2d sss_pm2d;
+int  sss_pm2d_create(sss_ctx* ctx, int grid_n, sss_pm2d** out);
+void sss_pm2d_destroy(sss_pm2d* p);
+/* bbox4 <- (xmin, xmax, ymin, ymax) of n points (grid_fuer, pm_kernel.py:110-124) */
+int  sss_pm2d_bbox(sss_pm2d* p, const double* x, const double* y, int64_t n, double* bbox4, void* stream);
+/* transforms of K_x, K_y = -G d / (|d|^2 + eps2)^1.5 for cell size h (:34-60) */
+int  sss_pm2d_build_kernels(sss_pm2d* p, double h, double eps2, double G, void* stream);
+/* acceleration field of n masses on the grid with origin (x0, y0) (:127-147) */
+int  sss_pm2d_field(sss_pm2d* p, const double* gx, const double* gy, const double* gm, int64_t n,
+                    double x0, double y0, double h, void* stream);
+/* field read back at n points with the deposit's stencil (:93-107, :150-154) */
+int  sss_pm2d_gather(sss_pm2d* p, const double* px, const double* py, int64_t n, double x0, double y0,
+                     double h, double* ax, double* ay, void* stream);
+/* the N x N crops of the last field into ax, ay (the arrays pm_force_field returns) */
+int  sss_pm2d_fields(sss_pm2d* p, double* ax, double* ay, void* stream);
+/* the N x N density of the last field call into rho (:63-90) */
+int  sss_pm2d_density(sss_pm2d* p, double* rho, void* stream);
+/* KDK piece (:264-273): v += hdt a; if drift, x += dt v */
+int  sss_pm2d_kick_drift(sss_pm2d* p, double* x, double* y, double* vx, double* vy, const double* ax,
+                         const double* ay, int64_t n, double hdt, double dt, int drift, void* stream);
+/* out[i] = (float)a[i] (snapshot rows, :274-280) */
+int  sss_pm2d_to_f32(sss_pm2d* p, const double* a, int64_t n, float* out, void* stream);
+
 /* ----------------------------------------------- no-allocation variant
  *
  * sss_allpairs_accel_noalloc computes exactly what sss_allpairs_accel

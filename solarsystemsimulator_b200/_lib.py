@@ -80,6 +80,19 @@ SIGNATURES = {
     "sss_broadphase": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_float, ctypes.c_float, _dp,
                                       _c_i64, ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64), _vp]),
+    "sss_pm2d_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "sss_pm2d_destroy": (None, [_vp]),
+    "sss_pm2d_bbox": (ctypes.c_int, [_vp, _dp, _dp, _c_i64, _dp, _vp]),
+    "sss_pm2d_build_kernels": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp]),
+    "sss_pm2d_field": (ctypes.c_int, [_vp, _dp, _dp, _dp, _c_i64, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, _vp]),
+    "sss_pm2d_gather": (ctypes.c_int, [_vp, _dp, _dp, _c_i64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       _dp, _dp, _vp]),
+    "sss_pm2d_density": (ctypes.c_int, [_vp, _dp, _vp]),
+    "sss_pm2d_fields": (ctypes.c_int, [_vp, _dp, _dp, _vp]),
+    "sss_pm2d_kick_drift": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, _vp]),
+    "sss_pm2d_to_f32": (ctypes.c_int, [_vp, _dp, _c_i64, _dp, _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,

@@ -4,7 +4,9 @@ The reference's array-level code (backend/pm_kernel.py, the broadphase in
 backend/film_producer.py, the NumPy oracles in backend/test_*.py) imports
 cupy. With this shim installed as sys.modules["cupy"] it runs unmodified on
 the CPU in f64 NumPy. Differences to CuPy that matter are pinned here:
-argsort is stable (CuPy sorts stably), asnumpy/asarray are identity-like.
+argsort is stable (CuPy sorts stably), and asarray always copies (CuPy's
+asarray of a host array is a device copy, so in-place updates on the
+"device" array must not reach the caller's array).
 """
 from __future__ import annotations
 
@@ -42,7 +44,7 @@ def install() -> types.ModuleType:
         if not name.startswith("__"):
             setattr(cp, name, getattr(np, name))
     cp.asnumpy = lambda a, *args, **kw: np.asarray(a)
-    cp.asarray = lambda a, dtype=None: np.asarray(a, dtype=dtype)
+    cp.asarray = lambda a, dtype=None: np.array(a, dtype=dtype, copy=True)
 
     def argsort(a, axis=-1, *args, **kw):
         return np.argsort(a, axis=axis, kind="stable")
