@@ -330,6 +330,17 @@ def run_ours(args, rank, world, local_rank):
         r, cores, desc = cpu_sample(w, seconds_target=args.cpu_seconds)
         cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
 
+    rows = None
+    if rank == 0 and not args.no_rows:
+        rows = {}
+        for name, fn in (("frame_solar_system_belt", measure_frame), ("broadphase_asteroid_clouds",
+                                                                       measure_broadphase),
+                         ("pm2d_isolated", measure_pm2d)):
+            try:
+                rows[name] = fn(dev, stream)
+            except Exception as exc:      # a row failing must not hide the headline line
+                rows[name] = {"error": repr(exc)}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -363,6 +374,7 @@ def run_ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk,
+            "rows": rows,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -385,6 +397,140 @@ def gpu_smi_id(dev: int) -> str:
     return str(dev)
 
 
+# ------------------------------------------------- the other hot-path rows
+def _ev_time(fn, stream, reps=1):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / reps
+
+
+def _frame_energy(f, mass, n, G):
+    """Energy of the massive bodies (asteroids are massless) from an f64 export."""
+    d = 3
+    pos = np.stack([f[c * n:(c + 1) * n] for c in range(d)], 1)
+    vel = np.stack([f[(d + c) * n:(d + c + 1) * n] for c in range(d)], 1)
+    m = mass.copy()
+    mi = np.flatnonzero(m > 0)
+    kin = 0.5 * np.sum(m[mi] * (vel[mi] ** 2).sum(1))
+    pot = 0.0
+    for a in range(len(mi)):
+        for b in range(a + 1, len(mi)):
+            r = np.sqrt(np.sum((pos[mi[a]] - pos[mi[b]]) ** 2) + 1e-6)
+            pot -= G * m[mi[a]] * m[mi[b]] / r
+    return kin + pot
+
+
+def measure_frame(dev, stream, steps=10_000):
+    """Solar system + 2000-asteroid belt, 3-D, AU/day, dt = 1 day (two 0.5-day
+    substeps), `steps` raster samples through NBodyCuda, K = 16 per launch."""
+    import time
+    import torch
+    from oracle import frame as of
+    from solarsystemsimulator_b200 import nbody_kernel as nk, workloads
+    w = workloads.solar_system_belt()
+    pos, vel, mass, is_ast, G = w["pos"], w["vel"], w["mass"], w["is_ast"], w["G"]
+    n = len(mass)
+    vis = np.ones(n, np.uint8)
+    sim = nk.NBodyCuda(dev, m_sub=nk.SUB_SAMPLES, G=G, max_sub_dt=0.5)
+    st = sim.load_state(pos[0], pos[1], vel[0], vel[1], mass, vis, is_ast, z=pos[2], vz=vel[2])
+    e0 = _frame_energy(sim.export_f64(st), mass, n, G)
+    sim.step_batch_device(st, 1.0, 16)                       # warm-up
+    st = sim.load_state(pos[0], pos[1], vel[0], vel[1], mass, vis, is_ast, z=pos[2], vz=vel[2])
+    launches = [16] * (steps // 16) + ([steps % 16] if steps % 16 else [])
+
+    def run():
+        for k in launches:
+            sim.step_batch_device(st, 1.0, k)
+    t = _ev_time(run, stream)
+    e1 = _frame_energy(sim.export_f64(st), mass, n, G)
+    # CPU: the oracle's restatement of the same kernel, a few raster samples
+    a, m = np.flatnonzero(is_ast != 0), np.flatnonzero(is_ast == 0)
+    ost = of.FrameState(pos[:, a], vel[:, a], mass[a], np.ones(len(a), bool), np.zeros(len(a)), pos[:, m],
+                        vel[:, m], mass[m], np.ones(len(m), bool), np.zeros(len(m)))
+    cpu_steps = 20
+    t0 = time.perf_counter()
+    of.frame_launch(ost, 1.0, cpu_steps, m_sub=8, G=G, max_sub_dt=0.5)
+    tc = time.perf_counter() - t0
+    return {"workload": "Sun + 8 planets + 2000 massless asteroids, 3-D, AU/day, Yoshida, dt = 1 day "
+                        f"(2 x 0.5-day substeps), {steps} steps, f64",
+            "steps_per_s": steps / t, "us_per_substep": t / (2 * steps) * 1e6, "seconds": t,
+            "energy_drift_massive": abs((e1 - e0) / e0),
+            "cpu_baseline": {"value": cpu_steps / tc, "unit": "steps/s", "cores": 1, "kind": "port",
+                             "sample": f"oracle/frame.py restatement of frame_kernel, {cpu_steps} steps"},
+            "bound": "latency (grid-free persistent kernel, no grid barrier: massless asteroids)"}
+
+
+def measure_broadphase(dev, stream, reps=5):
+    """Asteroid-cloud scene (200,000 asteroids in 5 Gaussian clouds) broadphase
+    on one f32 snapshot, dt = 0.5 day; CPU oracle on a 20,000-asteroid scene
+    of the same shape."""
+    import time
+    import torch
+    from oracle import broadphase as obp
+    from solarsystemsimulator_b200 import broadphase as bp, workloads
+
+    def scene(npc):
+        w = workloads.asteroid_clouds(n_per_cloud=npc)
+        a = np.flatnonzero(w["is_ast"] != 0)
+        f = [w["pos"][0, a], w["pos"][1, a], w["vel"][0, a], w["vel"][1, a]]
+        f = [x.astype(np.float32) for x in f]
+        rr = w["radius"][a].astype(np.float32)
+        dt = 0.5
+        v95 = float(np.percentile(np.hypot(f[2], f[3]), 95))
+        h = max(1e-4, 2.0 * v95 * dt)
+        return f, rr, dt, h, 2.0 * h + 2.0 * float(rr.max())
+
+    f, rr, dt, h, halo = scene(40_000)
+    dev_t = [torch.from_numpy(x).cuda(dev) for x in f]
+    rr_t = torch.from_numpy(rr).cuda(dev)
+    res, cand = bp.bounce_hits(*dev_t, dt, h, halo, rr=rr_t, device=dev)   # warm-up
+    t = _ev_time(lambda: bp.bounce_hits(*dev_t, dt, h, halo, rr=rr_t, device=dev), stream, reps)
+    fs, rrs, dts, hs, halos = scene(4_000)
+    t0 = time.perf_counter()
+    _, cand_cpu = obp.hits(*fs, rrs, dts, hs, halos)
+    tc = time.perf_counter() - t0
+    return {"workload": "5 Gaussian clouds x 40,000 asteroids (sigma 0.01 AU at 1-5 AU), f32 snapshot, "
+                        "dt = 0.5 day, one broadphase call",
+            "ms_per_call": t * 1e3, "candidates": int(cand), "hits": 0 if res is None else len(res[0]),
+            "g_candidates_per_s": cand / t / 1e9,
+            "cpu_baseline": {"value": cand_cpu / tc / 1e9, "unit": "G candidates/s", "cores": 1, "kind": "port",
+                             "sample": f"oracle/broadphase.py on 5 x 4,000 asteroids ({cand_cpu} candidates)"}}
+
+
+def measure_pm2d(dev, stream, steps=10):
+    """The reference's PM dynamics case: 10,000 bodies, grid 2048 (4096^2
+    padded f64 FFTs), KDK steps with tracers-free state."""
+    import time
+    import torch
+    from oracle import pm as opm
+    from solarsystemsimulator_b200 import pm_kernel as pk
+    rng = np.random.default_rng(44)
+    n, R, Mtot = 10000, 30000.0, 5.6e9
+    r = R * np.sqrt(rng.uniform(0, 1, n)); th = rng.uniform(0, 2 * np.pi, n)
+    x, y = r * np.cos(th), r * np.sin(th)
+    m = np.full(n, Mtot / n)
+    vvir = np.sqrt(pk.G_AU * Mtot / R)
+    ang = rng.uniform(0, 2 * np.pi, n)
+    vx, vy = 0.7 * vvir * np.cos(ang), 0.7 * vvir * np.sin(ang)
+    dt = (R / vvir) / 1000.0
+    sim = pk.NBodyPM([dev], grid_n=2048)
+    st = sim.load_state(x, y, vx, vy, m)
+    sim.step_batch(st, dt, 1)
+    t = _ev_time(lambda: sim.step_batch(st, dt, steps), stream) / steps
+    t0 = time.perf_counter()
+    opm.kdk(x, y, vx, vy, m, (np.zeros(0),) * 4, dt, 1, 2048)
+    tc = (time.perf_counter() - t0) / 2     # load_state's evaluation + one step
+    return {"workload": "2-D isolated PM, 10,000 bodies, grid 2048 (4096^2 padded f64 transforms), KDK",
+            "ms_per_step": t * 1e3, "steps_per_s": 1.0 / t,
+            "cpu_baseline": {"value": 1.0 / tc, "unit": "steps/s", "cores": 1, "kind": "port",
+                             "sample": "oracle/pm.py (NumPy f64 FFT) one force evaluation"}}
+
+
 def ctypes_double():
     import ctypes
     return ctypes.c_double()
@@ -398,6 +544,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-rows", action="store_true", help="skip the per-row measurements")
     ap.add_argument("--warmup-cpu", type=int, default=0)
     ap.add_argument("--n-side", type=int, default=N_SIDE,
                     help="sources = n_side^3 (64 is the configuration; smaller only for profiling)")

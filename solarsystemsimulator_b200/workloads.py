@@ -75,3 +75,110 @@ def structure_formation(n_side: int = 64, n_tracer: int = 524_288, sigma_delta: 
     tpos = qt + _interp_periodic(psi, qt).T
     n = len(pos)
     return {"pos": pos, "mass": np.full(n, 1.0 / n), "tracer_pos": tpos}
+
+
+# ------------------------------------------------ solar system + main belt
+
+SEED_SOLAR_BELT = 20260101
+G_AU_DAY = 2.959122e-4            # AU^3 / (Msun day^2) = 4 pi^2 / 365.25^2
+
+# (mass in Msun, semi-major axis in AU) of the eight planets
+PLANETS = ((1.6601e-7, 0.3871), (2.4478e-6, 0.7233), (3.0035e-6, 1.0000), (3.2272e-7, 1.5237),
+           (9.5479e-4, 5.2034), (2.8589e-4, 9.5371), (4.3662e-5, 19.1913), (5.1514e-5, 30.0690))
+
+
+def kepler_to_cartesian(a, e, inc, Omega, omega, M, mu):
+    """Positions and velocities (3, n) of Keplerian orbits (elliptic),
+    eccentric anomaly by Newton iteration."""
+    E = M.copy()
+    for _ in range(50):
+        E = E - (E - e * np.sin(E) - M) / (1 - e * np.cos(E))
+    cE, sE = np.cos(E), np.sin(E)
+    r = a * (1 - e * cE)
+    xp = a * (cE - e)
+    yp = a * np.sqrt(1 - e * e) * sE
+    n_mean = np.sqrt(mu / a ** 3)
+    vxp = -a * n_mean * sE / (1 - e * cE)
+    vyp = a * n_mean * np.sqrt(1 - e * e) * cE / (1 - e * cE)
+    cO, sO, co, so, ci, si = np.cos(Omega), np.sin(Omega), np.cos(omega), np.sin(omega), np.cos(inc), np.sin(inc)
+    R11 = cO * co - sO * so * ci; R12 = -cO * so - sO * co * ci
+    R21 = sO * co + cO * so * ci; R22 = -sO * so + cO * co * ci
+    R31 = so * si; R32 = co * si
+    pos = np.stack([R11 * xp + R12 * yp, R21 * xp + R22 * yp, R31 * xp + R32 * yp])
+    vel = np.stack([R11 * vxp + R12 * vyp, R21 * vxp + R22 * vyp, R31 * vxp + R32 * vyp])
+    return pos, vel
+
+
+def solar_system_belt(n_ast: int = 2000, seed: int = SEED_SOLAR_BELT):
+    """Sun + 8 planets on circular coplanar orbits (real masses and semi-major
+    axes) + n_ast massless asteroids with a ~ U[2.1, 3.3] AU, e ~ U[0, 0.15],
+    i ~ U[0, 10 deg], Omega, omega, M ~ U[0, 2 pi). Units AU, day, Msun.
+    Returns dict with pos (3, n), vel (3, n), mass, is_ast (n = 9 + n_ast)."""
+    rng = np.random.default_rng(seed)
+    G = G_AU_DAY
+    n = 9 + n_ast
+    pos = np.zeros((3, n)); vel = np.zeros((3, n)); mass = np.zeros(n)
+    mass[0] = 1.0
+    for k, (m, a) in enumerate(PLANETS, start=1):
+        th = rng.uniform(0, 2 * np.pi)
+        v = np.sqrt(G * (1.0 + m) / a)
+        pos[:, k] = (a * np.cos(th), a * np.sin(th), 0.0)
+        vel[:, k] = (-v * np.sin(th), v * np.cos(th), 0.0)
+        mass[k] = m
+    a = rng.uniform(2.1, 3.3, n_ast)
+    e = rng.uniform(0.0, 0.15, n_ast)
+    inc = rng.uniform(0.0, np.deg2rad(10.0), n_ast)
+    Om, om, M = (rng.uniform(0, 2 * np.pi, n_ast) for _ in range(3))
+    p, v = kepler_to_cartesian(a, e, inc, Om, om, M, G)
+    pos[:, 9:], vel[:, 9:] = p, v
+    # the sun at rest in the barycentre of the planets
+    ptot = (mass[None, 1:9] * vel[:, 1:9]).sum(1)
+    vel[:, 0] = -ptot / mass[0]
+    is_ast = np.zeros(n, np.uint8); is_ast[9:] = 1
+    return {"pos": pos, "vel": vel, "mass": mass, "is_ast": is_ast, "G": G}
+
+
+# ------------------------------------------------ asteroid clouds
+
+SEED_CLOUDS = 20260404
+
+
+def asteroid_clouds(n_per_cloud: int = 40_000, n_clouds: int = 5, seed: int = SEED_CLOUDS):
+    """A 1 Msun star, 7 planets (m ~ log-U[1e-6, 1e-3] at 0.4-30 AU) and
+    n_clouds Gaussian asteroid clouds (sigma 0.01 AU about random centres at
+    1-5 AU, local circular velocity + N(0, 1e-4) AU/day), radii log-U[1e-7,
+    1e-5] AU, density 2 g/cm^3. Units AU, day, Msun. 3-D (clouds thin in z)."""
+    rng = np.random.default_rng(seed)
+    G = G_AU_DAY
+    n_ast = n_per_cloud * n_clouds
+    n = 8 + n_ast
+    pos = np.zeros((3, n)); vel = np.zeros((3, n)); mass = np.zeros(n)
+    mass[0] = 1.0
+    for k in range(1, 8):
+        a = 10 ** rng.uniform(np.log10(0.4), np.log10(30.0))
+        m = 10 ** rng.uniform(-6, -3)
+        th = rng.uniform(0, 2 * np.pi)
+        v = np.sqrt(G * (1.0 + m) / a)
+        pos[:, k] = (a * np.cos(th), a * np.sin(th), 0.0)
+        vel[:, k] = (-v * np.sin(th), v * np.cos(th), 0.0)
+        mass[k] = m
+    i0 = 8
+    for c in range(n_clouds):
+        rc = rng.uniform(1.0, 5.0)
+        th = rng.uniform(0, 2 * np.pi)
+        cen = np.array([rc * np.cos(th), rc * np.sin(th), 0.0])
+        p = cen[:, None] + rng.normal(0, 0.01, (3, n_per_cloud))
+        r = np.hypot(p[0], p[1])
+        v = np.sqrt(G / r)
+        vel[0, i0:i0 + n_per_cloud] = -v * p[1] / r + rng.normal(0, 1e-4, n_per_cloud)
+        vel[1, i0:i0 + n_per_cloud] = v * p[0] / r + rng.normal(0, 1e-4, n_per_cloud)
+        vel[2, i0:i0 + n_per_cloud] = rng.normal(0, 1e-4, n_per_cloud)
+        pos[:, i0:i0 + n_per_cloud] = p
+        i0 += n_per_cloud
+    rad = 10 ** rng.uniform(-7, -5, n_ast)
+    au_cm = 1.495978707e13
+    msun_g = 1.98847e33
+    mass[8:] = (4.0 / 3.0) * np.pi * (rad * au_cm) ** 3 * 2.0 / msun_g
+    radius = np.zeros(n); radius[8:] = rad
+    is_ast = np.zeros(n, np.uint8); is_ast[8:] = 1
+    return {"pos": pos, "vel": vel, "mass": mass, "radius": radius, "is_ast": is_ast, "G": G}
