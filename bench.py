@@ -335,7 +335,7 @@ def run_ours(args, rank, world, local_rank):
         rows = {}
         for name, fn in (("frame_solar_system_belt", measure_frame), ("broadphase_asteroid_clouds",
                                                                        measure_broadphase),
-                         ("pm2d_isolated", measure_pm2d)):
+                         ("pm2d_isolated", measure_pm2d), ("batched_small_systems", measure_batched)):
             try:
                 rows[name] = fn(dev, stream)
             except Exception as exc:      # a row failing must not hide the headline line
@@ -529,6 +529,43 @@ def measure_pm2d(dev, stream, steps=10):
             "ms_per_step": t * 1e3, "steps_per_s": 1.0 / t,
             "cpu_baseline": {"value": 1.0 / tc, "unit": "steps/s", "cores": 1, "kind": "port",
                              "sample": "oracle/pm.py (NumPy f64 FFT) one force evaluation"}}
+
+
+def measure_batched(dev, stream, steps=10_000):
+    """4,096 independent systems (512 perturbed figure-8s, planetary systems of
+    3-64 bodies), f64 Yoshida-4, dt = 1e-3 of each innermost period; all
+    systems in one graph-captured launch set vs one launch per system."""
+    import time
+    from oracle import batched as ob
+    from solarsystemsimulator_b200 import batched, workloads
+    systems = workloads.batched_ensemble()
+    ens = batched.BatchedSystems(systems, device=dev)
+    ens.capture(steps)
+    ens.replay()                                          # warm-up
+    t = _ev_time(ens.replay, stream)
+    pairs = ens.pairs_per_step() * steps
+    # one launch per system, on 64 systems spread over the sizes, 1/10 of the steps
+    sample = list(np.linspace(0, len(systems) - 1, 64).astype(int))
+    t1 = _ev_time(lambda: ens.run_one_launch_per_system(steps // 10, systems=set(sample)), stream)
+    share = sum(systems[i]["mass"].size * (systems[i]["mass"].size - 1) for i in sample) / \
+        max(1, sum(s["mass"].size * (s["mass"].size - 1) for s in systems))
+    t1_full = t1 * 10 / max(share, 1e-12)
+    # CPU: the oracle on the same 64 systems, 10 steps
+    t0 = time.perf_counter()
+    for i in sample:
+        s = systems[i]
+        ob.yoshida(s["pos"], s["vel"], s["mass"], s["G"], s["dt"], 10)
+    tc = (time.perf_counter() - t0) / 10 / max(share, 1e-12)
+    maps = {str(g["max_n"]): list(g["map"]) for g in ens.groups}
+    return {"workload": "4096 systems (512 figure-8 + planetary 3-64 bodies), f64 Yoshida-4, dt = 1e-3 "
+                        f"innermost period, {steps} steps in one captured graph",
+            "steps_per_s": steps / t, "system_steps_per_s": len(systems) * steps / t,
+            "g_interactions_per_s": pairs / t / 1e9,
+            "one_launch_per_system_steps_per_s_est": steps / t1_full,
+            "speedup_vs_one_launch_per_system": t1_full / t,
+            "team_mapping_by_group_max_n": maps,
+            "cpu_baseline": {"value": 1.0 / tc, "unit": "ensemble steps/s", "cores": 1, "kind": "port",
+                             "sample": "oracle/batched.py, 64 systems x 10 steps, scaled by pair share"}}
 
 
 def ctypes_double():

@@ -239,6 +239,23 @@ int  sss_pm2d_kick_drift(sss_pm2d* p, double* x, double* y, double* vx, double* 
 /* out[i] = (float)a[i] (snapshot rows, :274-280) */
 int  sss_pm2d_to_f32(sss_pm2d* p, const double* a, int64_t n, float* out, void* stream);
 
+/* ------------------------------------------------ batched small systems
+ *
+ * Many independent systems of <= 64 bodies, f64 Yoshida-4 with a fixed
+ * per-system dt, `steps` steps in one persistent launch. Bodies of all
+ * systems are concatenated (x[c], v[c], m; system s owns [off[s], off[s+1]));
+ * G[s], dt[s] per system; the launch integrates the systems listed in
+ * sys_list[0..n_list) (all with at most max_n bodies) with a team of `team`
+ * lanes (1, 2, 4, 8, 16 or 32) holding `per_lane` bodies each
+ * (team * per_lane >= max_n). blocks = 0 picks one team per system.
+ * Pair force: the softened all-pairs formula within each system (eps2 may
+ * be 0; the self pair is excluded). No reference counterpart: the reference
+ * integrates one system at a time (nbody_kernel.py, index.html engines). */
+int sss_batched_launch(sss_ctx* ctx, int dim, double* const* x, double* const* v, const double* m,
+                       const int64_t* off, const double* G, const double* dt, const int* sys_list,
+                       int n_list, int max_n, int team, int per_lane, double eps2, int steps, int blocks,
+                       void* stream);
+
 /* ----------------------------------------------- no-allocation variant
  *
  * sss_allpairs_accel_noalloc computes exactly what sss_allpairs_accel

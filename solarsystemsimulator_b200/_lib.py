@@ -93,6 +93,9 @@ SIGNATURES = {
     "sss_pm2d_kick_drift": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_int, _vp]),
     "sss_pm2d_to_f32": (ctypes.c_int, [_vp, _dp, _c_i64, _dp, _vp]),
+    "sss_batched_launch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp, _dp,
+                                          _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,

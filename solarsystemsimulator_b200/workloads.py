@@ -182,3 +182,56 @@ def asteroid_clouds(n_per_cloud: int = 40_000, n_clouds: int = 5, seed: int = SE
     radius = np.zeros(n); radius[8:] = rad
     is_ast = np.zeros(n, np.uint8); is_ast[8:] = 1
     return {"pos": pos, "vel": vel, "mass": mass, "radius": radius, "is_ast": is_ast, "G": G}
+
+
+# ------------------------------------------------ batched small systems
+
+SEED_ENSEMBLE = 20260202
+FIGURE8_PERIOD = 6.32591398    # period of the figure-8 choreography (G = m = 1)
+
+
+def figure8(rng=None, noise: float = 0.0):
+    """The Chenciner-Montgomery figure-8 initial conditions of the reference
+    (index.html:2464-2490, G = m = 1, unscaled), optionally with N(0, noise)
+    velocity perturbations. Returns pos (3, 3), vel (3, 3), mass (3,)."""
+    px, py = 0.97000436, 0.24308753
+    vx, vy = 0.4662036850, 0.4323657300
+    pos = np.array([[-px, px, 0.0], [py, -py, 0.0], [0.0, 0.0, 0.0]])
+    vel = np.array([[vx, vx, -2 * vx], [vy, vy, -2 * vy], [0.0, 0.0, 0.0]])
+    if noise and rng is not None:
+        vel[:2] += rng.normal(0, noise, (2, 3))
+    return pos, vel, np.ones(3)
+
+
+def batched_ensemble(n_systems: int = 4096, n_figure8: int = 512, seed: int = SEED_ENSEMBLE):
+    """Independent systems: n_figure8 perturbed figure-8 choreographies (G = 1,
+    velocity noise N(0, 1e-3)) and planetary systems of 3-64 bodies (body
+    count log-uniform): a 1 Msun star + planets with a ~ log-U[0.05, 30] AU,
+    m ~ log-U[1e-7, 1e-3] Msun, e ~ U[0, 0.1], i ~ U[0, 5 deg], random angles
+    (G = 4 pi^2, AU/yr). dt = 1e-3 of each system's innermost period.
+    Returns a list of dicts (pos (3, n), vel (3, n), mass, G, dt)."""
+    rng = np.random.default_rng(seed)
+    systems = []
+    G_au = 4 * np.pi ** 2
+    for s in range(n_systems):
+        if s < n_figure8:
+            pos, vel, m = figure8(rng, 1e-3)
+            systems.append({"pos": pos, "vel": vel, "mass": m, "G": 1.0, "dt": 1e-3 * FIGURE8_PERIOD})
+            continue
+        n = int(np.round(np.exp(rng.uniform(np.log(3), np.log(64)))))
+        n = min(max(n, 3), 64)
+        k = n - 1
+        a = np.sort(np.exp(rng.uniform(np.log(0.05), np.log(30.0), k)))
+        m = np.exp(rng.uniform(np.log(1e-7), np.log(1e-3), k))
+        e = rng.uniform(0, 0.1, k)
+        inc = rng.uniform(0, np.deg2rad(5.0), k)
+        Om, om, M = (rng.uniform(0, 2 * np.pi, k) for _ in range(3))
+        p, v = kepler_to_cartesian(a, e, inc, Om, om, M, G_au * (1.0 + m))
+        pos = np.concatenate([np.zeros((3, 1)), p], 1)
+        vel = np.concatenate([np.zeros((3, 1)), v], 1)
+        mass = np.concatenate([[1.0], m])
+        vel -= (mass[None] * vel).sum(1, keepdims=True) / mass.sum()
+        pos -= (mass[None] * pos).sum(1, keepdims=True) / mass.sum()
+        p_in = 2 * np.pi * np.sqrt(a[0] ** 3 / (G_au * (1.0 + m[0])))
+        systems.append({"pos": pos, "vel": vel, "mass": mass, "G": G_au, "dt": 1e-3 * p_in})
+    return systems
