@@ -116,9 +116,13 @@ class BatchedSystems:
                 self._launch(g, steps, stream, sys_list=one, n_list=1)
 
     def capture(self, steps: int) -> None:
-        """Record `run(steps)` once into a CUDA graph (one launch per replay)."""
+        """Record `run(steps)` once into a CUDA graph (one launch per replay).
+        The state is unchanged by the capture itself."""
+        x0, v0 = self.x.clone(), self.v.clone()
         self.run(1)                                   # warm-up outside the capture
         torch.cuda.synchronize(self.device)
+        self.x.copy_(x0)
+        self.v.copy_(v0)
         self._graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self._graph):
             self.run(steps)
