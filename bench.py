@@ -582,6 +582,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-rows", action="store_true", help="skip the per-row measurements")
+    ap.add_argument("--row", choices=["frame", "broadphase", "pm2d", "batched"],
+                    help="run only this row's measurement (profiling) and print it")
+    ap.add_argument("--row-steps", type=int, default=0, help="steps of the --row measurement (0: default)")
     ap.add_argument("--warmup-cpu", type=int, default=0)
     ap.add_argument("--n-side", type=int, default=N_SIDE,
                     help="sources = n_side^3 (64 is the configuration; smaller only for profiling)")
@@ -594,6 +597,16 @@ def main():
     local_rank = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.row:
+        import torch
+        torch.cuda.set_device(local_rank)
+        fn = {"frame": measure_frame, "broadphase": measure_broadphase, "pm2d": measure_pm2d,
+              "batched": measure_batched}[args.row]
+        kw = {"steps": args.row_steps} if args.row_steps and args.row != "broadphase" else {}
+        if args.row == "broadphase" and args.row_steps:
+            kw = {"reps": args.row_steps}
+        print(json.dumps(fn(local_rank, torch.cuda.current_stream(local_rank), **kw)), flush=True)
+        return 0
     return run_ours(args, rank, world, local_rank)
 
 
