@@ -38,6 +38,9 @@ N_TRACER = 524_288
 EPS = 1e-3
 DT = 1e-3
 FLOP_PER_PAIR = 20          # the reference's own convention (TODO.md:73-74)
+# DRAM bytes (read + write) of one k_force_mixed launch on this workload, from an
+# ncu capture of the full-size launch (profiles/k_force_mixed_dram_traffic_262k.md)
+MIXED_DRAM_BYTES_PER_LAUNCH = 270_845_568
 METRIC = "G interactions/s (all-pairs self-gravity, mixed FP32-pair/FP64-accumulate, Yoshida-4)"
 UNIT = "G interactions/s"
 
@@ -363,7 +366,9 @@ def run_ours(args, rank, world, local_rank):
                                                  "targets": len(samp)},
             "energy_drift": abs((e_m1 - e_m0) / e_m0),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak["fp32"],
-                         "unit": "TFLOP/s", "frac": achieved / peak["fp32"], "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak["fp32"],
+                         "traffic": MIXED_DRAM_BYTES_PER_LAUNCH if (n_src, n_tgt) == (262144, 786432) else None,
+                         "traffic_unit": "bytes per launch (ncu capture)",
                          "kernel": "k_force_mixed", "kernel_ms": t_kernel_mixed * 1e3,
                          "flop_per_pair": FLOP_PER_PAIR,
                          "peak_source": "FFMA-chain probe measured in this run (no FP32 "
