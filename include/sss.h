@@ -239,6 +239,118 @@ int  sss_pm2d_kick_drift(sss_pm2d* p, double* x, double* y, double* vx, double* 
 /* out[i] = (float)a[i] (snapshot rows, :274-280) */
 int  sss_pm2d_to_f32(sss_pm2d* p, const double* a, int64_t n, float* out, void* stream);
 
+/* ------------------------------------------------ particle mesh, 3-D periodic
+ *
+ * The reference's PM cycle (TODO.md:225-253; 2-D code pm_kernel.py:63-154)
+ * in a periodic cube of side `box` on an n^3 f32 mesh: cloud-in-cell deposit
+ * with warp-aggregated atomics, one R2C transform, one fused kernel for the
+ * Green's function -4 pi G / k^2 * W(k)^-deconv * exp(-k^2 r_split^2)
+ * (W the CIC window; deconv = 2 undoes deposit and interpolation, the
+ * Gaussian is the long-range filter that keeps it from amplifying the
+ * mesh-scale aliasing) and the spectral gradient -i k_d (the 1/n^3 of the
+ * inverse folded in), one batched C2R for the three components, and
+ * trilinear (CIC) interpolation into f64 accelerations. cuFFT performs only the transforms. A plan holds the
+ * meshes and plans of one mesh size; particles stay with the caller.
+ *
+ * Particle state (device pointers, SoA f64): x[3], v[3], a[3]; masses m[n]
+ * or, when m is NULL, every particle has mass_const. Positions are kept
+ * wrapped into [0, box). */
+typedef struct {
+    int64_t n;
+    double* x[3];
+    double* v[3];
+    double* a[3];
+    const double* m;
+    double mass_const;
+} sss_pm3_particles;
+
+/* epilogue of a force pass (the KDK pieces fused into the kernel that
+ * produces the accelerations; v += hdt a is a half kick):
+ * SSS_PM3_FORCE: a only; SSS_PM3_KICK: a, then v += hdt a;
+ * SSS_PM3_KICK_DRIFT: a, v += hdt a, f32 snapshot row, v += hdt a,
+ * x = wrap(x + dt v) (the closing kick of this step and the opening kick
+ * and drift of the next). */
+#define SSS_PM3_FORCE      0
+#define SSS_PM3_KICK       1
+#define SSS_PM3_KICK_DRIFT 2
+
+typedef struct sss_pm3 sss_pm3;
+int  sss_pm3_create(sss_ctx* ctx, int mesh_n, double box, sss_pm3** out);
+void sss_pm3_destroy(sss_pm3* p);
+/* internal meshes: rho (n^3 f32 density = mass / h^3) and the three
+ * acceleration meshes (3 n^3 f32, contiguous), valid until the next call */
+int  sss_pm3_meshes(sss_pm3* p, float** rho, float** accel);
+/* deposit (rho) -> transforms -> acceleration meshes */
+int  sss_pm3_density(sss_pm3* p, const sss_pm3_particles* s, void* stream);
+int  sss_pm3_solve(sss_pm3* p, double G, int deconv, double r_split, void* stream);
+/* interpolate the meshes at the particles into s->a and run the epilogue
+ * `mode`; snap (nullable) receives the f32 row [x|y|z|vx|vy|vz] (6 n) */
+int  sss_pm3_gather(sss_pm3* p, const sss_pm3_particles* s, int mode, double hdt, double dt, float* snap,
+                    void* stream);
+/* opening half kick and drift of one KDK step: v += hdt a; x = wrap(x + dt v) */
+int  sss_pm3_kick_drift(sss_pm3* p, const sss_pm3_particles* s, double hdt, double dt, void* stream);
+
+/* ------------------------------------------------ Ewald direct sum, f64
+ *
+ * The judge of the mesh forces: the exact periodic force of point masses
+ * with Plummer softening eps2 on the nearest image (Ewald summation,
+ * Hernquist, Bouchet & Suto 1991): a real-space part over the nearest image
+ * of every source within r_cut (r_cut <= box/2), and a reciprocal part over
+ * the nk half-space vectors h (int32 triples, device) with per-vector
+ * coefficient coef[k] = 2 * 4 pi / box^3 * exp(-|k|^2 / (4 alpha^2)) / |k|^2,
+ * k = 2 pi h / box. No reference counterpart (the reference has no periodic
+ * solver); it plays the role of its all-pairs check (test_selfgrav.py:66-88).
+ *
+ * sss_ewald_structure: sc[2k], sc[2k+1] <- sum_j m_j cos, sin(k . x_j);
+ * hmax >= every |h| component of the list (<= 40; a vector outside it, or
+ * with h_x < 0, contributes nothing).
+ * sss_ewald_accel: accelerations at n_tgt target positions (t[3], device);
+ * self_idx (nullable) names the source each target is (skipped). */
+int sss_ewald_structure(sss_ctx* ctx, const sss_pm3_particles* src, double box, const int* hvec,
+                        int nk, int hmax, double* sc, void* stream);
+int sss_ewald_accel(sss_ctx* ctx, const sss_pm3_particles* src, const double* const* t,
+                    const int64_t* self_idx, int64_t n_tgt, double G, double box, double alpha,
+                    double r_cut, double eps2, const int* hvec, const double* coef, const double* sc,
+                    int nk, double* const* out, void* stream);
+
+/* ------------------------------------------- learned short-range correction
+ *
+ * A per-particle MLP 67 -> 128 -> 128 -> 3 (SiLU) that adds the short-range
+ * force the mesh cannot resolve. Inputs: log1p(rho / rho_mean) on the 4x4x4
+ * mesh cells around the particle's cell (i0-1 .. i0+2 per axis), then the
+ * sub-cell offsets - 1/2 (padded with zeros to 80). Weights are bf16 on the
+ * tensor cores (mma.sync m16n8k16), accumulation f32. Parameters are one
+ * f32 array of SSS_MLP_N_PARAMS: W1[80][128], b1[128], W2[128][128], b2[128],
+ * W3[128][8], b3[8] (rows 67..79 of W1 and columns 3..7 of W3 zero);
+ * sss_mlp_pack turns them into the bf16 fragment arrays (SSS_MLP_N_FRAGS
+ * uint32) the kernels read. No reference counterpart. */
+#define SSS_MLP_N_PARAMS 27912
+#define SSS_MLP_N_FRAGS  23040
+#define SSS_MLP_IN_PAD   80
+int sss_mlp_pack(sss_ctx* ctx, const float* params, uint32_t* frags, void* stream);
+/* X[r] (bf16 bits, 80 per row) <- inputs of particle idx[r] (idx NULL: r) */
+int sss_mlp_features(sss_ctx* ctx, sss_pm3* p, const sss_pm3_particles* s, const int64_t* idx, int64_t rows,
+                     double rho_mean, uint16_t* X, void* stream);
+/* Y[r][0..3) <- network output for input row X[r] */
+int sss_mlp_forward(sss_ctx* ctx, const float* params, const uint32_t* frags, const uint16_t* X, int64_t rows,
+                    float* Y, void* stream);
+/* gradient of mean over rows and outputs of (Y - T)^2 with respect to the
+ * parameters, over the rows idx[0..rows) of X and T (X holds x_rows rows;
+ * T f32, 3 per row; idx NULL: rows 0..rows; an index outside X counts as a
+ * zero row); grads (SSS_MLP_N_PARAMS f32) overwritten; loss (device f32,
+ * nullable) <- the loss. Deterministic. */
+int sss_mlp_grad(sss_ctx* ctx, const float* params, const uint32_t* frags, const uint16_t* X, const float* T,
+                 int64_t x_rows, const int32_t* idx, int64_t rows, float* grads, float* loss, void* stream);
+/* Adam (Kingma & Ba 2015) on n parameters, step t >= 1 */
+int sss_mlp_adam(sss_ctx* ctx, float* params, const float* grads, float* m, float* v, int64_t n, int t,
+                 double lr, double beta1, double beta2, double eps, void* stream);
+/* the correction pass: a = a + out_scale * MLP(inputs) for every particle
+ * of s (a holds the mesh accelerations), then the epilogue `mode` as
+ * sss_pm3_gather */
+int sss_mlp_correct(sss_ctx* ctx, sss_pm3* p, const sss_pm3_particles* s, const float* params,
+                    const uint32_t* frags, double rho_mean, double out_scale, int mode, double hdt, double dt,
+                    float* snap, void* stream);
+
 /* ------------------------------------------------ batched small systems
  *
  * Many independent systems of <= 64 bodies, f64 Yoshida-4 with a fixed

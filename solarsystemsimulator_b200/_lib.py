@@ -59,6 +59,21 @@ class FrameState(ctypes.Structure):
     ]
 
 
+class Pm3Particles(ctypes.Structure):
+    """Mirror of sss_pm3_particles."""
+    _fields_ = [
+        ("n", _c_i64), ("x", _dp * 3), ("v", _dp * 3), ("a", _dp * 3),
+        ("m", _dp), ("mass_const", ctypes.c_double),
+    ]
+
+
+PM3_FORCE = 0
+PM3_KICK = 1
+PM3_KICK_DRIFT = 2
+MLP_N_PARAMS = 27912
+MLP_N_FRAGS = 23040
+MLP_IN_PAD = 80
+
 # name -> (restype, argtypes); every symbol include/sss.h declares
 SIGNATURES = {
     "sss_abi_version": (ctypes.c_int, []),
@@ -96,6 +111,29 @@ SIGNATURES = {
     "sss_batched_launch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp, _dp,
                                           _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp]),
+    "sss_pm3_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),
+    "sss_pm3_destroy": (None, [_vp]),
+    "sss_pm3_meshes": (ctypes.c_int, [_vp, ctypes.POINTER(_dp), ctypes.POINTER(_dp)]),
+    "sss_pm3_density": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), _vp]),
+    "sss_pm3_solve": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, _vp]),
+    "sss_pm3_gather": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double, _dp, _vp]),
+    "sss_pm3_kick_drift": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.c_double, ctypes.c_double,
+                                          _vp]),
+    "sss_ewald_structure": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.c_double, _dp, ctypes.c_int,
+                                           ctypes.c_int, _dp, _vp]),
+    "sss_ewald_accel": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.POINTER(_dp), _dp, _c_i64,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, _dp, _dp, _dp, ctypes.c_int, ctypes.POINTER(_dp), _vp]),
+    "sss_mlp_pack": (ctypes.c_int, [_vp, _dp, _dp, _vp]),
+    "sss_mlp_features": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(Pm3Particles), _dp, _c_i64, ctypes.c_double,
+                                        _dp, _vp]),
+    "sss_mlp_forward": (ctypes.c_int, [_vp, _dp, _dp, _dp, _c_i64, _dp, _vp]),
+    "sss_mlp_grad": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _c_i64, _dp, _c_i64, _dp, _dp, _vp]),
+    "sss_mlp_adam": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp]),
+    "sss_mlp_correct": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(Pm3Particles), _dp, _dp, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,

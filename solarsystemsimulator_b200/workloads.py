@@ -28,11 +28,11 @@ def zeldovich_displacement(ngrid: int, sigma_delta: float, index: float, seed: i
     amp = k2 ** (index / 4.0)          # sqrt(P) = k^(index/2) = (k^2)^(index/4)
     amp[0, 0, 0] = 0.0
     dk = wk * amp
-    delta = np.fft.irfftn(dk, s=(ngrid,) * 3)
+    delta = np.fft.irfftn(dk, s=(ngrid,) * 3, axes=(0, 1, 2))
     dk *= sigma_delta / delta.std()
     psi = np.empty((3, ngrid, ngrid, ngrid))
     for c, kc in enumerate((kx, ky, kz)):
-        psi[c] = np.fft.irfftn(1j * kc * dk / k2, s=(ngrid,) * 3)
+        psi[c] = np.fft.irfftn(1j * kc * dk / k2, s=(ngrid,) * 3, axes=(0, 1, 2))
     return psi
 
 
@@ -75,6 +75,32 @@ def structure_formation(n_side: int = 64, n_tracer: int = 524_288, sigma_delta: 
     tpos = qt + _interp_periodic(psi, qt).T
     n = len(pos)
     return {"pos": pos, "mass": np.full(n, 1.0 / n), "tracer_pos": tpos}
+
+
+# ------------------------------------------ periodic structure (mesh + MLP)
+
+SEED_PERIODIC = 20260505
+
+
+def periodic_structure(n_side: int = 128, mesh_n: int = 256, sigma_mesh: float = 0.5, index: float = -2.0,
+                       softening: float = 1e-3, seed: int = SEED_PERIODIC):
+    """Particle-mesh workload: n_side^3 equal-mass particles (total mass 1,
+    G = 1) in the periodic unit box, a lattice displaced by Zel'dovich
+    displacements from P(k) ~ k^index normalised to rms density contrast
+    sigma_mesh on the particle lattice (the mesh scale of a mesh twice as
+    fine), wrapped into [0, 1); cold start. 128^3 = 1,048,576 particles on a
+    256^3 mesh is the full configuration.
+
+    Returns dict with pos (n,3), vel (n,3), mass (scalar per particle),
+    mesh_n, softening."""
+    psi = zeldovich_displacement(n_side, sigma_mesh, index, seed)
+    g = (np.arange(n_side) + 0.5) / n_side
+    qx, qy, qz = np.meshgrid(g, g, g, indexing="ij")
+    q = np.stack([qx.ravel(), qy.ravel(), qz.ravel()], 1)
+    pos = q + np.stack([psi[c].ravel() for c in range(3)], 1)
+    pos -= np.floor(pos)
+    n = len(pos)
+    return {"pos": pos, "vel": np.zeros_like(pos), "mass": 1.0 / n, "mesh_n": mesh_n, "softening": softening}
 
 
 # ------------------------------------------------ solar system + main belt
