@@ -38,7 +38,7 @@ static_assert(NFR == SSS_MLP_N_FRAGS, "fragment layout");
 static_assert(K1 == SSS_MLP_IN_PAD, "input width");
 
 constexpr int XS = 44;          // row stride (uint32) of a staged 16 x 80 bf16 input tile (88 bf16)
-constexpr int WARPS_FWD = 4;    // warps per CTA of the forward kernels
+constexpr int WARPS_FWD = 8;    // warps per CTA of the forward kernels (sharing one weight copy)
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);   // .x (low half) = lo
@@ -114,18 +114,37 @@ __device__ __forceinline__ void particle_features(const float* __restrict__ rho,
     int i[3];
     double t[3];
     for (int c = 0; c < 3; ++c) pm3_cell(s.x[c][p], inv_h, n, i[c], t[c]);
-    for (int a = 2 * half; a < 2 * half + 2; ++a) {
-        const int ix = (i[0] + a - 1 + n) % n;
-        for (int b = 0; b < 4; ++b) {
-            const int iy = (i[1] + b - 1 + n) % n;
-            const long long rowb = ((long long)ix * n + iy) * n;
+    // wrapped cell offsets of the patch, then all 32 loads in flight at once
+    long long ox[2];
+    int oy[4], oz[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int iz = (i[2] + e - 1 + n) % n;
-                const float v = log1pf(__ldg(rho + rowb + iz) * inv_mean);
-                row[a * 16 + b * 4 + e] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
-            }
-        }
+    for (int a = 0; a < 2; ++a) {
+        int ix = i[0] + 2 * half + a - 1;
+        ix += ix < 0 ? n : 0;
+        ix -= ix >= n ? n : 0;
+        ox[a] = (long long)ix * n * n;
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        int iy = i[1] + b - 1, iz = i[2] + b - 1;
+        iy += iy < 0 ? n : 0;
+        iy -= iy >= n ? n : 0;
+        iz += iz < 0 ? n : 0;
+        iz -= iz >= n ? n : 0;
+        oy[b] = iy * n;
+        oz[b] = iz;
+    }
+    float v[32];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[a * 16 + b * 4 + e] = __ldg(rho + ox[a] + oy[b] + oz[e]);
+#pragma unroll
+    for (int q = 0; q < 32; q += 2) {
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(log1pf(v[q] * inv_mean), log1pf(v[q + 1] * inv_mean));
+        *reinterpret_cast<__nv_bfloat162*>(row + half * 32 + q) = h2;
     }
     if (half == 1) {
         for (int c = 0; c < 3; ++c) row[64 + c] = __bfloat16_as_ushort(__float2bfloat16_rn((float)(t[c] - 0.5)));
@@ -218,7 +237,7 @@ __device__ __forceinline__ void stage_forward_weights(const float* __restrict__ 
 }
 
 // the correction pass over all particles (sss_mlp_correct)
-__global__ void __launch_bounds__(WARPS_FWD * 32) k_mlp_correct(const Pm3Parts s, const float* __restrict__ rho,
+__global__ void __launch_bounds__(WARPS_FWD * 32, 2) k_mlp_correct(const Pm3Parts s, const float* __restrict__ rho,
                                                                 int n, double inv_h, float inv_mean,
                                                                 const float* __restrict__ P,
                                                                 const uint32_t* __restrict__ F, double out_scale,
@@ -251,7 +270,7 @@ __global__ void __launch_bounds__(WARPS_FWD * 32) k_mlp_correct(const Pm3Parts s
 }
 
 // forward on given input rows (sss_mlp_forward)
-__global__ void __launch_bounds__(WARPS_FWD * 32) k_mlp_fwd(const uint16_t* __restrict__ X, long long rows,
+__global__ void __launch_bounds__(WARPS_FWD * 32, 2) k_mlp_fwd(const uint16_t* __restrict__ X, long long rows,
                                                             const float* __restrict__ P,
                                                             const uint32_t* __restrict__ F, float* __restrict__ Y) {
     extern __shared__ __align__(16) uint32_t smem[];
@@ -286,7 +305,7 @@ __global__ void __launch_bounds__(WARPS_FWD * 32) k_mlp_fwd(const uint16_t* __re
 // features of selected particles (sss_mlp_features)
 __global__ void k_mlp_features(const Pm3Parts s, const float* __restrict__ rho, int n, double inv_h, float inv_mean,
                                const long long* __restrict__ idx, long long rows, uint16_t* __restrict__ X) {
-    __shared__ uint16_t tile[4][16][88];
+    __shared__ __align__(16) uint16_t tile[4][16][88];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long r = ((long long)blockIdx.x * 4 + warp) * 16 + (lane & 15);
     long long p = -1;
@@ -656,7 +675,7 @@ extern "C" int sss_mlp_forward(sss_ctx* ctx, const float* params, const uint32_t
     const size_t smem = FWD_SMEM_U32 * sizeof(uint32_t);
     SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long tiles = (rows + 15) / 16;
-    const int blocks = (int)std::min<long long>((tiles + WARPS_FWD - 1) / WARPS_FWD, (long long)ctx->num_sms * 4);
+    const int blocks = (int)std::min<long long>((tiles + WARPS_FWD - 1) / WARPS_FWD, (long long)ctx->num_sms * 2);
     k_mlp_fwd<<<blocks, WARPS_FWD * 32, smem, (cudaStream_t)stream>>>(X, rows, params, frags, Y);
     SSS_LAUNCH_CHECK(ctx, "k_mlp_fwd");
     return SSS_OK;
@@ -676,7 +695,7 @@ extern "C" int sss_mlp_correct(sss_ctx* ctx, sss_pm3* p, const sss_pm3_particles
     const size_t smem = FWD_SMEM_U32 * sizeof(uint32_t);
     SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(k_mlp_correct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long tiles = (s->n + 15) / 16;
-    const int blocks = (int)std::min<long long>((tiles + WARPS_FWD - 1) / WARPS_FWD, (long long)ctx->num_sms * 4);
+    const int blocks = (int)std::min<long long>((tiles + WARPS_FWD - 1) / WARPS_FWD, (long long)ctx->num_sms * 2);
     Pm3Epi e{mode, hdt, dt, p->box, snap};
     k_mlp_correct<<<blocks, WARPS_FWD * 32, smem, (cudaStream_t)stream>>>(
         pm3_parts(s), p->rho, p->n, p->n / p->box, (float)(1.0 / rho_mean), params, frags, out_scale, e);

@@ -240,5 +240,8 @@ def test_learned_run_gains_and_judge_reverts(mods):
     st["buf"].copy_(buf0)
     sim.pm.forces(st, net2)
     sim.pm.step_batch(st, 2e-3, 5, net2)
+    # the deposit adds f32 weights by atomics in no fixed order, so two replays
+    # agree to rounding (~1e-12 here); the mesh-only force or the rejected
+    # network would move the particles by 5e-7 .. 1e-5 over these 5 steps
     d = (x_after - st["buf"][0:3]).abs()
-    assert float(torch.minimum(d, 1.0 - d).max()) <= 1e-12
+    assert float(torch.minimum(d, 1.0 - d).max()) <= 1e-9
