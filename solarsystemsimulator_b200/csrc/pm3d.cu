@@ -4,8 +4,8 @@
 // mesh in a periodic box.
 //
 //   deposit  : CIC, positions f64, weights f32, warp-aggregated atomics:
-//              lanes of a warp that hit the same node add their weights in
-//              registers first and one lane issues the atomic.
+//              lanes of a warp whose particles share a cell add their
+//              weights in registers first and one lane issues the atomics.
 //   solve    : cuFFT R2C -> k_spectrum3 (Green's function -4 pi G / k^2,
 //              divided by the CIC window W(k)^deconv (2: deposit and
 //              gather) and filtered by exp(-k^2 r_split^2), the spectral
@@ -35,16 +35,11 @@ int cufft_err(sss_ctx* ctx, cufftResult r, const char* what) {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-// Sum of v over the lanes of this warp whose key equals this lane's key;
-// valid in the lowest such lane (the group's leader), which is returned in
-// *leader. All 32 lanes must call it. Groups add in lane order.
-__device__ __forceinline__ float warp_group_sum(int key, float v, bool& leader) {
+// Sum of v over the lanes in `peers` (this lane's group, lane order); all 32
+// lanes must call it with their own group and the warp's largest group
+// size `most`.
+__device__ __forceinline__ float group_sum(unsigned peers, unsigned most, float v) {
     const int lane = threadIdx.x & 31;
-    const unsigned peers = __match_any_sync(FULL, key);
-    leader = (__ffs(peers) - 1) == lane;
-    const unsigned size = __popc(peers);
-    const unsigned most = __reduce_max_sync(FULL, size);
-    if (most == 1) return v;
     float sum = 0.0f;
     unsigned rest = peers;
     for (unsigned k = 0; k < most; ++k) {
@@ -58,6 +53,11 @@ __device__ __forceinline__ float warp_group_sum(int key, float v, bool& leader) 
     return sum;
 }
 
+// Warp-aggregated CIC deposit. Lanes whose particles lie in the same cell
+// share all 8 corner nodes: one __match_any_sync on the cell finds them, the
+// group's weights are added in registers (lane order) and its lowest lane
+// issues one atomic per corner. Particles of different cells that share a
+// node still add separately (atomics keep that correct).
 __global__ void __launch_bounds__(256) k_deposit3(const Pm3Parts s, int n, double inv_h, double inv_h3,
                                                   float* __restrict__ rho) {
     const int lane = threadIdx.x & 31;
@@ -73,15 +73,21 @@ __global__ void __launch_bounds__(256) k_deposit3(const Pm3Parts s, int n, doubl
             for (int c = 0; c < 3; ++c) pm3_cell(s.x[c][p], inv_h, n, i[c], t[c]);
             mass = (s.m ? s.m[p] : s.mass_const) * inv_h3;
         }
+        const int cell = ok ? (i[0] * n + i[1]) * n + i[2] : -1;
+        const unsigned peers = __match_any_sync(FULL, cell);
+        const bool leader = ok && (__ffs(peers) - 1) == lane;
+        const unsigned most = __reduce_max_sync(FULL, (unsigned)__popc(peers));
         const int j[3] = {i[0] + 1 == n ? 0 : i[0] + 1, i[1] + 1 == n ? 0 : i[1] + 1, i[2] + 1 == n ? 0 : i[2] + 1};
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
             const int dx = c >> 2, dy = (c >> 1) & 1, dz = c & 1;
             const double w = (dx ? t[0] : 1.0 - t[0]) * (dy ? t[1] : 1.0 - t[1]) * (dz ? t[2] : 1.0 - t[2]);
-            const int key = ok ? ((dx ? j[0] : i[0]) * n + (dy ? j[1] : i[1])) * n + (dz ? j[2] : i[2]) : -1;
-            bool leader;
-            const float sum = warp_group_sum(key, (float)(mass * w), leader);
-            if (ok && leader) atomicAdd(rho + key, sum);
+            float v = (float)(mass * w);
+            if (most > 1) v = group_sum(peers, most, v);
+            if (leader) {
+                const int key = ((dx ? j[0] : i[0]) * n + (dy ? j[1] : i[1])) * n + (dz ? j[2] : i[2]);
+                atomicAdd(rho + key, v);
+            }
         }
     }
 }
