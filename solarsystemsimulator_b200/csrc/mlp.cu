@@ -269,6 +269,236 @@ __global__ void __launch_bounds__(WARPS_FWD * 32, 2) k_mlp_correct(const Pm3Part
     }
 }
 
+// ------------------------------------------- correction pass on tcgen05
+
+// The correction pass with layers 1 and 2 on the 5th-generation tensor
+// cores: one CTA of 128 threads owns a tile of 128 particles (one particle
+// per thread = one TMEM lane). Operands live in shared memory in the
+// canonical no-swizzle K-major layout (8-row x 16-byte core matrices,
+// K-adjacent core matrices 128 bytes apart, 8-row groups K*16 bytes apart);
+// one thread issues tcgen05.mma (M = N = 128, K = 16 per instruction) into
+// f32 accumulators in TMEM (256 columns: layer 1 | layer 2), tcgen05.commit
+// signals an mbarrier, and every thread reads its own row back with
+// tcgen05.ld for bias + SiLU (bf16 row of the next operand) or, after layer
+// 2, for the 128 x 3 output layer on the CUDA cores and the KDK epilogue.
+// The rounding points are those of the mma.sync kernels (bf16 inputs,
+// weights and hidden activations; f32 sums). Waits are bounded; the TMEM
+// columns are freed on every path.
+namespace tc {
+constexpr int ROWS = 128;
+constexpr int OFF_W1 = 0;                          // W1^T: 128 x 80 bf16 (B operand, rows = outputs)
+constexpr int OFF_W2 = OFF_W1 + HID * K1 * 2;      // W2^T: 128 x 128 bf16
+constexpr int OFF_X = OFF_W2 + HID * HID * 2;      // inputs: 128 x 80 bf16 (A operand, rows = particles)
+constexpr int OFF_H = OFF_X + ROWS * K1 * 2;       // hidden 1: 128 x 128 bf16
+constexpr int OFF_F = OFF_H + ROWS * HID * 2;      // f32: b1[128] b2[128] b3[8] W3[128][3]
+constexpr int N_F = HID + HID + K3 + HID * 3;
+constexpr int OFF_BAR = (OFF_F + N_F * 4 + 15) / 16 * 16;
+constexpr int SMEM = OFF_BAR + 16;
+constexpr uint32_t TMEM_COLS = 256;
+// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, N = 128, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                           ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ int canon(int r, int k, int K) {
+    return ((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// shared-memory matrix descriptor: start, leading offset (K direction) 128 B,
+// stride offset (8-row groups) K * 16 B, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, int K) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)((K * 16) >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_smem_to_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// D[tmem] (+)= A[M x K] B[N x K]^T over K / 16 instructions, then commit to bar
+__device__ __forceinline__ void mma_layer(uint32_t tmem_d, uint32_t sa, uint32_t sb, int K, uint64_t* bar) {
+    for (int kk = 0; kk < K / 16; ++kk) {
+        const uint64_t da = desc(sa + kk * 256, K), db = desc(sb + kk * 256, K);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            :: "r"(tmem_d), "l"(da), "l"(db), "r"(IDESC), "r"(kk) : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(sss_smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+}
+}  // namespace tc
+
+__global__ void __launch_bounds__(tc::ROWS, 2) k_mlp_correct_tc(const Pm3Parts s, const float* __restrict__ rho,
+                                                                int n, double inv_h, float inv_mean,
+                                                                const float* __restrict__ P, double out_scale,
+                                                                const Pm3Epi e, int* status) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    float* sFl = reinterpret_cast<float*>(sm + tc::OFF_F);
+    float* sb1 = sFl;
+    float* sb2 = sFl + HID;
+    float* sb3 = sFl + 2 * HID;
+    float* sW3 = sFl + 2 * HID + K3;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + tc::OFF_BAR);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + tc::OFF_BAR + 8);
+    // weights in the canonical layout (W^T: row = output unit, K = input)
+    for (int i = tid; i < K1 * HID; i += blockDim.x) {
+        const int k = i / HID, c = i % HID;
+        *reinterpret_cast<__nv_bfloat16*>(sm + tc::OFF_W1 + tc::canon(c, k, K1)) =
+            __float2bfloat16_rn(P[OFF_W1 + i]);
+    }
+    for (int i = tid; i < HID * HID; i += blockDim.x) {
+        const int k = i / HID, c = i % HID;
+        *reinterpret_cast<__nv_bfloat16*>(sm + tc::OFF_W2 + tc::canon(c, k, HID)) =
+            __float2bfloat16_rn(P[OFF_W2 + i]);
+    }
+    for (int i = tid; i < HID; i += blockDim.x) {
+        sb1[i] = P[OFF_B1 + i];
+        sb2[i] = P[OFF_B2 + i];
+        for (int c = 0; c < 3; ++c) sW3[i * 3 + c] = __bfloat162float(__float2bfloat16_rn(P[OFF_W3 + i * K3 + c]));
+    }
+    if (tid < K3) sb3[tid] = P[OFF_B3 + tid];
+    if (tid == 0) {
+        sss_mbar_init(bar, 1);
+        sss_fence_mbar_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(sss_smem_addr(tslot)), "r"(tc::TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t d1 = tmem, d2 = tmem + HID;
+    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    const uint32_t sX = sss_smem_addr(sm + tc::OFF_X), sH = sss_smem_addr(sm + tc::OFF_H);
+    const uint32_t sW1 = sss_smem_addr(sm + tc::OFF_W1), sW2 = sss_smem_addr(sm + tc::OFF_W2);
+    unsigned phase = 0;
+    const long long tiles = (s.n + tc::ROWS - 1) / tc::ROWS;
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long long p = tile * tc::ROWS + tid;
+        // ---- inputs of this thread's particle -> row tid of X
+        {
+            uint32_t row[K1 / 2];
+#pragma unroll
+            for (int q = 0; q < K1 / 2; ++q) row[q] = 0u;
+            if (p < s.n) {
+                int i[3];
+                double t[3];
+                for (int c = 0; c < 3; ++c) pm3_cell(s.x[c][p], inv_h, n, i[c], t[c]);
+                long long ox[4];
+                int oy[4], oz[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    int ix = i[0] + a - 1, iy = i[1] + a - 1, iz = i[2] + a - 1;
+                    ix += ix < 0 ? n : 0;
+                    ix -= ix >= n ? n : 0;
+                    iy += iy < 0 ? n : 0;
+                    iy -= iy >= n ? n : 0;
+                    iz += iz < 0 ? n : 0;
+                    iz -= iz >= n ? n : 0;
+                    ox[a] = (long long)ix * n * n;
+                    oy[a] = iy * n;
+                    oz[a] = iz;
+                }
+                float v[64];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) v[a * 16 + b * 4 + c] = __ldg(rho + ox[a] + oy[b] + oz[c]);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) row[q] = pack2(log1pf(v[2 * q] * inv_mean), log1pf(v[2 * q + 1] * inv_mean));
+                row[32] = pack2((float)(t[0] - 0.5), (float)(t[1] - 0.5));
+                row[33] = pack2((float)(t[2] - 0.5), 0.0f);
+            }
+#pragma unroll
+            for (int j = 0; j < K1 / 8; ++j)
+                *reinterpret_cast<uint4*>(sm + tc::OFF_X + tc::canon(tid, 8 * j, K1)) =
+                    make_uint4(row[4 * j], row[4 * j + 1], row[4 * j + 2], row[4 * j + 3]);
+        }
+        tc::fence_smem_to_async();
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
+        // ---- layer 1 on the tensor cores
+        if (tid == 0) tc::mma_layer(d1, sX, sW1, K1, bar);
+        int bad = sss_mbar_wait_bounded(bar, phase, status) ? 0 : 1;
+        phase ^= 1u;
+        if (__syncthreads_or(bad)) break;
+        tc::fence_after();
+#pragma unroll 1
+        for (int j = 0; j < HID / 32; ++j) {
+            float v[32];
+            tc::tmem_ld32(d1 + lane_base + 32 * j, v);
+            uint32_t h[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                h[q] = pack2(silu(v[2 * q] + sb1[32 * j + 2 * q]), silu(v[2 * q + 1] + sb1[32 * j + 2 * q + 1]));
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                *reinterpret_cast<uint4*>(sm + tc::OFF_H + tc::canon(tid, 32 * j + 8 * u, HID)) =
+                    make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
+        }
+        tc::fence_smem_to_async();
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
+        // ---- layer 2 on the tensor cores
+        if (tid == 0) tc::mma_layer(d2, sH, sW2, HID, bar);
+        bad = sss_mbar_wait_bounded(bar, phase, status) ? 0 : 1;
+        phase ^= 1u;
+        if (__syncthreads_or(bad)) break;
+        tc::fence_after();
+        float y0 = sb3[0], y1 = sb3[1], y2 = sb3[2];
+#pragma unroll 1
+        for (int j = 0; j < HID / 32; ++j) {
+            float v[32];
+            tc::tmem_ld32(d2 + lane_base + 32 * j, v);
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const int k = 32 * j + q;
+                const float hq = __bfloat162float(__float2bfloat16_rn(silu(v[q] + sb2[k])));
+                y0 = fmaf(hq, sW3[3 * k], y0);
+                y1 = fmaf(hq, sW3[3 * k + 1], y1);
+                y2 = fmaf(hq, sW3[3 * k + 2], y2);
+            }
+        }
+        if (p < s.n) {
+            const double ax = s.a[0][p] + out_scale * (double)y0;
+            const double ay = s.a[1][p] + out_scale * (double)y1;
+            const double az = s.a[2][p] + out_scale * (double)y2;
+            pm3_epilogue(s, e, p, ax, ay, az);
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(tc::TMEM_COLS)
+                     : "memory");
+}
+
 // forward on given input rows (sss_mlp_forward)
 __global__ void __launch_bounds__(WARPS_FWD * 32, 2) k_mlp_fwd(const uint16_t* __restrict__ X, long long rows,
                                                             const float* __restrict__ P,
@@ -692,13 +922,12 @@ extern "C" int sss_mlp_correct(sss_ctx* ctx, sss_pm3* p, const sss_pm3_particles
         if (!s->x[c] || !s->v[c] || !s->a[c]) return sss_set_err(ctx, SSS_ERR_ARG, "NULL particle array");
     if (!(rho_mean > 0.0)) return sss_set_err(ctx, SSS_ERR_ARG, "rho_mean must be > 0");
     if (mode < SSS_PM3_FORCE || mode > SSS_PM3_KICK_DRIFT) return sss_set_err(ctx, SSS_ERR_ARG, "bad mode");
-    const size_t smem = FWD_SMEM_U32 * sizeof(uint32_t);
-    SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(k_mlp_correct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long long tiles = (s->n + 15) / 16;
-    const int blocks = (int)std::min<long long>((tiles + WARPS_FWD - 1) / WARPS_FWD, (long long)ctx->num_sms * 2);
+    SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(k_mlp_correct_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM));
+    const long long tiles = (s->n + tc::ROWS - 1) / tc::ROWS;
+    const int blocks = (int)std::min<long long>(tiles, (long long)ctx->num_sms * 2);
     Pm3Epi e{mode, hdt, dt, p->box, snap};
-    k_mlp_correct<<<blocks, WARPS_FWD * 32, smem, (cudaStream_t)stream>>>(
-        pm3_parts(s), p->rho, p->n, p->n / p->box, (float)(1.0 / rho_mean), params, frags, out_scale, e);
+    k_mlp_correct_tc<<<blocks, tc::ROWS, tc::SMEM, (cudaStream_t)stream>>>(
+        pm3_parts(s), p->rho, p->n, p->n / p->box, (float)(1.0 / rho_mean), params, out_scale, e, ctx->d_status);
     SSS_LAUNCH_CHECK(ctx, "k_mlp_correct");
     return SSS_OK;
 }

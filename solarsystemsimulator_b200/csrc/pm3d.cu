@@ -92,44 +92,54 @@ __global__ void __launch_bounds__(256) k_deposit3(const Pm3Parts s, int n, doubl
     }
 }
 
+// Per-axis tables of the spectrum kernel, index i of a full axis (frequency
+// f = i for i < n/2, i - n otherwise): kd = k_i (0 on the Nyquist index:
+// the derivative of that mode is dropped so the spectra stay Hermitian),
+// k2 = k_i^2, fac = sinc(pi f / n)^(-2 deconv) * exp(-k_i^2 rs2). The
+// Green's function factorises: W(k)^-deconv e^{-k^2 rs2} = fac_x fac_y fac_z.
+// The half axis of the real transform (iz <= n/2) reads the same tables.
+__global__ void k_spectrum_tables(int n, double box, int deconv, double rs2, double* __restrict__ tab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int f = i < n / 2 ? i : i - n;
+    const double k = 2.0 * 3.14159265358979323846 / box * f;
+    double fac = 1.0;
+    if (f != 0) {
+        const double a = (double)f / (double)n;
+        const double sinc = sinpi(a) / (3.14159265358979323846 * a);
+        const double s2 = sinc * sinc;
+        for (int q = 0; q < deconv; ++q) fac /= s2;
+    }
+    if (rs2 > 0.0) fac *= exp(-k * k * rs2);
+    tab[i] = (i == n / 2) ? 0.0 : k;
+    tab[n + i] = k * k;
+    tab[2 * n + i] = fac;
+}
+
 // Acceleration spectra from the density spectrum (half-complex layout,
-// index (ix, iy, iz) with iz in [0, n/2]); see the file comment.
-__global__ void __launch_bounds__(256) k_spectrum3(const float2* __restrict__ rk, int n, double box, double G,
-                                                   int deconv, double rs2, float2* __restrict__ ak) {
+// index (ix, iy, iz), iz in [0, n/2]); grid (z blocks, n, n):
+// a_d = -i k_d phi, phi = -4 pi G rho_k fac / k^2  ->  a_d = i k_d c rho_k
+// with c = 4 pi G fac / (k^2 n^3) (the inverse transform's 1/n^3 folded in).
+__global__ void __launch_bounds__(128) k_spectrum3(const float2* __restrict__ rk, int n, double cscale,
+                                                   const double* __restrict__ tab, float2* __restrict__ ak) {
     const int nh = n / 2 + 1;
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iz >= nh) return;
+    const int iy = blockIdx.y, ix = blockIdx.z;
     const long long m = (long long)n * n * nh;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m) return;
-    const int iz = (int)(t % nh);
-    const int iy = (int)((t / nh) % n);
-    const int ix = (int)(t / ((long long)nh * n));
-    const int fx = ix < n / 2 ? ix : ix - n;
-    const int fy = iy < n / 2 ? iy : iy - n;
-    const int fz = iz;
+    const long long t = ((long long)ix * n + iy) * nh + iz;
     float2 out[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    if (fx != 0 || fy != 0 || fz != 0) {
-        const double two_pi_l = 2.0 * 3.14159265358979323846 / box;
-        const double kx = two_pi_l * fx, ky = two_pi_l * fy, kz = two_pi_l * fz;
-        const double k2 = kx * kx + ky * ky + kz * kz;
-        // sinc(k_d h / 2) = sin(pi f / n) / (pi f / n)
-        auto sinc = [n](int f) -> double {
-            if (f == 0) return 1.0;
-            const double a = (double)f / (double)n;
-            return sinpi(a) / (3.14159265358979323846 * a);
-        };
-        const double s3 = sinc(fx) * sinc(fy) * sinc(fz);
-        const double w = s3 * s3;                   // CIC window W(k)
-        double wd = 1.0;
-        for (int q = 0; q < deconv; ++q) wd *= w;
-        const double nn = (double)n * n * n;
-        // a_d = -i k_d phi, phi = -4 pi G rho_k e^{-k^2 rs^2} / (k^2 W^deconv) -> a_d = i k_d c rho_k
-        const double filt = rs2 > 0.0 ? exp(-k2 * rs2) : 1.0;
-        const double c = 4.0 * 3.14159265358979323846 * G * filt / (k2 * wd * nn);
+    if (ix != 0 || iy != 0 || iz != 0) {
+        const double* kd = tab;
+        const double* k2t = tab + n;
+        const double* fac = tab + 2 * n;
+        const double k2 = k2t[ix] + k2t[iy] + k2t[iz];
+        const double c = cscale * (fac[ix] * fac[iy] * fac[iz]) / k2;
         const float2 r = rk[t];
-        const double kd[3] = {fx == -n / 2 ? 0.0 : kx, fy == -n / 2 ? 0.0 : ky, fz == n / 2 ? 0.0 : kz};
+        const double kk[3] = {kd[ix], kd[iy], kd[iz]};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const double f = kd[d] * c;
+            const double f = kk[d] * c;
             out[d] = make_float2((float)(-f * (double)r.y), (float)(f * (double)r.x));
         }
     }
@@ -177,6 +187,7 @@ void pm3_free(sss_pm3* p) {
     cudaFree(p->rk);
     cudaFree(p->ak);
     cudaFree(p->acc);
+    cudaFree(p->tab);
     free(p);
 }
 
@@ -209,6 +220,8 @@ extern "C" int sss_pm3_create(sss_ctx* ctx, int mesh_n, double box, sss_pm3** ou
     e = e ? e : cudaMalloc(&p->rk, m * sizeof(float2));
     e = e ? e : cudaMalloc(&p->ak, 3 * m * sizeof(float2));
     e = e ? e : cudaMalloc(&p->acc, 3 * n3 * sizeof(float));
+    e = e ? e : cudaMalloc(&p->tab, 3 * (size_t)mesh_n * sizeof(double));
+    p->tab_deconv = -1;
     if (e != cudaSuccess) {
         pm3_free(p);
         return sss_cuda_err(ctx, e, "cudaMalloc (pm3)");
@@ -267,8 +280,16 @@ extern "C" int sss_pm3_solve(sss_pm3* p, double G, int deconv, double r_split, v
     cufftSetStream(p->inv3, st);
     cufftResult r = cufftExecR2C(p->fwd, p->rho, (cufftComplex*)p->rk);
     if (r != CUFFT_SUCCESS) return cufft_err(ctx, r, "cufftExecR2C");
-    const long long m = (long long)p->n * p->n * (p->n / 2 + 1);
-    k_spectrum3<<<blocks_for(m, 256), 256, 0, st>>>(p->rk, p->n, p->box, G, deconv, r_split * r_split, p->ak);
+    const double rs2 = r_split * r_split;
+    if (p->tab_deconv != deconv || p->tab_rs2 != rs2) {
+        k_spectrum_tables<<<blocks_for(p->n, 128), 128, 0, st>>>(p->n, p->box, deconv, rs2, p->tab);
+        SSS_LAUNCH_CHECK(ctx, "k_spectrum_tables");
+        p->tab_deconv = deconv;
+        p->tab_rs2 = rs2;
+    }
+    const int nh = p->n / 2 + 1;
+    const double cscale = 4.0 * 3.14159265358979323846 * G / ((double)p->n * p->n * p->n);
+    k_spectrum3<<<dim3((nh + 127) / 128, p->n, p->n), 128, 0, st>>>(p->rk, p->n, cscale, p->tab, p->ak);
     SSS_LAUNCH_CHECK(ctx, "k_spectrum3");
     r = cufftExecC2R(p->inv3, (cufftComplex*)p->ak, p->acc);
     if (r != CUFFT_SUCCESS) return cufft_err(ctx, r, "cufftExecC2R");

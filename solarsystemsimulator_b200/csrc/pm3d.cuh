@@ -17,6 +17,9 @@ struct sss_pm3 {
     float* acc;         // 3 n^3 acceleration meshes (contiguous)
     cufftHandle fwd;    // R2C n^3
     cufftHandle inv3;   // C2R n^3, batch 3
+    double* tab;        // per-axis tables of the spectrum kernel: kd[n], k2[n], fac[n]
+    int tab_deconv;     // parameters the tables were built for (-1: none yet)
+    double tab_rs2;
 };
 
 // Particle state passed by value to kernels.

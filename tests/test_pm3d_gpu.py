@@ -187,18 +187,29 @@ def test_adam_matches_oracle(mods):
     assert np.abs(net.params.double().cpu().numpy() - p).max() <= 1e-6
 
 
-def test_correction_pass_adds_the_network_output(mods):
+@pytest.mark.parametrize("n", [10000, 128 * 37])
+def test_correction_pass_adds_the_network_output(mods, n):
+    # the correction pass (tcgen05, one particle per TMEM lane) against the
+    # mma.sync forward on the same inputs: both round at the same points
+    # (bf16 inputs, weights, hidden activations; f32 sums) but sum in a
+    # different order, so a hidden value may round to its bf16 neighbour
     _lib, pm3d, mlp, _ = mods
-    pos, vel, m = _cloud(10000, 11)
+    pos, vel, m = _cloud(n, 11)
     pm = pm3d.PMPeriodic3D(32, 1.0, 1.0)
     st = pm.load_state(pos, vel, m)
     net = mlp.ShortRangeMLP(0, seed=5)
     net.out_scale = 0.25
     a_pm = pm.forces(st).clone()
     a = pm.forces(st, net).clone()
-    X = net.features(pm, st["parts"], torch.arange(10000, device="cuda"), st["rho_mean"])
+    X = net.features(pm, st["parts"], torch.arange(n, device="cuda"), st["rho_mean"])
     y = net.forward(X).double().T * 0.25
-    assert float((a - a_pm - y).abs().max()) <= 1e-12 + 1e-6 * float(y.abs().max())
+    err = (a - a_pm - y).abs()
+    rms = float(torch.sqrt(torch.mean(y * y)))
+    assert float(err.median()) <= 1e-4 * rms
+    assert float(err.max()) <= 2e-2 * rms
+    ref, _ = o.forward(net.params.double().cpu().numpy(), _x_to_f64(X))
+    e2 = np.abs((a - a_pm).cpu().numpy().T / 0.25 - ref)
+    assert np.median(e2) <= 1e-4 * rms / 0.25 and e2.max() <= 2e-2 * rms / 0.25
 
 
 def test_training_reduces_the_loss(mods):
