@@ -53,9 +53,11 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the fast exponential and division (both a few
+// ulp; the result is rounded to bf16 or multiplied into a bf16 delta)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
+    const float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -236,39 +238,6 @@ __device__ __forceinline__ void stage_forward_weights(const float* __restrict__ 
     if (threadIdx.x < K3) sB[2 * HID + threadIdx.x] = P[OFF_B3 + threadIdx.x];
 }
 
-// the correction pass over all particles (sss_mlp_correct)
-__global__ void __launch_bounds__(WARPS_FWD * 32, 2) k_mlp_correct(const Pm3Parts s, const float* __restrict__ rho,
-                                                                int n, double inv_h, float inv_mean,
-                                                                const float* __restrict__ P,
-                                                                const uint32_t* __restrict__ F, double out_scale,
-                                                                const Pm3Epi e) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    uint32_t* sF = smem;
-    float* sB = reinterpret_cast<float*>(smem + FR_W3T);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* Xs = smem + FR_W3T + 2 * HID + K3 + warp * (16 * XS + 16 * 4);
-    float* Ys = reinterpret_cast<float*>(Xs + 16 * XS);
-    stage_forward_weights(P, F, sF, sB);
-    __syncthreads();
-    const long long tiles = (s.n + 15) / 16;
-    for (long long tile = (long long)blockIdx.x * WARPS_FWD + warp; tile < tiles;
-         tile += (long long)gridDim.x * WARPS_FWD) {
-        const long long p = tile * 16 + (lane & 15);
-        particle_features(rho, n, inv_h, inv_mean, s, p < s.n ? p : -1, lane >> 4,
-                          reinterpret_cast<uint16_t*>(Xs + (lane & 15) * XS));
-        __syncwarp();
-        tile_forward(sF, sB, Xs, Ys);
-        __syncwarp();
-        if (lane < 16 && p < s.n) {
-            const double ax = s.a[0][p] + out_scale * (double)Ys[lane * 4 + 0];
-            const double ay = s.a[1][p] + out_scale * (double)Ys[lane * 4 + 1];
-            const double az = s.a[2][p] + out_scale * (double)Ys[lane * 4 + 2];
-            pm3_epilogue(s, e, p, ax, ay, az);
-        }
-        __syncwarp();
-    }
-}
-
 // ------------------------------------------- correction pass on tcgen05
 
 // The correction pass with layers 1 and 2 on the 5th-generation tensor
@@ -328,7 +297,7 @@ __device__ __forceinline__ void mma_layer(uint32_t tmem_d, uint32_t sa, uint32_t
                  :: "r"(sss_smem_addr(bar)) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t addr, float (&v)[32]) {
     uint32_t r[32];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -338,11 +307,54 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 }  // namespace tc
+
+// inputs of particle p (p >= n: zeros) into row r of the canonical X tile
+__device__ __forceinline__ void tc_features(const Pm3Parts& s, const float* __restrict__ rho, int n, double inv_h,
+                                            float inv_mean, long long p, int r, uint8_t* sx) {
+    uint32_t row[K1 / 2];
+#pragma unroll
+    for (int q = 0; q < K1 / 2; ++q) row[q] = 0u;
+    if (p < s.n) {
+        int i[3];
+        double t[3];
+        for (int c = 0; c < 3; ++c) pm3_cell(s.x[c][p], inv_h, n, i[c], t[c]);
+        long long ox[4];
+        int oy[4], oz[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            int ix = i[0] + a - 1, iy = i[1] + a - 1, iz = i[2] + a - 1;
+            ix += ix < 0 ? n : 0;
+            ix -= ix >= n ? n : 0;
+            iy += iy < 0 ? n : 0;
+            iy -= iy >= n ? n : 0;
+            iz += iz < 0 ? n : 0;
+            iz -= iz >= n ? n : 0;
+            ox[a] = (long long)ix * n * n;
+            oy[a] = iy * n;
+            oz[a] = iz;
+        }
+        float v[64];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) v[a * 16 + b * 4 + c] = __ldg(rho + ox[a] + oy[b] + oz[c]);
+#pragma unroll
+        for (int q = 0; q < 32; ++q) row[q] = pack2(log1pf(v[2 * q] * inv_mean), log1pf(v[2 * q + 1] * inv_mean));
+        row[32] = pack2((float)(t[0] - 0.5), (float)(t[1] - 0.5));
+        row[33] = pack2((float)(t[2] - 0.5), 0.0f);
+    }
+#pragma unroll
+    for (int j = 0; j < K1 / 8; ++j)
+        *reinterpret_cast<uint4*>(sx + tc::canon(r, 8 * j, K1)) =
+            make_uint4(row[4 * j], row[4 * j + 1], row[4 * j + 2], row[4 * j + 3]);
+}
 
 __global__ void __launch_bounds__(tc::ROWS, 2) k_mlp_correct_tc(const Pm3Parts s, const float* __restrict__ rho,
                                                                 int n, double inv_h, float inv_mean,
@@ -394,49 +406,10 @@ __global__ void __launch_bounds__(tc::ROWS, 2) k_mlp_correct_tc(const Pm3Parts s
     const uint32_t sW1 = sss_smem_addr(sm + tc::OFF_W1), sW2 = sss_smem_addr(sm + tc::OFF_W2);
     unsigned phase = 0;
     const long long tiles = (s.n + tc::ROWS - 1) / tc::ROWS;
+    if (blockIdx.x < tiles) tc_features(s, rho, n, inv_h, inv_mean, (long long)blockIdx.x * tc::ROWS + tid, tid,
+                                        sm + tc::OFF_X);
     for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const long long p = tile * tc::ROWS + tid;
-        // ---- inputs of this thread's particle -> row tid of X
-        {
-            uint32_t row[K1 / 2];
-#pragma unroll
-            for (int q = 0; q < K1 / 2; ++q) row[q] = 0u;
-            if (p < s.n) {
-                int i[3];
-                double t[3];
-                for (int c = 0; c < 3; ++c) pm3_cell(s.x[c][p], inv_h, n, i[c], t[c]);
-                long long ox[4];
-                int oy[4], oz[4];
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    int ix = i[0] + a - 1, iy = i[1] + a - 1, iz = i[2] + a - 1;
-                    ix += ix < 0 ? n : 0;
-                    ix -= ix >= n ? n : 0;
-                    iy += iy < 0 ? n : 0;
-                    iy -= iy >= n ? n : 0;
-                    iz += iz < 0 ? n : 0;
-                    iz -= iz >= n ? n : 0;
-                    ox[a] = (long long)ix * n * n;
-                    oy[a] = iy * n;
-                    oz[a] = iz;
-                }
-                float v[64];
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) v[a * 16 + b * 4 + c] = __ldg(rho + ox[a] + oy[b] + oz[c]);
-#pragma unroll
-                for (int q = 0; q < 32; ++q) row[q] = pack2(log1pf(v[2 * q] * inv_mean), log1pf(v[2 * q + 1] * inv_mean));
-                row[32] = pack2((float)(t[0] - 0.5), (float)(t[1] - 0.5));
-                row[33] = pack2((float)(t[2] - 0.5), 0.0f);
-            }
-#pragma unroll
-            for (int j = 0; j < K1 / 8; ++j)
-                *reinterpret_cast<uint4*>(sm + tc::OFF_X + tc::canon(tid, 8 * j, K1)) =
-                    make_uint4(row[4 * j], row[4 * j + 1], row[4 * j + 2], row[4 * j + 3]);
-        }
         tc::fence_smem_to_async();
         tc::fence_before();
         __syncthreads();
@@ -448,17 +421,24 @@ __global__ void __launch_bounds__(tc::ROWS, 2) k_mlp_correct_tc(const Pm3Parts s
         if (__syncthreads_or(bad)) break;
         tc::fence_after();
 #pragma unroll 1
-        for (int j = 0; j < HID / 32; ++j) {
-            float v[32];
-            tc::tmem_ld32(d1 + lane_base + 32 * j, v);
-            uint32_t h[16];
+        for (int j2 = 0; j2 < HID / 64; ++j2) {
+            float v[2][32];
+            tc::tmem_ld32_nowait(d1 + lane_base + 64 * j2, v[0]);
+            tc::tmem_ld32_nowait(d1 + lane_base + 64 * j2 + 32, v[1]);
+            tc::tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 16; ++q)
-                h[q] = pack2(silu(v[2 * q] + sb1[32 * j + 2 * q]), silu(v[2 * q + 1] + sb1[32 * j + 2 * q + 1]));
+            for (int hh = 0; hh < 2; ++hh) {
+                const int j = 2 * j2 + hh;
+                uint32_t h[16];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                *reinterpret_cast<uint4*>(sm + tc::OFF_H + tc::canon(tid, 32 * j + 8 * u, HID)) =
-                    make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
+                for (int q = 0; q < 16; ++q)
+                    h[q] = pack2(silu(v[hh][2 * q] + sb1[32 * j + 2 * q]),
+                                 silu(v[hh][2 * q + 1] + sb1[32 * j + 2 * q + 1]));
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    *reinterpret_cast<uint4*>(sm + tc::OFF_H + tc::canon(tid, 32 * j + 8 * u, HID)) =
+                        make_uint4(h[4 * u], h[4 * u + 1], h[4 * u + 2], h[4 * u + 3]);
+            }
         }
         tc::fence_smem_to_async();
         tc::fence_before();
@@ -466,19 +446,25 @@ __global__ void __launch_bounds__(tc::ROWS, 2) k_mlp_correct_tc(const Pm3Parts s
         tc::fence_after();
         // ---- layer 2 on the tensor cores
         if (tid == 0) tc::mma_layer(d2, sH, sW2, HID, bar);
+        // the input tile is free once layer 1 has completed: gather the next
+        // tile's inputs while layer 2 runs
+        if (tile + gridDim.x < tiles)
+            tc_features(s, rho, n, inv_h, inv_mean, (tile + gridDim.x) * tc::ROWS + tid, tid, sm + tc::OFF_X);
         bad = sss_mbar_wait_bounded(bar, phase, status) ? 0 : 1;
         phase ^= 1u;
         if (__syncthreads_or(bad)) break;
         tc::fence_after();
         float y0 = sb3[0], y1 = sb3[1], y2 = sb3[2];
 #pragma unroll 1
-        for (int j = 0; j < HID / 32; ++j) {
-            float v[32];
-            tc::tmem_ld32(d2 + lane_base + 32 * j, v);
+        for (int j2 = 0; j2 < HID / 64; ++j2) {
+            float v[2][32];
+            tc::tmem_ld32_nowait(d2 + lane_base + 64 * j2, v[0]);
+            tc::tmem_ld32_nowait(d2 + lane_base + 64 * j2 + 32, v[1]);
+            tc::tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                const int k = 32 * j + q;
-                const float hq = __bfloat162float(__float2bfloat16_rn(silu(v[q] + sb2[k])));
+            for (int q = 0; q < 64; ++q) {
+                const int k = 64 * j2 + q;
+                const float hq = __bfloat162float(__float2bfloat16_rn(silu(v[q >> 5][q & 31] + sb2[k])));
                 y0 = fmaf(hq, sW3[3 * k], y0);
                 y1 = fmaf(hq, sW3[3 * k + 1], y1);
                 y2 = fmaf(hq, sW3[3 * k + 2], y2);
