@@ -239,6 +239,41 @@ int  sss_pm2d_kick_drift(sss_pm2d* p, double* x, double* y, double* vx, double* 
 /* out[i] = (float)a[i] (snapshot rows, :274-280) */
 int  sss_pm2d_to_f32(sss_pm2d* p, const double* a, int64_t n, float* out, void* stream);
 
+/* ------------------------------------------------- collision response
+ *
+ * The per-sample collision analysis of the asteroid films (2-D), on the
+ * device. Arrays are device arrays over the n bodies of a sample: f32
+ * snapshot rows x, y, vx, vy; f32 contact radii rr; u8 visibility and
+ * asteroid flags; f64 masses and radii. Both calls are synchronous (counts
+ * return to the host).
+ *
+ * sss_collide_sweep replaces analyze_merge (film_producer.py:707-779): the
+ * alive massive bodies m_idx[0..m_count) (vis and mass > 0) against every
+ * alive body, the segment from the previous positions (px, py) to this
+ * sample and the segment extrapolated by dt_y, in f32 as the reference;
+ * pairs receives int32 triples (massive, body, fraction bits as f32) in the
+ * reference's row-major order, runaways the bodies with v^2 > 9 v_esc^2
+ * from the massive barycentre (ascending). SSS_ERR_CAPACITY when more than
+ * cap_pairs / cap_run were found (the counts tell how many).
+ *
+ * sss_collide_bounce replaces bounce_deltas (:916-1019) for the broadphase
+ * hits (sss_broadphase triples, any order; n <= SSS_COLLIDE_MAX_BODIES): hits
+ * sorted into the reference's order, at most one hit per body (greedy in
+ * that order), impulse with restitution e and overlap push in f64.
+ * pairs_out receives the active hits as int32 (a, b) pairs in order
+ * (capacity n_hits pairs); touched_out the bodies they touch, ascending
+ * (capacity min(n, 2 n_hits)), deltas_out their (dx, dy, dvx, dvy). */
+#define SSS_COLLIDE_MAX_BODIES 1600000
+int sss_collide_sweep(sss_ctx* ctx, int64_t n, const float* gx, const float* gy, const float* gvx, const float* gvy,
+                      const float* px, const float* py, const float* rr, const unsigned char* vis,
+                      const unsigned char* is_ast, const double* mass, const int64_t* m_idx, int m_count,
+                      double dt_y, double G, int* pairs, int64_t cap_pairs, int* runaways, int64_t cap_run,
+                      int64_t* n_pairs, int64_t* n_run, void* stream);
+int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const float* y, const float* vx, const float* vy,
+                       const double* real_r, const double* mass, const int* hits, int64_t n_hits, double dt_y,
+                       double e, int* pairs_out, int64_t* touched_out, double* deltas_out, int64_t* n_act,
+                       int64_t* n_touched, void* stream);
+
 /* ------------------------------------------------ particle mesh, 3-D periodic
  *
  * The reference's PM cycle (TODO.md:225-253; 2-D code pm_kernel.py:63-154)

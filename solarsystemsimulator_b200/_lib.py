@@ -73,6 +73,7 @@ PM3_KICK_DRIFT = 2
 MLP_N_PARAMS = 27912
 MLP_N_FRAGS = 23040
 MLP_IN_PAD = 80
+COLLIDE_MAX_BODIES = 1600000
 
 # name -> (restype, argtypes); every symbol include/sss.h declares
 SIGNATURES = {
@@ -111,6 +112,12 @@ SIGNATURES = {
     "sss_batched_launch": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp, _dp,
                                           _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp]),
+    "sss_collide_sweep": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                         ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _c_i64, _dp, _c_i64,
+                                         ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64), _vp]),
+    "sss_collide_bounce": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
+                                          ctypes.c_double, _dp, _dp, _dp, ctypes.POINTER(_c_i64),
+                                          ctypes.POINTER(_c_i64), _vp]),
     "sss_pm3_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),
     "sss_pm3_destroy": (None, [_vp]),
     "sss_pm3_meshes": (ctypes.c_int, [_vp, ctypes.POINTER(_dp), ctypes.POINTER(_dp)]),

@@ -38,11 +38,11 @@ def _dev_u8(a, device) -> torch.Tensor:
     return torch.as_tensor(np.ascontiguousarray(np.asarray(a) != 0, dtype=np.uint8)).to(device)
 
 
-def bounce_hits(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, rr, is_ast=None, vis=None,
-                lo: float = -np.inf, hi: float = np.inf, device: int = 0):
-    """Colliding asteroid pairs in the stripe [lo, hi) (film_producer.py:223-317).
-
-    Returns ((i, j) int64 host arrays or None, candidate-pair count)."""
+def bounce_hits_device(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, rr, is_ast=None, vis=None,
+                       lo: float = -np.inf, hi: float = np.inf, device: int = 0):
+    """The hit list on the device, unsorted: (int32 (k, 3) tensor of
+    (offset index, a, b), k, candidate-pair count) — the input of the
+    device-side bounce response (sss_collide_bounce sorts it)."""
     dev = torch.device("cuda", device)
     x, y, vx, vy = (_dev_f32(a, dev) for a in (gx, gy, gvx, gvy))
     n = x.numel()
@@ -66,12 +66,22 @@ def bounce_hits(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, rr, is_
         ctx.check(rc)
         break
     k = int(nh.value)
+    return buf[:k], k, int(nc.value)
+
+
+def bounce_hits(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, rr, is_ast=None, vis=None,
+                lo: float = -np.inf, hi: float = np.inf, device: int = 0):
+    """Colliding asteroid pairs in the stripe [lo, hi) (film_producer.py:223-317).
+
+    Returns ((i, j) int64 host arrays or None, candidate-pair count)."""
+    buf, k, nc = bounce_hits_device(gx, gy, gvx, gvy, dt_y, h, halo, rr=rr, is_ast=is_ast, vis=vis, lo=lo, hi=hi,
+                                    device=device)
     if k == 0:
-        return None, int(nc.value)
-    h_ = buf[:k].cpu().numpy().astype(np.int64)
+        return None, nc
+    h_ = buf.cpu().numpy().astype(np.int64)
     order = np.lexsort((h_[:, 2], h_[:, 1], h_[:, 0]))      # (offset, a, b): the reference's order
     h_ = h_[order]
-    return (h_[:, 1].copy(), h_[:, 2].copy()), int(nc.value)
+    return (h_[:, 1].copy(), h_[:, 2].copy()), nc
 
 
 class Erkennungskarte:

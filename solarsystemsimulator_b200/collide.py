@@ -1,0 +1,182 @@
+"""Collision response of the asteroid films on one B200: the per-sample
+analysis of the reference's film producer with its array parts on the device.
+
+    cr = CollisionResponse(mass, real_r, vis, is_ast, is_star_bh, m_idx)
+    pairs, runaways = cr.analyze_merge(g, dt_y)          # analyze_merge, film_producer.py:707-779
+    res = cr.bounce_deltas(g, hits_dev, n_hits, dt_y)    # bounce_deltas, :916-1019
+    events, shatter = cr.apply_merges(sim, st, sample, pairs, runaways, k_ev)   # apply_merges, :781-861
+    cr.apply_bounce(sim, st, res)                        # apply_bounce, :1021-1040 (deltas on the device)
+
+`g` is the sample on the device as f32 rows (4, n) [x|y|vx|vy] (the row the
+detection card holds); `sample` the same row on the host (f32, 4n). The
+host mirrors mass / real_r / vis are updated by apply_merges exactly as the
+reference's are; `refresh()` copies them to the device mirrors (the
+reference's stammdaten_laden, :636-643), which the caller does after a batch
+whose merges changed them.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+G_AU = 4 * np.pi * np.pi
+BOUNCE_E = 0.6            # restitution (film_producer.py:47)
+SHATTER_V_ESC = 1.5       # body x body impacts at >= 1.5 v_esc stop the film for the client's shatter
+
+
+class CollisionResponse:
+    def __init__(self, mass, real_r, vis, is_ast, is_star_bh=None, m_idx=None, device: int = 0, G: float = G_AU,
+                 bounce_e: float = BOUNCE_E, shatter: bool = True):
+        self.device = int(device)
+        self.ctx = _lib.context(device)
+        self.dev = torch.device("cuda", self.device)
+        self.mass = np.array(mass, dtype=np.float64, copy=True)
+        self.real_r = np.array(real_r, dtype=np.float64, copy=True)
+        self.vis = np.array(vis, dtype=np.uint8, copy=True)
+        self.is_ast = np.asarray(is_ast) != 0
+        self.n = len(self.mass)
+        self.is_star_bh = (np.zeros(self.n, bool) if is_star_bh is None else np.asarray(is_star_bh) != 0)
+        self.m_idx = np.flatnonzero(~self.is_ast) if m_idx is None else np.asarray(m_idx, np.int64)
+        if len(self.m_idx) > 64:
+            raise ValueError(f"zu viele massive Koerper: {len(self.m_idx)} > 64")
+        self.G = float(G)
+        self.e = float(bounce_e)
+        self.shatter = bool(shatter)
+        self.prev = None                # (px, py) device f32 of the previous analysed sample
+        self.d_ast = torch.as_tensor(self.is_ast.astype(np.uint8)).to(self.dev)
+        self.d_midx = torch.as_tensor(self.m_idx.astype(np.int64)).to(self.dev)
+        self.refresh()
+
+    def refresh(self) -> None:
+        """Copy the host mirrors (vis, radii, masses) to the device."""
+        self.d_vis = torch.as_tensor(self.vis).to(self.dev)
+        self.d_rr32 = torch.as_tensor(self.real_r.astype(np.float32)).to(self.dev)
+        self.d_rr = torch.as_tensor(self.real_r).to(self.dev)
+        self.d_mass = torch.as_tensor(self.mass).to(self.dev)
+
+    def _s(self):
+        return ctypes.c_void_p(_lib.stream_handle(self.device))
+
+    # ---------------------------------------------------------- analysis
+    def analyze_merge(self, g: torch.Tensor, dt_y: float, cap: int = 65536):
+        """Merge candidates [(massive, body, frac)] and runaways (int64
+        array or None) of the sample g (device f32 (4, n))."""
+        g = g.contiguous()
+        n = self.n
+        px, py = (g[0], g[1]) if self.prev is None else self.prev
+        pairs = torch.empty((cap, 3), dtype=torch.int32, device=self.dev)
+        run = torch.empty(max(n, 1), dtype=torch.int32, device=self.dev)
+        npair, nrun = ctypes.c_int64(), ctypes.c_int64()
+        with torch.cuda.device(self.device):
+            rc = self.ctx.lib.sss_collide_sweep(
+                self.ctx.ptr, n, g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(), g[3].data_ptr(),
+                px.data_ptr(), py.data_ptr(), self.d_rr32.data_ptr(), self.d_vis.data_ptr(), self.d_ast.data_ptr(),
+                self.d_mass.data_ptr(), self.d_midx.data_ptr(), len(self.m_idx), float(dt_y), self.G,
+                pairs.data_ptr(), cap, run.data_ptr(), n, ctypes.byref(npair), ctypes.byref(nrun), self._s())
+        self.ctx.check(rc)
+        self.prev = (g[0].clone(), g[1].clone())
+        k = npair.value
+        out = []
+        if k:
+            p = pairs[:k].cpu().numpy()
+            fr = p[:, 2].copy().view(np.float32)
+            out = [(int(a), int(b), float(f)) for a, b, f in zip(p[:, 0], p[:, 1], fr)]
+        runaways = run[:nrun.value].cpu().numpy().astype(np.int64) if nrun.value else None
+        return out, runaways
+
+    def bounce_deltas(self, g: torch.Tensor, hits: torch.Tensor, n_hits: int, dt_y: float):
+        """None or (hi, hj, touched, deltas) as device tensors: the active
+        hits in order (int32), the touched bodies ascending (int64) and their
+        (dx, dy, dvx, dvy) (f64)."""
+        if n_hits <= 0:
+            return None
+        g = g.contiguous()
+        n = self.n
+        pairs = torch.empty((n_hits, 2), dtype=torch.int32, device=self.dev)
+        cap_t = min(n, 2 * n_hits)
+        touched = torch.empty(cap_t, dtype=torch.int64, device=self.dev)
+        deltas = torch.empty((cap_t, 4), dtype=torch.float64, device=self.dev)
+        na, nt = ctypes.c_int64(), ctypes.c_int64()
+        with torch.cuda.device(self.device):
+            rc = self.ctx.lib.sss_collide_bounce(
+                self.ctx.ptr, n, g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(), g[3].data_ptr(),
+                self.d_rr.data_ptr(), self.d_mass.data_ptr(), hits.data_ptr(), int(n_hits), float(dt_y), self.e,
+                pairs.data_ptr(), touched.data_ptr(), deltas.data_ptr(), ctypes.byref(na), ctypes.byref(nt),
+                self._s())
+        self.ctx.check(rc)
+        if na.value == 0:
+            return None
+        return pairs[:na.value, 0], pairs[:na.value, 1], touched[:nt.value], deltas[:nt.value]
+
+    # ---------------------------------------------------------- application
+    def apply_merges(self, sim, st, sample: np.ndarray, pairs, runaways, k_ev: int = 0, contact: dict | None = None):
+        """Apply merges and runaway removals in order (apply_merges,
+        film_producer.py:781-861) to the simulation and the host mirrors.
+        Returns (events, shatter): events (a, b, new_mass, kind, frac, x, y),
+        kind 0 merge / 2 runaway; shatter (a, b, frac) when a body x body
+        impact at >= 1.5 v_esc stopped the processing (the reference freezes
+        the film there and leaves the fragments to its client)."""
+        n = self.n
+        sx, sy = sample[0:n], sample[n:2 * n]
+        svx, svy = sample[2 * n:3 * n], sample[3 * n:4 * n]
+        mass, vis, rr = self.mass, self.vis, self.real_r
+        events = []
+        contact = {} if contact is None else contact
+        for mi, j, frac in pairs:
+            tk = contact.pop(j, None)
+            if tk is not None:
+                f_kern = tk - (k_ev + 1)
+                if -1.0 <= f_kern <= 1.0:
+                    frac = f_kern
+            if (self.shatter and not self.is_ast[mi] and not self.is_ast[j] and not self.is_star_bh[mi]
+                    and not self.is_star_bh[j] and vis[mi] and vis[j] and mass[mi] > 0 and mass[j] > 0):
+                v_imp = float(np.hypot(svx[j] - svx[mi], svy[j] - svy[mi]))
+                touch = max(1e-12, rr[mi] + rr[j])
+                v_esc = float(np.sqrt(2.0 * self.G * (mass[mi] + mass[j]) / touch))
+                if v_imp >= SHATTER_V_ESC * v_esc:
+                    return events, (int(mi), int(j), frac)
+            if not vis[mi] or not vis[j] or mass[mi] <= 0:
+                continue
+            a, b = (mi, j) if mass[mi] >= mass[j] else (j, mi)
+            m_a, m_b = mass[a], mass[b]
+            m_ges = m_a + m_b
+            if m_ges <= 0:
+                continue
+            nx = (sx[a] * m_a + sx[b] * m_b) / m_ges
+            ny = (sy[a] * m_a + sy[b] * m_b) / m_ges
+            nvx = (svx[a] * m_a + svx[b] * m_b) / m_ges
+            nvy = (svy[a] * m_a + svy[b] * m_b) / m_ges
+            if sim is not None:
+                sim.apply_body_state(st, a, nx, ny, nvx, nvy, m_ges)
+                sim.deactivate_body(st, b)
+            mass[a] = m_ges
+            mass[b] = 0.0
+            vis[b] = 0
+            rr[a] = (rr[a] ** 3 + rr[b] ** 3) ** (1.0 / 3.0)
+            if sim is not None:
+                sim.set_radius(st, a, float(rr[a]))
+            events.append((int(a), int(b), float(m_ges), 0, float(frac), float(nx), float(ny)))
+        if runaways is not None:
+            for j in runaways:
+                j = int(j)
+                if not vis[j]:
+                    continue
+                if sim is not None:
+                    sim.deactivate_body(st, j)
+                mass[j] = 0.0
+                vis[j] = 0
+                events.append((0xFFFFFFFF, j, 0.0, 2, 0.0, float(sx[j]), float(sy[j])))
+        return events, None
+
+    def apply_bounce(self, sim, st, res) -> int:
+        """Add the bounce deltas to the simulation on the device (apply_bounce,
+        film_producer.py:1021-1040); returns the number of bounces."""
+        if res is None:
+            return 0
+        hi, hj, touched, deltas = res
+        sim.apply_deltas_device(st, touched, deltas, int(touched.numel()))
+        return int(hi.numel())

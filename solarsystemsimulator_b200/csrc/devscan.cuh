@@ -6,6 +6,8 @@
 #include "sss_internal.cuh"
 
 namespace sss_dev {
+// internal linkage: every translation unit that includes this header gets its own copy of the kernels
+namespace {
 
 constexpr int SCAN_NT = 256;
 constexpr int SCAN_ITEMS = 8;
@@ -205,4 +207,5 @@ inline cudaError_t radix_sort(unsigned long long* k0, unsigned* v0, unsigned lon
     return cudaGetLastError();   // 8 passes: the result is back in (k0, v0)
 }
 
+}  // namespace
 }  // namespace sss_dev

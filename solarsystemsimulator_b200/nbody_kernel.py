@@ -283,6 +283,23 @@ class NBodyCuda:
             raise ValueError("apply_deltas: idx must be unique")
         self._scatter(st, idx, deltas, 1)
 
+    def apply_deltas_device(self, st: dict, idx, deltas, m: int) -> None:
+        """apply_deltas for device arrays (idx int64 [m] unique original
+        indices, deltas f64 [m][2*dim]) without a host round trip."""
+        if m <= 0:
+            return
+        if "slot_d" not in st:
+            slot = np.where(st["inv_kind"] > 0, st["inv_pos"], -st["inv_pos"] - 1).astype(np.int64)
+            st["slot_d"] = torch.as_tensor(slot).to(torch.device("cuda", self.device))
+        s_t = st["slot_d"][idx[:m]].contiguous()
+        v_t = deltas[:m].contiguous()
+        if v_t.shape[1] != 2 * st["dim"]:
+            raise ValueError(f"expected {2 * st['dim']} values per body, got {v_t.shape[1]}")
+        with torch.cuda.device(self.device):
+            rc = self._ctx.lib.sss_frame_scatter(self._ctx.ptr, ctypes.byref(st["c"]), s_t.data_ptr(),
+                                                 v_t.data_ptr(), int(m), 1, self._stream())
+        self._ctx.check(rc)
+
     def apply_body_state(self, st: dict, idx: int, x: float, y: float, vx: float, vy: float,
                          mass: float, *, z: float = 0.0, vz: float = 0.0) -> None:
         """Set one body completely (x, y, vx, vy, mass) (nbody_kernel.py:990-1010)."""
