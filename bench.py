@@ -339,7 +339,8 @@ def run_ours(args, rank, world, local_rank):
         for name, fn in (("frame_solar_system_belt", measure_frame), ("broadphase_asteroid_clouds",
                                                                        measure_broadphase),
                          ("pm2d_isolated", measure_pm2d), ("batched_small_systems", measure_batched),
-                         ("pm3d_learned", measure_pm3d_learned)):
+                         ("pm3d_learned", measure_pm3d_learned),
+                         ("collisions_asteroid_clouds", measure_collisions)):
             try:
                 rows[name] = fn(dev, stream)
             except Exception as exc:      # a row failing must not hide the headline line
@@ -574,6 +575,103 @@ def measure_batched(dev, stream, steps=10_000):
                              "sample": "oracle/batched.py, 64 systems x 10 steps, scaled by pair share"}}
 
 
+def measure_collisions(dev, stream, samples=16):
+    """The asteroid-clouds film on the device: 200,000 asteroids in 5 clouds,
+    a star and 7 planets (2-D film units AU / yr), raster 0.5 day. Per
+    sample: frame integration (NBodyCuda, 8 samples per launch), broadphase,
+    bounce response applied on the device, merge sweep + runaways, merges."""
+    import time
+    import torch
+    from oracle import collide as oc
+    from solarsystemsimulator_b200 import broadphase as bp
+    from solarsystemsimulator_b200.collide import CollisionResponse
+    from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
+    from solarsystemsimulator_b200.workloads import asteroid_clouds
+    w = asteroid_clouds()
+    n = w["pos"].shape[1]
+    x, y = w["pos"][0], w["pos"][1]
+    vx, vy = w["vel"][0] * 365.25, w["vel"][1] * 365.25
+    rr = w["radius"].copy()
+    rng = np.random.default_rng(5)
+    rr[0] = 0.00465
+    rr[1:8] = 10 ** rng.uniform(-5, -4.3, 7)
+    vis = np.ones(n, np.uint8)
+    sim = NBodyCuda([dev])
+    st = sim.load_state(x, y, vx, vy, w["mass"], vis, w["is_ast"], rr)
+    cr = CollisionResponse(w["mass"], rr, vis, w["is_ast"])
+    dt_y = 0.5 / 365.25
+    K = 8
+    rr32 = torch.as_tensor(rr.astype(np.float32)).to(f"cuda:{dev}")
+    ast_max = float(rr[8:].max())
+    t = {"frame": 0.0, "broadphase": 0.0, "bounce": 0.0, "sweep": 0.0, "merges": 0.0}
+    counts = {"hits": 0, "bounces": 0, "merge_pairs": 0, "runaways": 0, "candidates": 0}
+    last = None
+
+    def sync():
+        torch.cuda.synchronize(dev)
+
+    done = -K                                            # one untimed batch first (kernel loading, scratch)
+    while done < samples:
+        if done == 0:
+            for key in t:
+                t[key] = 0.0
+            for key in counts:
+                counts[key] = 0
+        t0 = time.perf_counter()
+        snap = sim.step_batch_device(st, dt_y, K)            # (K, 4, n) f32, device
+        sync()
+        t["frame"] += time.perf_counter() - t0
+        for k in range(K):
+            g = snap[k].reshape(4, n)
+            t0 = time.perf_counter()
+            alive = torch.nonzero((cr.d_ast != 0) & (cr.d_vis != 0)).flatten()
+            v95 = float(torch.quantile(torch.hypot(g[2][alive], g[3][alive]).double(), 0.95))
+            h = max(1e-4, 2.0 * v95 * dt_y)
+            buf, nh, nc = bp.bounce_hits_device(g[0], g[1], g[2], g[3], dt_y, h, 2.0 * h + 2.0 * ast_max, rr=rr32,
+                                                is_ast=cr.d_ast, vis=cr.d_vis, device=dev)
+            sync()
+            t1 = time.perf_counter()
+            res = cr.bounce_deltas(g, buf, nh, dt_y)
+            nb = cr.apply_bounce(sim, st, res)
+            sync()
+            t2 = time.perf_counter()
+            pairs, run = cr.analyze_merge(g, dt_y)
+            t3 = time.perf_counter()
+            if pairs or run is not None:
+                sample = g.reshape(-1).cpu().numpy()
+                cr.apply_merges(sim, st, sample, pairs, run, k_ev=done)
+                cr.refresh()
+            t4 = time.perf_counter()
+            t["broadphase"] += t1 - t0
+            t["bounce"] += t2 - t1
+            t["sweep"] += t3 - t2
+            t["merges"] += t4 - t3
+            counts["hits"] += nh
+            counts["bounces"] += nb
+            counts["candidates"] += nc
+            counts["merge_pairs"] += len(pairs)
+            counts["runaways"] += 0 if run is None else len(run)
+            last = (g.cpu().numpy(), buf.cpu().numpy())
+            done += 1
+    total = sum(t.values())
+    # CPU: the oracle's sweep and bounce response of the last sample (its broadphase has its own row)
+    g, hits = last
+    order = np.lexsort((hits[:, 2], hits[:, 1], hits[:, 0]))
+    hits = hits[order]
+    t0 = time.perf_counter()
+    oc.merge_sweep(*g, g[0], g[1], rr.astype(np.float32), cr.vis, w["is_ast"], cr.mass, np.arange(8), dt_y)
+    oc.bounce_deltas(*g, cr.real_r, cr.mass, hits[:, 1], hits[:, 2], dt_y)
+    tc = time.perf_counter() - t0
+    return {"workload": "5 Gaussian clouds x 40,000 asteroids + star + 7 planets, 2-D film (AU, yr), raster 0.5 day, "
+                        f"{samples} samples: frame integration, broadphase, bounce response, merge sweep, merges",
+            "samples_per_s": samples / total,
+            "ms_per_sample": {k: v / samples * 1e3 for k, v in t.items()},
+            "per_sample": {k: v / samples for k, v in counts.items()},
+            "response_ms_per_sample": (t["bounce"] + t["sweep"] + t["merges"]) / samples * 1e3,
+            "cpu_baseline": {"value": 1.0 / tc, "unit": "samples/s (sweep + bounce response only)", "cores": 1,
+                             "kind": "port", "sample": "oracle/collide.py merge_sweep + bounce_deltas on one sample"}}
+
+
 def measure_pm3d_learned(dev, stream, steps=500):
     """Periodic PM with the learned short-range correction: 1,048,576
     particles (Zel'dovich lattice, sigma 0.5 at the mesh scale) on a 256^3
@@ -679,7 +777,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-rows", action="store_true", help="skip the per-row measurements")
-    ap.add_argument("--row", choices=["frame", "broadphase", "pm2d", "batched", "pm3d"],
+    ap.add_argument("--row", choices=["frame", "broadphase", "pm2d", "batched", "pm3d", "collisions"],
                     help="run only this row's measurement (profiling) and print it")
     ap.add_argument("--row-steps", type=int, default=0, help="steps of the --row measurement (0: default)")
     ap.add_argument("--warmup-cpu", type=int, default=0)
@@ -698,8 +796,10 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         fn = {"frame": measure_frame, "broadphase": measure_broadphase, "pm2d": measure_pm2d,
-              "batched": measure_batched, "pm3d": measure_pm3d_learned}[args.row]
-        kw = {"steps": args.row_steps} if args.row_steps and args.row != "broadphase" else {}
+              "batched": measure_batched, "pm3d": measure_pm3d_learned, "collisions": measure_collisions}[args.row]
+        kw = {"steps": args.row_steps} if args.row_steps and args.row not in ("broadphase", "collisions") else {}
+        if args.row == "collisions" and args.row_steps:
+            kw = {"samples": args.row_steps}
         if args.row == "broadphase" and args.row_steps:
             kw = {"reps": args.row_steps}
         print(json.dumps(fn(local_rank, torch.cuda.current_stream(local_rank), **kw)), flush=True)
