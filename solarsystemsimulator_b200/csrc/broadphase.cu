@@ -18,16 +18,18 @@
 //   values, again without contraction.
 // The candidate list is never materialised: one kernel walks the flattened
 // candidate index space (offset-major, then body, then range position — the
-// reference's expansion order) in contiguous runs per thread, tests each
-// pair and appends hits. The host sorts the hits by (offset, a, b), which is
-// the reference's output order.
+// reference's expansion order) in contiguous chunks per warp, one candidate
+// per lane, tests each pair and appends hits; the partners' values are read
+// from records stored in sorted-key order (one gather per call), so the
+// lanes of a warp read consecutive records. The host
+// sorts the hits by (offset, a, b), which is the reference's output order.
 
 #include "devscan.cuh"
 
 namespace {
 
 constexpr int BP_NT = 256;
-constexpr int BP_RUN = 32;   // candidates per thread run
+constexpr int BP_CHUNK = 8192;   // consecutive candidates per warp
 
 __device__ __forceinline__ long long cell_key(long long cx, long long cy) {
     // int64 wrap-around multiply (the reference's `cx * int64(73856093) ^ cy * int64(19349663)`)
@@ -132,42 +134,61 @@ struct Hit {
     unsigned a, b;
 };
 
+// A body's snapshot values as the tests read them.
+struct Body {
+    float x, y, vx, vy, rr;
+};
+
 // f32 closest-approach prefilter (film_producer.py:241-259), op by op.
-__device__ __forceinline__ bool ccd_f32(const float* x, const float* y, const float* vx, const float* vy,
-                                        const float* rr, unsigned a, unsigned b, float dtf) {
-    const float dpx = __fsub_rn(x[b], x[a]);
-    const float dpy = __fsub_rn(y[b], y[a]);
-    const float dvx = __fsub_rn(vx[b], vx[a]);
-    const float dvy = __fsub_rn(vy[b], vy[a]);
+__device__ __forceinline__ bool ccd_f32(const Body& A, const Body& B, float dtf) {
+    const float dpx = __fsub_rn(B.x, A.x);
+    const float dpy = __fsub_rn(B.y, A.y);
+    const float dvx = __fsub_rn(B.vx, A.vx);
+    const float dvy = __fsub_rn(B.vy, A.vy);
     const float dv2 = __fadd_rn(__fmul_rn(dvx, dvx), __fmul_rn(dvy, dvy));
     const float num = -__fadd_rn(__fmul_rn(dpx, dvx), __fmul_rn(dpy, dvy));
     const float t = fminf(fmaxf(__fdiv_rn(num, dv2 > 0.f ? dv2 : 1.0f), -dtf), dtf);
     const float cxm = __fadd_rn(dpx, __fmul_rn(dvx, t));
     const float cym = __fadd_rn(dpy, __fmul_rn(dvy, t));
-    const float rsum = __fadd_rn(__fadd_rn(rr[a], rr[b]), 1e-6f);
+    const float rsum = __fadd_rn(__fadd_rn(A.rr, B.rr), 1e-6f);
     return __fadd_rn(__fmul_rn(cxm, cxm), __fmul_rn(cym, cym)) <= __fmul_rn(rsum, rsum);
 }
 
 // exact recheck in f64 of the f32 values (film_producer.py:303-314)
-__device__ __forceinline__ bool ccd_f64(const float* x, const float* y, const float* vx, const float* vy,
-                                        const float* rr, unsigned a, unsigned b, double dt) {
-    const double dpx = __dsub_rn((double)x[b], (double)x[a]);
-    const double dpy = __dsub_rn((double)y[b], (double)y[a]);
-    const double dvx = __dsub_rn((double)vx[b], (double)vx[a]);
-    const double dvy = __dsub_rn((double)vy[b], (double)vy[a]);
+__device__ __forceinline__ bool ccd_f64(const Body& A, const Body& B, double dt) {
+    const double dpx = __dsub_rn((double)B.x, (double)A.x);
+    const double dpy = __dsub_rn((double)B.y, (double)A.y);
+    const double dvx = __dsub_rn((double)B.vx, (double)A.vx);
+    const double dvy = __dsub_rn((double)B.vy, (double)A.vy);
     const double dv2 = __dadd_rn(__dmul_rn(dvx, dvx), __dmul_rn(dvy, dvy));
     const double num = -__dadd_rn(__dmul_rn(dpx, dvx), __dmul_rn(dpy, dvy));
     const double t = fmin(fmax(__ddiv_rn(num, dv2 > 0.0 ? dv2 : 1.0), -dt), dt);
     const double cxm = __dadd_rn(dpx, __dmul_rn(dvx, t));
     const double cym = __dadd_rn(dpy, __dmul_rn(dvy, t));
-    const double rsum = __dadd_rn((double)rr[a], (double)rr[b]);
+    const double rsum = __dadd_rn((double)A.rr, (double)B.rr);
     return __dadd_rn(__dmul_rn(cxm, cxm), __dmul_rn(cym, cym)) <= __dmul_rn(rsum, rsum);
+}
+
+// Body records in sorted-key order: position pos holds the body of row
+// order[pos] (x, y, vx, vy | rr bits, body index), so a segment's partners
+// are read from consecutive records instead of through two index arrays.
+__global__ void k_sorted_records(const float* __restrict__ x, const float* __restrict__ y,
+                                 const float* __restrict__ vx, const float* __restrict__ vy,
+                                 const float* __restrict__ rr, const unsigned* __restrict__ ai,
+                                 const unsigned* __restrict__ order, long long na, float4* __restrict__ rec,
+                                 uint2* __restrict__ rec2) {
+    const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= na) return;
+    const unsigned b = ai[order[pos]];
+    rec[pos] = make_float4(x[b], y[b], vx[b], vy[b]);
+    rec2[pos] = make_uint2(__float_as_uint(rr[b]), b);
 }
 
 struct CandArgs {
     const float *x, *y, *vx, *vy, *rr;
     const unsigned* ai;          // row -> body
-    const unsigned* order;       // sorted position -> row
+    const float4* rec;           // sorted position -> (x, y, vx, vy) of its body
+    const uint2* rec2;           // sorted position -> (rr bits, body)
     const long long* seg_lo;     // [5*na]
     const long long* seg_start;  // [5*na + 1] exclusive prefix of segment lengths
     long long n_seg, total;
@@ -188,35 +209,68 @@ __device__ __forceinline__ long long find_segment(const long long* start, long l
     return lo;
 }
 
+// keep rule, f32 prefilter, ownership, f64 recheck, append (film_producer.py:241-314)
+// Pairs that provably fail the f32 test are skipped before it. For every t
+// in [-dt, dt], |dp + dv t| >= |dp| - (|dvx| + |dvy|) dt; if |dp| exceeds
+// twice reach = (|dvx| + |dvy|) dt + rsum, the closest approach is at least
+// 2 rsum. The f32 evaluation of the test errs by a few ulp of |dp|, below
+// 1e-7 AU while |dp| < 1 AU, while rsum >= 1e-6 AU (radii + 1e-6), so such
+// a pair can never pass it: the skip changes no result, only the work.
+__device__ __forceinline__ bool surely_apart(const Body& A, const Body& B, float dtf) {
+    const float dpx = B.x - A.x, dpy = B.y - A.y;
+    const float dp2 = dpx * dpx + dpy * dpy;
+    const float reach = (fabsf(B.vx - A.vx) + fabsf(B.vy - A.vy)) * dtf + (A.rr + B.rr + 1e-6f);
+    return dp2 < 1.0f && dp2 > 4.0001f * reach * reach;
+}
+
+__device__ __forceinline__ void test_pair(const CandArgs& a, int o, unsigned ab, const Body& A, uint2 q, float4 v) {
+    const unsigned bb = q.y;
+    const bool keep = (o == 0) ? (ab < bb) : (ab != bb);
+    if (!keep) return;
+    const Body B{v.x, v.y, v.z, v.w, __uint_as_float(q.x)};
+    if (surely_apart(A, B, a.dtf)) return;
+    if (!ccd_f32(A, B, a.dtf)) return;
+    if (!(fminf(A.x, B.x) < a.hi)) return;          // ownership (:296)
+    if (!ccd_f64(A, B, a.dt)) return;
+    const unsigned long long slot = atomicAdd(a.n_hits, 1ull);
+    if ((long long)slot < a.cap) a.hits[slot] = Hit{o, ab, bb};
+}
+
+// A warp owns BP_CHUNK consecutive candidates of the flattened space and
+// walks them 32 at a time, lane l taking candidate base + l: the partners'
+// records of a step are consecutive (coalesced), the first body is shared
+// by the lanes of a segment (broadcast). Lane 0 finds the chunk's first
+// segment by binary search; every lane then moves forward through the
+// segment starts as its index grows.
 __global__ void __launch_bounds__(BP_NT) k_candidates(const CandArgs a) {
-    const long long runs = (a.total + BP_RUN - 1) / BP_RUN;
+    const int lane = threadIdx.x & 31;
+    const long long chunks = (a.total + BP_CHUNK - 1) / BP_CHUNK;
     const long long na = a.n_seg / 5;
-    for (long long run = (long long)blockIdx.x * blockDim.x + threadIdx.x; run < runs;
-         run += (long long)gridDim.x * blockDim.x) {
-        long long idx = run * BP_RUN;
-        const long long end = min(idx + BP_RUN, a.total);
-        long long s = find_segment(a.seg_start, a.n_seg, idx);
-        while (idx < end) {
-            long long seg_end = a.seg_start[s + 1];
-            while (seg_end <= idx) {          // skip empty segments
-                ++s;
-                seg_end = a.seg_start[s + 1];
+    const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long c = warp0; c < chunks; c += warps) {
+        const long long base = c * BP_CHUNK;
+        const long long end = min(base + BP_CHUNK, a.total);
+        long long s0 = 0;
+        if (lane == 0) s0 = find_segment(a.seg_start, a.n_seg, base);
+        long long s = __shfl_sync(0xffffffffu, s0, 0);
+        long long cur = -1;
+        int o = 0;
+        unsigned ab = 0;
+        long long col0 = 0;
+        Body A{0.f, 0.f, 0.f, 0.f, 0.f};
+        for (long long idx = base + lane; idx < end; idx += 32) {
+            while (a.seg_start[s + 1] <= idx) ++s;
+            if (s != cur) {
+                cur = s;
+                o = (int)(s / na);
+                const long long r = s - (long long)o * na;
+                ab = a.ai[r];
+                A = Body{a.x[ab], a.y[ab], a.vx[ab], a.vy[ab], a.rr[ab]};
+                col0 = a.seg_lo[s] - a.seg_start[s];
             }
-            const int o = (int)(s / na);
-            const long long r = s - (long long)o * na;
-            const unsigned ab = a.ai[r];
-            const long long col0 = a.seg_lo[s] - a.seg_start[s];
-            const long long stop = min(end, seg_end);
-            for (; idx < stop; ++idx) {
-                const unsigned bb = a.ai[a.order[col0 + idx]];
-                const bool keep = (o == 0) ? (ab < bb) : (ab != bb);
-                if (!keep) continue;
-                if (!ccd_f32(a.x, a.y, a.vx, a.vy, a.rr, ab, bb, a.dtf)) continue;
-                if (!(fminf(a.x[ab], a.x[bb]) < a.hi)) continue;          // ownership (:296)
-                if (!ccd_f64(a.x, a.y, a.vx, a.vy, a.rr, ab, bb, a.dt)) continue;
-                const unsigned long long slot = atomicAdd(a.n_hits, 1ull);
-                if ((long long)slot < a.cap) a.hits[slot] = Hit{o, ab, bb};
-            }
+            const long long j = col0 + idx;
+            test_pair(a, o, ab, A, a.rec2[j], a.rec[j]);
         }
     }
 }
@@ -254,6 +308,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_v = take(nn);                  // v0 + v1 (unsigned, 2 per long long)
     const size_t o_ai = take((nn + 1) / 2 + 1);
     const size_t o_seglo = take(5 * nn), o_segst = take(5 * nn + 1);
+    const size_t o_rec = take(2 * nn), o_rec2 = take(nn);      // float4 and uint2 per alive body
     const size_t o_nh = take(1);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off * sizeof(long long), &scr);
@@ -270,6 +325,8 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     unsigned* ai = (unsigned*)(S + o_ai);
     long long* seg_lo = S + o_seglo;
     long long* seg_st = S + o_segst;
+    float4* rec = (float4*)(S + o_rec);
+    uint2* rec2 = (uint2*)(S + o_rec2);
     unsigned long long* d_nh = (unsigned long long*)(S + o_nh);
 
     // 1) alive compaction (ascending body order) + cells + keys
@@ -284,6 +341,8 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     SSS_LAUNCH_CHECK(ctx, "k_alive_scatter");
     // 2) stable sort of the keys (ascending signed order)
     SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, na, scan_tmp, s));
+    k_sorted_records<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, na, rec, rec2);
+    SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
     // 3) equal-key range of every (offset, body)
     const long long nseg = 5 * na;
     k_ranges<<<(unsigned)((nseg + 255) / 256), 256, 0, s>>>(cx, cy, na, k0, seg_lo, seg_st);
@@ -303,7 +362,8 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     CandArgs ca;
     ca.x = x; ca.y = y; ca.vx = vx; ca.vy = vy; ca.rr = rr;
     ca.ai = ai;
-    ca.order = v0;
+    ca.rec = rec;
+    ca.rec2 = rec2;
     ca.seg_lo = seg_lo;
     ca.seg_start = seg_st;
     ca.n_seg = nseg;
@@ -314,8 +374,8 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     ca.hits = (Hit*)out_hits;
     ca.cap = capacity;
     ca.n_hits = d_nh;
-    const long long runs = (total + BP_RUN - 1) / BP_RUN;
-    long long blocks = (runs + BP_NT - 1) / BP_NT;
+    const long long chunks = (total + BP_CHUNK - 1) / BP_CHUNK;
+    long long blocks = (chunks + BP_NT / 32 - 1) / (BP_NT / 32);
     const long long max_blocks = (long long)ctx->num_sms * 32;
     if (blocks > max_blocks) blocks = max_blocks;
     k_candidates<<<(unsigned)blocks, BP_NT, 0, s>>>(ca);
