@@ -584,6 +584,7 @@ def measure_collisions(dev, stream, samples=16):
     import torch
     from oracle import collide as oc
     from solarsystemsimulator_b200 import broadphase as bp
+    from solarsystemsimulator_b200 import ring
     from solarsystemsimulator_b200.collide import CollisionResponse
     from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
     from solarsystemsimulator_b200.workloads import asteroid_clouds
@@ -603,7 +604,11 @@ def measure_collisions(dev, stream, samples=16):
     K = 8
     rr32 = torch.as_tensor(rr.astype(np.float32)).to(f"cuda:{dev}")
     ast_max = float(rr[8:].max())
-    t = {"frame": 0.0, "broadphase": 0.0, "bounce": 0.0, "sweep": 0.0, "merges": 0.0}
+    sub_max = ring.sub_max_fuer(n)
+    nbytes = ring.slot_bytes(n, sim.m_sub, sub_max)
+    slot_dev = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{dev}")
+    slot_host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    t = {"frame": 0.0, "ring": 0.0, "broadphase": 0.0, "bounce": 0.0, "sweep": 0.0, "merges": 0.0}
     counts = {"hits": 0, "bounces": 0, "merge_pairs": 0, "runaways": 0, "candidates": 0}
     last = None
 
@@ -623,6 +628,11 @@ def measure_collisions(dev, stream, samples=16):
         t["frame"] += time.perf_counter() - t0
         for k in range(K):
             g = snap[k].reshape(4, n)
+            t0 = time.perf_counter()
+            ring.write_slot(sim, st, k, slot_dev, sub_max)      # the ring slot, then to the host ring
+            slot_host.copy_(slot_dev, non_blocking=True)
+            sync()
+            t["ring"] += time.perf_counter() - t0
             t0 = time.perf_counter()
             alive = torch.nonzero((cr.d_ast != 0) & (cr.d_vis != 0)).flatten()
             v95 = float(torch.quantile(torch.hypot(g[2][alive], g[3][alive]).double(), 0.95))
@@ -663,7 +673,8 @@ def measure_collisions(dev, stream, samples=16):
     oc.bounce_deltas(*g, cr.real_r, cr.mass, hits[:, 1], hits[:, 2], dt_y)
     tc = time.perf_counter() - t0
     return {"workload": "5 Gaussian clouds x 40,000 asteroids + star + 7 planets, 2-D film (AU, yr), raster 0.5 day, "
-                        f"{samples} samples: frame integration, broadphase, bounce response, merge sweep, merges",
+                        f"{samples} samples: frame integration, ring slot to a pinned host buffer, broadphase, "
+                        "bounce response, merge sweep, merges",
             "samples_per_s": samples / total,
             "ms_per_sample": {k: v / samples * 1e3 for k, v in t.items()},
             "per_sample": {k: v / samples for k, v in counts.items()},

@@ -274,6 +274,29 @@ int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const float* y, 
                        double e, int* pairs_out, int64_t* touched_out, double* deltas_out, int64_t* n_act,
                        int64_t* n_touched, void* stream);
 
+/* ------------------------------------------------------- film ring slots
+ *
+ * sss_ring_slot replaces schreibe_slot (film_producer.py:79-123): one ring
+ * slot (device bytes, slot_bytes = 8n + 4 + sub_max (4 + 8 m_sub)) from a
+ * frame snapshot row (device f32 [x|y|...], at least 2n values) and the
+ * sample's sub-samples as sss_frame_launch leaves them (sub_pos
+ * [m_sub][dim][n_ast], sub_n [n_ast]; a_idx [n_ast] the original index of
+ * every asteroid slot, ascending). Writes x|y, the count, the indices of the
+ * hot asteroids (gap-free chains) ascending and their chains (nh, mSub, 2);
+ * at most sub_max are kept (the lowest indices). *n_hot (host) receives how
+ * many were hot (more than sub_max = overflow). Synchronous. Entries beyond
+ * the count are left as they were.
+ *
+ * sss_ring_reorder replaces the self-gravity row reorder (:1245-1261): K rows
+ * [x_m|y_m|vx_m|vy_m|x_t|y_t] (nm masses at original indices sg_m, nt tracers
+ * at sg_t) into K rows [x|y|vx|vy] of n bodies in original order, tracer
+ * velocities 0. */
+int sss_ring_slot(sss_ctx* ctx, const float* row, int64_t n, const float* sub_pos, const unsigned char* sub_n,
+                  const int64_t* a_idx, int64_t n_ast, int m_sub, int dim, int64_t sub_max, unsigned char* slot,
+                  int64_t* n_hot, void* stream);
+int sss_ring_reorder(sss_ctx* ctx, const float* rows, int K, const int64_t* sg_m, int64_t nm, const int64_t* sg_t,
+                     int64_t nt, int64_t n, float* out, void* stream);
+
 /* ------------------------------------------------ particle mesh, 3-D periodic
  *
  * The reference's PM cycle (TODO.md:225-253; 2-D code pm_kernel.py:63-154)
