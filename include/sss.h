@@ -297,6 +297,26 @@ int sss_ring_slot(sss_ctx* ctx, const float* row, int64_t n, const float* sub_po
 int sss_ring_reorder(sss_ctx* ctx, const float* rows, int K, const int64_t* sg_m, int64_t nm, const int64_t* sg_t,
                      int64_t nt, int64_t n, float* out, void* stream);
 
+/* ------------------------------------------------------- stream frames
+ *
+ * The server's per-sample stream core (server.py: build_frame :378-537,
+ * _anzeige_koords :99-111, _lod_auswahl :629-684, _dichte_filter :686-747,
+ * _index_hash :117-131) on the device, with the reference's arithmetic.
+ * sss_stream_sample: the bodies of one f32 sample (x, y) that are alive
+ * (kill_t > t_cut) and inside box (host: x0, y0, spanx, spany as the
+ * session's floats), thinned by the density LOD to about `budget` points
+ * (massive bodies first, then the system's asteroids, then injected ones;
+ * injected may be NULL), ascending in sel (u32), with their u16 box
+ * coordinates; log_zoom uses the log-radial display coordinates. *n_sel
+ * (host) receives the count; sel/qx/qy need capacity n. Synchronous.
+ * sss_stream_minmax: (min x, max x, min y, max y) of the display coordinates
+ * of all n bodies into out4 (host), the input of the automatic box. */
+int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const float* y, const double* kill_t, double t_cut,
+                      const unsigned char* is_ast, const unsigned char* injected, const double* box, int log_zoom,
+                      int64_t budget, unsigned* sel, uint16_t* qx, uint16_t* qy, int64_t* n_sel, void* stream);
+int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const float* y, int log_zoom, float* out4,
+                      void* stream);
+
 /* ------------------------------------------------ particle mesh, 3-D periodic
  *
  * The reference's PM cycle (TODO.md:225-253; 2-D code pm_kernel.py:63-154)

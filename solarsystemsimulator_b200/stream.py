@@ -1,0 +1,86 @@
+"""The server's per-sample stream core on one B200 (reference
+backend/server.py: FilmSession.build_frame with _anzeige_koords,
+_lod_auswahl, _dichte_filter and _index_hash): culling by box and kill time,
+the density LOD and the u16 quantisation of a sample, bit-exact against the
+reference (linear display coordinates; the log zoom evaluates hypot and
+log1p on the device).
+
+    sf = StreamFrames(is_ast, injected, visible)
+    box = sf.box(x_dev, y_dev, view, log_zoom)              # the session's box rule
+    sel, qx, qy = sf.sample(x_dev, y_dev, t_i, raster_days, box, log_zoom, budget)
+    sf.kill(idx, t)                                         # the event stream's kill times
+
+The frame bytes around it (header, events, sub-sample chains, the unchanged
+index list flag) stay with the server's own packing code.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+LOD_MAX = 120_000        # server.py build_frame: the client's decode limit per sample
+
+
+def lod_budget(setting: int, bandwidth: float) -> int:
+    """Points per sample (build_frame's lod_max)."""
+    return setting or min(LOD_MAX, max(20000, int(bandwidth * 0.7 / 20.0 / 8.0)))
+
+
+class StreamFrames:
+    def __init__(self, is_ast, injected=None, visible=None, device: int = 0):
+        self.device = int(device)
+        self.dev = torch.device("cuda", self.device)
+        self.ctx = _lib.context(device)
+        is_ast = np.asarray(is_ast) != 0
+        self.n = len(is_ast)
+        self.d_ast = torch.as_tensor(is_ast.astype(np.uint8)).to(self.dev)
+        self.d_inj = (torch.as_tensor((np.asarray(injected) != 0).astype(np.uint8)).to(self.dev)
+                      if injected is not None else None)
+        vis = np.ones(self.n, bool) if visible is None else np.asarray(visible) != 0
+        self.kill_t = torch.as_tensor(np.where(vis, np.inf, -np.inf)).to(self.dev)
+        self.sel = torch.empty(self.n, dtype=torch.int32, device=self.dev)
+        self.qx = torch.empty(self.n, dtype=torch.int16, device=self.dev)
+        self.qy = torch.empty(self.n, dtype=torch.int16, device=self.dev)
+
+    def _s(self):
+        return ctypes.c_void_p(_lib.stream_handle(self.device))
+
+    def kill(self, idx, t: float) -> None:
+        """Kill time of bodies (min with the known one), as the event stream sets it."""
+        i = torch.as_tensor(np.asarray(idx, np.int64)).to(self.dev)
+        self.kill_t[i] = torch.minimum(self.kill_t[i], torch.full_like(self.kill_t[i], float(t)))
+
+    def box(self, x, y, view, log_zoom: bool):
+        """The reference box: 2x the viewport about the camera, or before
+        the client reported one, the whole distribution plus 5 %."""
+        cx, cy, hw, hh = (float(v) for v in view)
+        if hw > 0 and hh > 0:
+            return (cx - 2 * hw, cy - 2 * hh, max(4 * hw, 1e-6), max(4 * hh, 1e-6))
+        out = (ctypes.c_float * 4)()
+        with torch.cuda.device(self.device):
+            self.ctx.check(self.ctx.lib.sss_stream_minmax(self.ctx.ptr, self.n, x.data_ptr(), y.data_ptr(),
+                                                          int(bool(log_zoom)), out, self._s()))
+        bx0, bx1, by0, by1 = (float(v) for v in out)
+        mx = 0.05 * max(bx1 - bx0, 1e-6)
+        my = 0.05 * max(by1 - by0, 1e-6)
+        return (bx0 - mx, by0 - my, max(bx1 - bx0 + 2 * mx, 1e-6), max(by1 - by0 + 2 * my, 1e-6))
+
+    def sample(self, x, y, t_i: float, raster_days: float, box, log_zoom: bool, budget: int):
+        """(sel u32, qx u16, qy u16) views of one sample (device tensors,
+        valid until the next call)."""
+        x = x.contiguous()
+        y = y.contiguous()
+        b = (ctypes.c_double * 4)(*(float(v) for v in box))
+        cnt = ctypes.c_int64()
+        with torch.cuda.device(self.device):
+            self.ctx.check(self.ctx.lib.sss_stream_sample(
+                self.ctx.ptr, self.n, x.data_ptr(), y.data_ptr(), self.kill_t.data_ptr(), float(t_i - raster_days),
+                self.d_ast.data_ptr(), self.d_inj.data_ptr() if self.d_inj is not None else None, b,
+                int(bool(log_zoom)), int(budget), self.sel.data_ptr(), self.qx.data_ptr(), self.qy.data_ptr(),
+                ctypes.byref(cnt), self._s()))
+        m = cnt.value
+        return self.sel[:m], self.qx[:m], self.qy[:m]

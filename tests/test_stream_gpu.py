@@ -1,0 +1,134 @@
+"""GPU stream frames (sss_stream_sample / sss_stream_minmax) against the
+golden frames of the reference's own build_frame: the box, the culled and
+thinned index lists and the u16 coordinates of both samples, bit for bit
+(the log zoom may round hypot/log1p differently from the host C library:
+there the index lists must agree but for a handful of bodies)."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+SCENES = ["wolken", "massenwolke", "autobox_log", "klein_tot"]
+
+
+@pytest.mark.parametrize("scene", SCENES)
+def test_frames_match_reference(load_golden, scene):
+    from solarsystemsimulator_b200.stream import StreamFrames
+    g = load_golden(f"server_frame_{scene}.npz")
+    log_zoom = bool(g["log_zoom"])
+    sf = StreamFrames(g["is_ast"], g["injected"])
+    sf.kill_t = torch.as_tensor(g["kill_t"]).cuda()
+    x0, y0 = torch.as_tensor(g["x0"]).cuda(), torch.as_tensor(g["y0"]).cuda()
+    box = sf.box(x0, y0, tuple(g["view"]), log_zoom)
+    if log_zoom:
+        assert np.allclose(box, g["box"], rtol=1e-6, atol=0)
+        box = tuple(float(v) for v in g["box"])
+    else:
+        assert box == tuple(float(v) for v in g["box"])
+    for k in range(2):
+        t_i = float(g["t0"]) + (k + 1) * float(g["raster_days"])
+        x, y = torch.as_tensor(g[f"x{k}"]).cuda(), torch.as_tensor(g[f"y{k}"]).cuda()
+        sel, qx, qy = (t.cpu().numpy() for t in sf.sample(x, y, t_i, float(g["raster_days"]), box, log_zoom,
+                                                          int(g["budget"])))
+        sel = sel.view(np.uint32)
+        qx = qx.view(np.uint16)
+        qy = qy.view(np.uint16)
+        ref = g[f"sel{k}"]
+        if not log_zoom:
+            assert np.array_equal(sel, ref)
+            assert np.array_equal(qx, g[f"qx{k}"]) and np.array_equal(qy, g[f"qy{k}"])
+        else:
+            diff = len(np.setxor1d(sel, ref))
+            assert diff <= 10, diff
+            common, ia, ib = np.intersect1d(sel, ref, return_indices=True)
+            assert np.abs(qx[ia].astype(int) - g[f"qx{k}"][ib].astype(int)).max() <= 1
+            assert np.abs(qy[ia].astype(int) - g[f"qy{k}"][ib].astype(int)).max() <= 1
+
+
+def _scene(n_mass, n_ast, n_inj, seed, spread=1.0):
+    rng = np.random.default_rng(seed)
+    n = n_mass + n_ast + n_inj
+    x = np.zeros(n)
+    y = np.zeros(n)
+    x[:n_mass] = rng.uniform(-5, 5, n_mass)
+    y[:n_mass] = rng.uniform(-5, 5, n_mass)
+    cen = rng.uniform(-3, 3, (8, 2))
+    lab = rng.integers(0, 8, n_ast + n_inj)
+    sig = 10 ** rng.uniform(-2.5, -0.3, 8) * spread
+    x[n_mass:] = cen[lab, 0] + rng.normal(0, 1, n_ast + n_inj) * sig[lab]
+    y[n_mass:] = cen[lab, 1] + rng.normal(0, 1, n_ast + n_inj) * sig[lab]
+    is_ast = np.zeros(n, bool)
+    is_ast[n_mass:] = True
+    inj = np.zeros(n, bool)
+    inj[n_mass + n_ast:] = True
+    kill_t = np.full(n, np.inf)
+    dead = rng.choice(n, n // 50, replace=False)
+    kill_t[dead] = rng.uniform(-1, 1, len(dead))
+    return x.astype(np.float32), y.astype(np.float32), is_ast, inj, kill_t
+
+
+# (masses, system asteroids, injected, view, budget): the film's full LOD
+# budget over 600k bodies, the self-gravity cloud branch, a budget below
+# the masses (masses only) and a box that holds nobody
+LARGE = {
+    "asteroids_600k": (20, 500_000, 100_000, (0.0, 0.0, 2.0, 2.0), 120_000),
+    "mass_cloud": (40_000, 200_000, 0, (0.5, 0.0, 3.0, 3.0), 30_000),
+    "masses_only": (150, 50_000, 0, (0.0, 0.0, 4.0, 4.0), 100),
+    "empty_box": (10, 10_000, 1000, (400.0, 400.0, 1.0, 1.0), 1000),
+}
+
+
+@pytest.mark.parametrize("name", list(LARGE))
+def test_large_samples_match_oracle(name):
+    """Linear display coordinates at film sizes: bit-exact against the oracle."""
+    from oracle import frames as ofr
+    from solarsystemsimulator_b200.stream import StreamFrames
+    nm, na, ni, view, budget = LARGE[name]
+    x, y, a, inj, kill_t = _scene(nm, na, ni, seed=len(name))
+    sf = StreamFrames(a, inj)
+    sf.kill_t = torch.as_tensor(kill_t).cuda()
+    xd, yd = torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda()
+    box = sf.box(xd, yd, view, False)
+    assert box == ofr.make_box(x, y, view)
+    t_i = 0.5
+    sel, qx, qy = (t.cpu().numpy() for t in sf.sample(xd, yd, t_i, 0.5, box, False, budget))
+    rs, rx, ry = ofr.sample_frame(x, y, kill_t > 0.0, a, inj, box, False, budget)
+    assert np.array_equal(sel.view(np.uint32), rs)
+    assert np.array_equal(qx.view(np.uint16), rx) and np.array_equal(qy.view(np.uint16), ry)
+    if name == "empty_box":
+        assert len(rs) == 0
+    else:
+        assert 0 < len(rs) <= max(budget, nm) * 1.05
+
+
+def test_autobox_matches_oracle_log_zoom():
+    """Automatic box (no view yet) and the log zoom at 300k bodies."""
+    from oracle import frames as ofr
+    from solarsystemsimulator_b200.stream import StreamFrames
+    x, y, a, inj, kill_t = _scene(9, 300_000, 0, seed=3, spread=3.0)
+    sf = StreamFrames(a, inj)
+    xd, yd = torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda()
+    box_lin = sf.box(xd, yd, (0, 0, -1, -1), False)
+    assert box_lin == ofr.make_box(x, y, (0, 0, -1, -1))
+    qx0, qy0 = ofr.display_coords(x, y, True)
+    ref_box = ofr.make_box(qx0, qy0, (0, 0, -1, -1))
+    box = sf.box(xd, yd, (0, 0, -1, -1), True)
+    assert np.allclose(box, ref_box, rtol=1e-6, atol=1e-7)
+    sel, _, _ = (t.cpu().numpy() for t in sf.sample(xd, yd, 0.5, 0.5, ref_box, True, 60_000))
+    rs, _, _ = ofr.sample_frame(x, y, np.ones(len(x), bool), a, inj, ref_box, True, 60_000)
+    assert len(np.setxor1d(sel.view(np.uint32), rs)) <= 1e-4 * len(rs) + 10
+
+
+def test_kill_times():
+    from solarsystemsimulator_b200.stream import StreamFrames
+    x, y, a, inj, _ = _scene(5, 2000, 0, seed=1)
+    sf = StreamFrames(a, inj)
+    sf.kill([7, 9, 11], 0.25)
+    sf.kill([9], 1.0)                     # a later kill does not revive an earlier one
+    xd, yd = torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda()
+    box = (-100.0, -100.0, 200.0, 200.0)
+    sel = sf.sample(xd, yd, 0.5, 0.5, box, False, 10**6)[0].cpu().numpy()
+    assert len(sel) == len(x) and 7 in sel                  # t_cut 0.0 < 0.25
+    sel = sf.sample(xd, yd, 1.0, 0.5, box, False, 10**6)[0].cpu().numpy()
+    assert len(sel) == len(x) - 3 and not {7, 9, 11} & set(sel.tolist())
