@@ -340,7 +340,7 @@ def run_ours(args, rank, world, local_rank):
                                                                        measure_broadphase),
                          ("pm2d_isolated", measure_pm2d), ("batched_small_systems", measure_batched),
                          ("pm3d_learned", measure_pm3d_learned),
-                         ("collisions_asteroid_clouds", measure_collisions)):
+                         ("collisions_asteroid_clouds", measure_collisions), ("stream_frames", measure_stream)):
             try:
                 rows[name] = fn(dev, stream)
             except Exception as exc:      # a row failing must not hide the headline line
@@ -587,6 +587,7 @@ def measure_collisions(dev, stream, samples=16):
     from solarsystemsimulator_b200 import ring
     from solarsystemsimulator_b200.collide import CollisionResponse
     from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
+    from solarsystemsimulator_b200.stream import LOD_MAX, StreamFrames
     from solarsystemsimulator_b200.workloads import asteroid_clouds
     w = asteroid_clouds()
     n = w["pos"].shape[1]
@@ -608,8 +609,10 @@ def measure_collisions(dev, stream, samples=16):
     nbytes = ring.slot_bytes(n, sim.m_sub, sub_max)
     slot_dev = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{dev}")
     slot_host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
-    t = {"frame": 0.0, "ring": 0.0, "broadphase": 0.0, "bounce": 0.0, "sweep": 0.0, "merges": 0.0}
-    counts = {"hits": 0, "bounces": 0, "merge_pairs": 0, "runaways": 0, "candidates": 0}
+    sf = StreamFrames(w["is_ast"], device=dev)
+    box = None
+    t = {"frame": 0.0, "ring": 0.0, "stream": 0.0, "broadphase": 0.0, "bounce": 0.0, "sweep": 0.0, "merges": 0.0}
+    counts = {"hits": 0, "bounces": 0, "merge_pairs": 0, "runaways": 0, "candidates": 0, "frame_points": 0}
     last = None
 
     def sync():
@@ -634,6 +637,12 @@ def measure_collisions(dev, stream, samples=16):
             sync()
             t["ring"] += time.perf_counter() - t0
             t0 = time.perf_counter()
+            if k == 0:                                   # the automatic box from the batch's first sample
+                box = sf.box(g[0], g[1], (0.0, 0.0, -1.0, -1.0), False)
+            sel, _, _ = sf.sample(g[0], g[1], float(done + 1), 1.0, box, False, LOD_MAX)
+            counts["frame_points"] += sel.numel()
+            t["stream"] += time.perf_counter() - t0
+            t0 = time.perf_counter()
             alive = torch.nonzero((cr.d_ast != 0) & (cr.d_vis != 0)).flatten()
             v95 = float(torch.quantile(torch.hypot(g[2][alive], g[3][alive]).double(), 0.95))
             h = max(1e-4, 2.0 * v95 * dt_y)
@@ -649,8 +658,12 @@ def measure_collisions(dev, stream, samples=16):
             t3 = time.perf_counter()
             if pairs or run is not None:
                 sample = g.reshape(-1).cpu().numpy()
+                vis_before = cr.vis.copy()
                 cr.apply_merges(sim, st, sample, pairs, run, k_ev=done)
                 cr.refresh()
+                gone = np.flatnonzero((vis_before != 0) & (cr.vis == 0))
+                if len(gone):
+                    sf.kill(gone, float(done + 1))
             t4 = time.perf_counter()
             t["broadphase"] += t1 - t0
             t["bounce"] += t2 - t1
@@ -673,14 +686,97 @@ def measure_collisions(dev, stream, samples=16):
     oc.bounce_deltas(*g, cr.real_r, cr.mass, hits[:, 1], hits[:, 2], dt_y)
     tc = time.perf_counter() - t0
     return {"workload": "5 Gaussian clouds x 40,000 asteroids + star + 7 planets, 2-D film (AU, yr), raster 0.5 day, "
-                        f"{samples} samples: frame integration, ring slot to a pinned host buffer, broadphase, "
-                        "bounce response, merge sweep, merges",
+                        f"{samples} samples: frame integration, ring slot to a pinned host buffer, stream frame "
+                        "(automatic box, LOD 120,000), broadphase, bounce response, merge sweep, merges",
             "samples_per_s": samples / total,
             "ms_per_sample": {k: v / samples * 1e3 for k, v in t.items()},
             "per_sample": {k: v / samples for k, v in counts.items()},
             "response_ms_per_sample": (t["bounce"] + t["sweep"] + t["merges"]) / samples * 1e3,
             "cpu_baseline": {"value": 1.0 / tc, "unit": "samples/s (sweep + bounce response only)", "cores": 1,
                              "kind": "port", "sample": "oracle/collide.py merge_sweep + bounce_deltas on one sample"}}
+
+
+def _stream_scene(n_mass=20, n_ast=900_000, n_inj=100_000, seed=11):
+    """Masses on a 10 AU square, asteroids and injected asteroids in 8
+    Gaussian clouds (sigma 0.003-0.5 AU), 2 % of the bodies killed at a random
+    time in [-1, 1]: one f32 sample of a film."""
+    rng = np.random.default_rng(seed)
+    n = n_mass + n_ast + n_inj
+    x = np.zeros(n)
+    y = np.zeros(n)
+    x[:n_mass] = rng.uniform(-5, 5, n_mass)
+    y[:n_mass] = rng.uniform(-5, 5, n_mass)
+    cen = rng.uniform(-3, 3, (8, 2))
+    lab = rng.integers(0, 8, n_ast + n_inj)
+    sig = 10 ** rng.uniform(-2.5, -0.3, 8)
+    x[n_mass:] = cen[lab, 0] + rng.normal(0, 1, n_ast + n_inj) * sig[lab]
+    y[n_mass:] = cen[lab, 1] + rng.normal(0, 1, n_ast + n_inj) * sig[lab]
+    is_ast = np.zeros(n, bool)
+    is_ast[n_mass:] = True
+    inj = np.zeros(n, bool)
+    inj[n_mass + n_ast:] = True
+    kill_t = np.full(n, np.inf)
+    dead = rng.choice(n, n // 50, replace=False)
+    kill_t[dead] = rng.uniform(-1, 1, len(dead))
+    return x.astype(np.float32), y.astype(np.float32), is_ast, inj, kill_t
+
+
+def measure_stream(dev, stream, samples=200):
+    """The server's stream core per sample (cull by box and kill time,
+    density LOD to the client's 120,000-point limit, ascending compaction,
+    u16 quantisation) on 1,000,020 bodies, inputs resident; linear zoom with
+    a view box over the clouds, and log zoom with the automatic box. e2e adds
+    the D2H copy of the frame payload (u32 indices + 2 x u16) per sample."""
+    import time
+    import torch
+    from oracle import frames as ofr
+    from solarsystemsimulator_b200.stream import LOD_MAX, StreamFrames
+    x, y, a, inj, kill_t = _stream_scene()
+    n = len(x)
+    sf = StreamFrames(a, inj, device=dev)
+    sf.kill_t = torch.as_tensor(kill_t).to(f"cuda:{dev}")
+    xd, yd = torch.as_tensor(x).to(f"cuda:{dev}"), torch.as_tensor(y).to(f"cuda:{dev}")
+    host = torch.empty(8 * n, dtype=torch.uint8).pin_memory()
+    peak = float(json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                             "MEASURED_PEAKS.json")))["hbm_gbs"])
+    out = {"workload": "stream frames: 20 masses + 900,000 asteroids + 100,000 injected in 8 Gaussian clouds, "
+                       "2 % killed, one f32 sample per call, LOD budget 120,000",
+           "samples": samples}
+    for mode, view, log_zoom in (("linear_view", (0.0, 0.0, 2.5, 2.5), False),
+                                 ("log_autobox", (0.0, 0.0, -1.0, -1.0), True)):
+        box = sf.box(xd, yd, view, log_zoom)
+        kept = [0]
+
+        def one():
+            sel, qx, qy = sf.sample(xd, yd, 0.5, 0.5, box, log_zoom, LOD_MAX)
+            kept[0] = sel.numel()
+
+        def one_e2e():
+            sel, qx, qy = sf.sample(xd, yd, 0.5, 0.5, box, log_zoom, LOD_MAX)
+            m = sel.numel()
+            host[:4 * m].view(torch.int32).copy_(sel, non_blocking=True)
+            host[4 * m:6 * m].view(torch.int16).copy_(qx, non_blocking=True)
+            host[6 * m:8 * m].view(torch.int16).copy_(qy, non_blocking=True)
+            kept[0] = m
+
+        for _ in range(3):
+            one_e2e()
+        t = _ev_time(one, stream, samples)
+        te = _ev_time(one_e2e, stream, samples)
+        m = kept[0]
+        alg = n * (4 + 4 + 8 + 1 + 1) + m * 8           # sample, kill times, flags in; the kept payload out
+        qxs, qys = ofr.display_coords(x, y, log_zoom)
+        cpu_box = ofr.make_box(qxs, qys, view)
+        t0 = time.perf_counter()
+        ofr.sample_frame(x, y, kill_t > 0.0, a, inj, cpu_box, log_zoom, LOD_MAX)
+        tc = time.perf_counter() - t0
+        out[mode] = {"samples_per_s": 1.0 / t, "ms_per_sample": t * 1e3, "kept": int(m),
+                     "e2e": {"samples_per_s": 1.0 / te, "d2h_bytes_per_sample": 8 * m},
+                     "algorithmic_bytes_per_sample": alg, "achieved_gbs": alg / t / 1e9,
+                     "frac_of_measured_hbm": alg / t / 1e9 / peak,
+                     "cpu_baseline": {"value": 1.0 / tc, "unit": "samples/s", "cores": 1, "kind": "port",
+                                      "sample": "oracle/frames.py sample_frame on the same sample"}}
+    return out
 
 
 def measure_pm3d_learned(dev, stream, steps=500):
@@ -788,7 +884,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-rows", action="store_true", help="skip the per-row measurements")
-    ap.add_argument("--row", choices=["frame", "broadphase", "pm2d", "batched", "pm3d", "collisions"],
+    ap.add_argument("--row", choices=["frame", "broadphase", "pm2d", "batched", "pm3d", "collisions", "stream"],
                     help="run only this row's measurement (profiling) and print it")
     ap.add_argument("--row-steps", type=int, default=0, help="steps of the --row measurement (0: default)")
     ap.add_argument("--warmup-cpu", type=int, default=0)
@@ -807,8 +903,12 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         fn = {"frame": measure_frame, "broadphase": measure_broadphase, "pm2d": measure_pm2d,
-              "batched": measure_batched, "pm3d": measure_pm3d_learned, "collisions": measure_collisions}[args.row]
-        kw = {"steps": args.row_steps} if args.row_steps and args.row not in ("broadphase", "collisions") else {}
+              "batched": measure_batched, "pm3d": measure_pm3d_learned, "collisions": measure_collisions,
+              "stream": measure_stream}[args.row]
+        kw = ({"steps": args.row_steps} if args.row_steps and args.row not in ("broadphase", "collisions", "stream")
+              else {})
+        if args.row == "stream" and args.row_steps:
+            kw = {"samples": args.row_steps}
         if args.row == "collisions" and args.row_steps:
             kw = {"samples": args.row_steps}
         if args.row == "broadphase" and args.row_steps:

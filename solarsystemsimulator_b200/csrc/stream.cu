@@ -15,8 +15,14 @@
 // body with the bilinear rate and the SplitMix64 hash of its index. The kept
 // bodies are compacted in ascending order (the reference's np.sort of the
 // concatenated tiers) and quantised in the same pass.
+//
+// The bisection resolves 5 halvings per round: the sum is monotone in s
+// (every term is, and rounded addition is monotone), so the 31 midpoints of
+// the next 5 levels of the halving tree can be summed at once and the 5
+// decisions read off them afterwards, each midpoint formed by the same
+// arithmetic as the sequential halving.
 
-#include "devscan.cuh"
+#include "sss_internal.cuh"
 
 #include <algorithm>
 
@@ -24,7 +30,7 @@ namespace {
 
 constexpr int K = 512;                 // LOD cells per axis (server.py LOD_ZELLEN)
 constexpr int K2 = K * K;
-constexpr int LEAVES = K2 / 128;       // 2048 pairwise-sum leaves
+constexpr int LEAVES = K2 / 128;       // 2048 pairwise-sum leaves of 128 cells
 constexpr double LOG33 = 3.4965075614664802;     // log(33) as the double the reference holds
 constexpr float LOG33F = (float)LOG33;           // cast to f32 as NumPy casts the weak scalar
 
@@ -43,83 +49,9 @@ __global__ void k_disp(const float* __restrict__ x, const float* __restrict__ y,
     qy[i] = __fmul_rn(y[i], sk);
 }
 
-// tier per body: 0 culled out, 1 massive, 2 asteroid, 3 injected asteroid
-__global__ void k_cull(const float* __restrict__ qx, const float* __restrict__ qy, const double* __restrict__ kill_t,
-                       double t_cut, const unsigned char* __restrict__ is_ast,
-                       const unsigned char* __restrict__ injected, long long n, Box b,
-                       unsigned char* __restrict__ tier, unsigned long long* __restrict__ cnt4) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    unsigned char t = 0;
-    if (kill_t[i] > t_cut && qx[i] >= b.x0 && qx[i] <= b.x1 && qy[i] >= b.y0 && qy[i] <= b.y1)
-        t = !is_ast[i] ? 1 : (injected && injected[i] ? 3 : 2);
-    tier[i] = t;
-    if (t) atomicAdd(cnt4 + t, 1ull);
-}
-
 __device__ __forceinline__ int cell_of(float q, float o, float s) {
     const int c = (int)__fmul_rn(__fdiv_rn(__fsub_rn(q, o), s), (float)K);
     return min(max(c, 0), K - 1);
-}
-
-// counts of the bodies whose tier is in the mask (bit t = tier t)
-__global__ void k_hist(const float* __restrict__ qx, const float* __restrict__ qy,
-                       const unsigned char* __restrict__ tier, long long n, int mask, Box b,
-                       int* __restrict__ counts) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !((mask >> tier[i]) & 1)) return;
-    atomicAdd(counts + cell_of(qy[i], b.y0, b.sy) * K + cell_of(qx[i], b.x0, b.sx), 1);
-}
-
-__global__ void k_weights(const int* __restrict__ counts, double* __restrict__ w) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < K2) w[c] = counts[c] > 0 ? __dsqrt_rn((double)counts[c]) : 0.0;
-}
-
-// one pairwise-sum leaf of 128 cells of min(count, s w), s = (lo + hi) / 2
-__global__ void k_leaf(const int* __restrict__ counts, const double* __restrict__ w,
-                       const double* __restrict__ lohi, double* __restrict__ leaf) {
-    const int L = blockIdx.x * blockDim.x + threadIdx.x;
-    if (L >= LEAVES) return;
-    const double s = __dmul_rn(0.5, __dadd_rn(lohi[0], lohi[1]));
-    const int base = L * 128;
-    double r[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) r[j] = fmin((double)counts[base + j], __dmul_rn(s, w[base + j]));
-    for (int i = 8; i < 128; i += 8)
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-            r[j] = __dadd_rn(r[j], fmin((double)counts[base + i + j], __dmul_rn(s, w[base + i + j])));
-    leaf[L] = __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), __dadd_rn(r[2], r[3])),
-                        __dadd_rn(__dadd_rn(r[4], r[5]), __dadd_rn(r[6], r[7])));
-}
-
-// pairwise levels over the 2048 leaves (left + right), then the bisection step
-__global__ void __launch_bounds__(1024) k_tree(const double* __restrict__ leaf, double budget,
-                                              double* __restrict__ lohi) {
-    __shared__ double s[LEAVES];
-    for (int i = threadIdx.x; i < LEAVES; i += blockDim.x) s[i] = leaf[i];
-    __syncthreads();
-    for (int m = LEAVES / 2; m >= 1; m >>= 1) {
-        double v = 0.0;
-        if ((int)threadIdx.x < m) v = __dadd_rn(s[2 * threadIdx.x], s[2 * threadIdx.x + 1]);
-        __syncthreads();
-        if ((int)threadIdx.x < m) s[threadIdx.x] = v;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const double sm = __dmul_rn(0.5, __dadd_rn(lohi[0], lohi[1]));
-        if (s[0] > budget) lohi[1] = sm;
-        else lohi[0] = sm;
-    }
-}
-
-__global__ void k_rates(const int* __restrict__ counts, const double* __restrict__ w, const double* __restrict__ lohi,
-                        double* __restrict__ rate) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= K2) return;
-    const double lo = lohi[0];
-    rate[c] = counts[c] > 0 ? __ddiv_rn(fmin((double)counts[c], __dmul_rn(lo, w[c])), (double)counts[c]) : 0.0;
 }
 
 __device__ __forceinline__ double index_hash(unsigned long long h) {
@@ -136,54 +68,9 @@ __device__ __forceinline__ float frac_coord(float q, float o, float s) {
     return fminf(fmaxf(f, 0.0f), (float)(K - 1));
 }
 
-// keep decision of the bodies of the masked tiers; keep[i] = 1, count kept
-__global__ void k_keep(const float* __restrict__ qx, const float* __restrict__ qy,
-                       const unsigned char* __restrict__ tier, long long n, int mask, Box b,
-                       const double* __restrict__ rate, unsigned char* __restrict__ keep,
-                       unsigned long long* __restrict__ kept) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !((mask >> tier[i]) & 1)) return;
-    const float fx = frac_coord(qx[i], b.x0, b.sx), fy = frac_coord(qy[i], b.y0, b.sy);
-    const int ix = (int)floorf(fx), iy = (int)floorf(fy);
-    const int ix1 = min(ix + 1, K - 1), iy1 = min(iy + 1, K - 1);
-    const double tx = __dsub_rn((double)fx, (double)ix), ty = __dsub_rn((double)fy, (double)iy);
-    const double ux = __dsub_rn(1.0, tx), uy = __dsub_rn(1.0, ty);
-    double rp = __dmul_rn(__dmul_rn(rate[iy * K + ix], ux), uy);
-    rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(rate[iy * K + ix1], tx), uy));
-    rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(rate[iy1 * K + ix], ux), ty));
-    rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(rate[iy1 * K + ix1], tx), ty));
-    if (index_hash((unsigned long long)i) < rp) {
-        keep[i] = 1;
-        atomicAdd(kept, 1ull);
-    }
-}
-
-// keep[i] = 1 for every body of the masked tiers (a tier under its budget)
-__global__ void k_keep_all(const unsigned char* __restrict__ tier, long long n, int mask,
-                           unsigned char* __restrict__ keep) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && ((mask >> tier[i]) & 1)) keep[i] = 1;
-}
-
-__global__ void k_keep_flags(const unsigned char* __restrict__ keep, long long n, long long* __restrict__ f) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) f[i] = keep[i];
-}
-
 __device__ __forceinline__ unsigned short quant(float q, float o, float s) {
     const float v = __fmul_rn(__fdiv_rn(__fsub_rn(q, o), s), 65535.0f);
     return (unsigned short)fminf(fmaxf(v, 0.0f), 65535.0f);
-}
-
-__global__ void k_emit(const float* __restrict__ qx, const float* __restrict__ qy, const long long* __restrict__ f,
-                       const long long* __restrict__ pos, long long n, Box b, unsigned* __restrict__ sel,
-                       unsigned short* __restrict__ ox, unsigned short* __restrict__ oy) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !f[i]) return;
-    const long long q = pos[i];
-    sel[q] = (unsigned)i;
-    ox[q] = quant(qx[i], b.x0, b.sx);
-    oy[q] = quant(qy[i], b.y0, b.sy);
 }
 
 __global__ void k_minmax(const float* __restrict__ qx, const float* __restrict__ qy, long long n,
@@ -216,61 +103,494 @@ __global__ void k_minmax(const float* __restrict__ qx, const float* __restrict__
 size_t al(size_t b) { return (b + 255) / 256 * 256; }
 unsigned nb(long long n) { return (unsigned)((n + 255) / 256); }
 
+// ---------------------------------------------------------------- one sample
+// The whole sample is one cooperative launch of SAMPLE_THREADS-thread blocks,
+// all resident at once; its phases are separated by grid barriers:
+//   cull      display coordinates, tier per body (keep = 0), tier counts
+//   (plan)    every block reads the tier counts and takes the reference's
+//             branch of _lod_auswahl; the plan is uniform over the grid
+//   filter    per thinned tier: cell counts (hist), 8 bisection rounds of
+//             5 halvings each (group sums, then every block adds the top
+//             levels and walks the same decisions), rates, keep decisions
+//   emit      per-block kept counts, then each block places its contiguous
+//             range of bodies in ascending order
+// A barrier wait polls at most BARRIER_POLLS times; when it runs out the
+// block records SSS_ERR_TIMEOUT and every block returns at its next barrier.
+constexpr int SAMPLE_THREADS = 512;
+constexpr int SAMPLE_WARPS = SAMPLE_THREADS / 32;
+constexpr unsigned BARRIER_POLLS = 1u << 21;        // about a second with the 32 ns back-off
+constexpr int HIST_CHUNK = SAMPLE_THREADS * 4;      // bodies per shared-memory table fill
+constexpr int HIST_SLOTS = 2 * HIST_CHUNK;          // 4096: the hash yields 12 bits
+constexpr int EMIT_SUB = SAMPLE_THREADS * 4;        // bodies per block scan in the emit phase
+constexpr int BISECT_D = 5;                         // halvings per round
+constexpr int CAND = (1 << BISECT_D) - 1;           // 31 midpoints per round, lanes 0..30
+constexpr int GROUP_LEAVES = SAMPLE_WARPS;          // 16 leaves of 128 cells per group (warp = leaf)
+constexpr int GROUP_CELLS = GROUP_LEAVES * 128;
+constexpr int GROUPS = LEAVES / GROUP_LEAVES;       // 128 groups
+static_assert(HIST_SLOTS == 1 << 12, "12-bit hash");
+static_assert(CAND < 32, "one lane per candidate");
+static_assert(40 % BISECT_D == 0, "whole rounds of halvings");
+
+struct Ctl {                                        // zeroed before every launch
+    unsigned bar;                                   // grid barrier arrivals
+    int err;
+    unsigned long long tier_cnt[4];
+    unsigned long long kept[2];
+    long long total;
+};
+
+struct SampleArgs {
+    const float* x;
+    const float* y;
+    const double* kill_t;
+    const unsigned char* is_ast;
+    const unsigned char* injected;                  // may be NULL
+    double t_cut;
+    Box b;
+    int log_zoom;
+    long long n, budget;
+    float* qx;                                      // display coordinates (log zoom), n
+    float* qy;
+    unsigned char* tier;                            // n
+    unsigned char* keep;                            // n
+    int* counts;                                    // K2 cell counts (cleared in the cull phase)
+    double* rate;                                   // K2 rate quads (4 doubles per cell)
+    double* part;                                   // 2 x CAND x GROUPS group sums
+    long long* blockcnt;                            // gridDim.x
+    unsigned* sel;
+    unsigned short* ox;
+    unsigned short* oy;
+    Ctl* ctl;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// false: a wait ran out here or in another block (the caller returns)
+__device__ __forceinline__ bool grid_barrier(Ctl* ctl, unsigned& epoch, int* s_bad) {
+    ++epoch;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // release: the block's writes (ordered before this thread by the
+        // block barrier) become visible with the arrival; acquire: the
+        // other blocks' writes are visible once their arrivals are seen
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&ctl->bar) : "memory");
+        const unsigned target = epoch * gridDim.x;
+        int bad = 0;
+        for (unsigned polls = 0; ld_acquire_u32(&ctl->bar) < target; ++polls) {
+            if (polls >= BARRIER_POLLS || *(volatile int*)&ctl->err) {
+                atomicExch(&ctl->err, SSS_ERR_TIMEOUT);
+                bad = 1;
+                break;
+            }
+            __nanosleep(32);
+        }
+        *s_bad = bad;
+    }
+    __syncthreads();
+    return !*s_bad;
+}
+
+__device__ __forceinline__ long long block_sum_ll(long long v, long long* s_red) {
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    long long t = 0;
+#pragma unroll
+    for (int w = 0; w < SAMPLE_WARPS; ++w) t += s_red[w];
+    return t;
+}
+
+// midpoint of heap node h (1-based) of the halving tree below [lo, hi]
+__device__ __forceinline__ double node_mid(int h, double lo, double hi) {
+    const int depth = 31 - __clz(h);
+    for (int b = depth - 1; b >= 0; --b) {
+        const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
+        if ((h >> b) & 1) lo = s;
+        else hi = s;
+    }
+    return __dmul_rn(0.5, __dadd_rn(lo, hi));
+}
+
+// weight of a cell: count ** 0.5 (a correctly rounded square root)
+__device__ __forceinline__ double cell_weight(int c) { return c > 0 ? __dsqrt_rn((double)c) : 0.0; }
+
+struct Smem {
+    union {
+        struct {                                    // hist phase
+            int key[HIST_SLOTS];
+            int val[HIST_SLOTS];
+        } h;
+        struct {                                    // bisection: one group's cells
+            double c[GROUP_CELLS];
+            double w[GROUP_CELLS];
+        } g;
+    } u;
+    double leaf[GROUP_LEAVES][32];
+    double tot[32];
+    long long red[SAMPLE_WARPS];
+    int wcnt[SAMPLE_WARPS];
+    int bad;
+};
+
+// Cell counts of the bodies whose tier is in mask: each block fills a
+// shared-memory open-addressing table from HIST_CHUNK bodies (dense clouds
+// put many bodies of a chunk into a few cells) and adds every distinct cell
+// to the global counts once. The table has twice the chunk's slots, so a
+// probe ends within HIST_SLOTS steps.
+__device__ void phase_hist(const SampleArgs& a, const float* qx, const float* qy, int mask, Smem& sm) {
+    for (long long c0 = (long long)blockIdx.x * HIST_CHUNK; c0 < a.n; c0 += (long long)gridDim.x * HIST_CHUNK) {
+        for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS) {
+            sm.u.h.key[j] = -1;
+            sm.u.h.val[j] = 0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < HIST_CHUNK / SAMPLE_THREADS; ++r) {
+            const long long i = c0 + (long long)r * SAMPLE_THREADS + threadIdx.x;
+            if (i >= a.n) break;
+            const unsigned char t = __ldcg(a.tier + i);
+            if (!((mask >> t) & 1)) continue;
+            const int c = cell_of(__ldcg(qy + i), a.b.y0, a.b.sy) * K + cell_of(__ldcg(qx + i), a.b.x0, a.b.sx);
+            unsigned h = ((unsigned)c * 2654435761u) >> 20;       // Fibonacci hash to 12 bits
+            for (int probe = 0; probe < HIST_SLOTS; ++probe) {
+                const int prev = atomicCAS(sm.u.h.key + h, -1, c);
+                if (prev == -1 || prev == c) {
+                    atomicAdd(sm.u.h.val + h, 1);
+                    break;
+                }
+                h = (h + 1) & (HIST_SLOTS - 1);
+            }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS)
+            if (sm.u.h.key[j] >= 0) atomicAdd(a.counts + sm.u.h.key[j], sm.u.h.val[j]);
+        __syncthreads();
+    }
+}
+
+// Group sums of the CAND midpoints below [lo, hi] for the groups of this
+// block: warp = leaf of 128 cells (NumPy's pairwise leaf: eight interleaved
+// partial sums, combined ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7))), lane =
+// midpoint; then the 4 pairwise levels over the group's 16 leaves. A leaf of
+// empty cells sums to +0 for every midpoint, as its terms min(0, s * 0) = +0
+// do; in a leaf with occupied cells the +0 terms of its empty cells are added
+// like the others (exactly).
+__device__ void phase_group_sums(const SampleArgs& a, double lo, double hi, double* part, Smem& sm) {
+    const int leaf = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int g = blockIdx.x; g < GROUPS; g += gridDim.x) {
+        constexpr int PER_T = GROUP_CELLS / SAMPLE_THREADS;
+        int cv[PER_T];
+#pragma unroll
+        for (int k = 0; k < PER_T; ++k) cv[k] = __ldcg(a.counts + g * GROUP_CELLS + k * SAMPLE_THREADS + threadIdx.x);
+#pragma unroll
+        for (int k = 0; k < PER_T; ++k) {
+            sm.u.g.c[k * SAMPLE_THREADS + threadIdx.x] = (double)cv[k];
+            sm.u.g.w[k * SAMPLE_THREADS + threadIdx.x] = cell_weight(cv[k]);
+        }
+        __syncthreads();
+        bool occ = false;
+        for (int j = lane; j < 128; j += 32) occ |= sm.u.g.c[leaf * 128 + j] != 0.0;
+        occ = __any_sync(0xffffffffu, occ);
+        if (lane < CAND) {
+            double sum = 0.0;
+            if (occ) {
+                const double s = node_mid(lane + 1, lo, hi);
+                const double* c = sm.u.g.c + leaf * 128;
+                const double* w = sm.u.g.w + leaf * 128;
+                double r[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) r[j] = fmin(c[j], __dmul_rn(s, w[j]));
+                for (int i = 8; i < 128; i += 8)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) r[j] = __dadd_rn(r[j], fmin(c[i + j], __dmul_rn(s, w[i + j])));
+                sum = __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), __dadd_rn(r[2], r[3])),
+                                __dadd_rn(__dadd_rn(r[4], r[5]), __dadd_rn(r[6], r[7])));
+            }
+            sm.leaf[leaf][lane] = sum;
+        }
+        __syncthreads();
+        for (int m = GROUP_LEAVES / 2; m >= 1; m >>= 1) {
+            double v = 0.0;
+            if (leaf < m && lane < CAND) v = __dadd_rn(sm.leaf[2 * leaf][lane], sm.leaf[2 * leaf + 1][lane]);
+            __syncthreads();
+            if (leaf < m && lane < CAND) sm.leaf[leaf][lane] = v;
+            __syncthreads();
+        }
+        if (threadIdx.x < CAND) part[threadIdx.x * GROUPS + g] = sm.leaf[0][threadIdx.x];
+        __syncthreads();
+    }
+}
+
+// the top 7 pairwise levels over the 128 group sums of every midpoint (a
+// warp per midpoint: lane l adds groups 4l..4l+3 in two levels, then five
+// shuffle levels pair lanes (l, l + d) for d = 1, 2, 4, 8, 16), then the
+// BISECT_D decisions, taken alike by every block
+static_assert(GROUPS == 4 * 32, "four group sums per lane");
+__device__ void phase_walk(const double* part, double budget, double& lo, double& hi, Smem& sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = warp; c < CAND; c += SAMPLE_WARPS) {
+        const double2 p0 = __ldcg((const double2*)(part + c * GROUPS + 4 * lane));
+        const double2 p1 = __ldcg((const double2*)(part + c * GROUPS + 4 * lane + 2));
+        double v = __dadd_rn(__dadd_rn(p0.x, p0.y), __dadd_rn(p1.x, p1.y));
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, v, d);
+            if ((lane & (2 * d - 1)) == 0) v = __dadd_rn(v, o);
+        }
+        if (lane == 0) sm.tot[c] = v;
+    }
+    __syncthreads();
+    int node = 1;
+    for (int d = 0; d < BISECT_D; ++d) {
+        const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
+        if (sm.tot[node - 1] > budget) {
+            hi = s;
+            node = 2 * node;
+        } else {
+            lo = s;
+            node = 2 * node + 1;
+        }
+    }
+}
+
+// The reference's _dichte_filter over the tiers in mask with `budget`
+// points (size > budget); keep[i] = 1 for the kept bodies, their number in
+// ctl->kept[slot]. Returns false when a barrier gave up.
+__device__ bool filter(const SampleArgs& a, const float* qx, const float* qy, int mask, long long budget, int slot,
+                       unsigned& epoch, Smem& sm) {
+    phase_hist(a, qx, qy, mask, sm);
+    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
+    double lo = 0.0, hi = (double)budget;
+    for (int round = 0; round < 40 / BISECT_D; ++round) {
+        double* part = a.part + (round & 1) * CAND * GROUPS;
+        phase_group_sums(a, lo, hi, part, sm);
+        if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
+        phase_walk(part, (double)budget, lo, hi, sm);
+    }
+    const long long T = (long long)gridDim.x * SAMPLE_THREADS;
+    const long long gt = (long long)blockIdx.x * SAMPLE_THREADS + threadIdx.x;
+    // rate quad of cell (iy, ix): the rates of (iy, ix), (iy, ix1), (iy1, ix),
+    // (iy1, ix1), the four a body's bilinear rate reads, in one 32-byte sector
+    for (long long c = gt; c < K2; c += T) {
+        const int ix = (int)(c % K), iy = (int)(c / K);
+        const int ix1 = min(ix + 1, K - 1), iy1 = min(iy + 1, K - 1);
+        const int cells[4] = {iy * K + ix, iy * K + ix1, iy1 * K + ix, iy1 * K + ix1};
+        double r[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = __ldcg(a.counts + cells[q]);
+            r[q] = k > 0 ? __ddiv_rn(fmin((double)k, __dmul_rn(lo, cell_weight(k))), (double)k) : 0.0;
+        }
+        double2* dst = (double2*)(a.rate + 4 * c);
+        dst[0] = make_double2(r[0], r[1]);
+        dst[1] = make_double2(r[2], r[3]);
+    }
+    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
+    const unsigned char* __restrict__ tier = a.tier;
+    unsigned char* __restrict__ keep = a.keep;
+    long long kept = 0;
+    for (long long i0 = gt; i0 < a.n; i0 += 2 * T) {
+        unsigned char t[2];
+        float px[2], py[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const long long i = i0 + u * T;
+            t[u] = i < a.n ? __ldcg(tier + i) : 0;
+            px[u] = i < a.n ? __ldcg(qx + i) : 0.0f;
+            py[u] = i < a.n ? __ldcg(qy + i) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (!((mask >> t[u]) & 1)) continue;
+            const long long i = i0 + u * T;
+            const float fx = frac_coord(px[u], a.b.x0, a.b.sx), fy = frac_coord(py[u], a.b.y0, a.b.sy);
+            const int ix = (int)floorf(fx), iy = (int)floorf(fy);
+            const double2* rq = (const double2*)(a.rate + 4 * (iy * K + ix));
+            const double2 r0 = __ldcg(rq), r1 = __ldcg(rq + 1);
+            const double tx = __dsub_rn((double)fx, (double)ix), ty = __dsub_rn((double)fy, (double)iy);
+            const double ux = __dsub_rn(1.0, tx), uy = __dsub_rn(1.0, ty);
+            double rp = __dmul_rn(__dmul_rn(r0.x, ux), uy);
+            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r0.y, tx), uy));
+            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r1.x, ux), ty));
+            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r1.y, tx), ty));
+            if (index_hash((unsigned long long)i) < rp) {
+                keep[i] = 1;
+                ++kept;
+            }
+        }
+    }
+    // the cell counts are dead now (the rates hold what the keep decisions
+    // need): clear them for a following filter
+    for (long long c = gt; c < K2; c += T) a.counts[c] = 0;
+    kept = block_sum_ll(kept, sm.red);
+    if (threadIdx.x == 0 && kept) atomicAdd(a.ctl->kept + slot, (unsigned long long)kept);
+    return grid_barrier(a.ctl, epoch, &sm.bad);
+}
+
+__global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
+    __shared__ Smem sm;
+    unsigned epoch = 0;
+    const long long T = (long long)gridDim.x * SAMPLE_THREADS;
+    const long long gt = (long long)blockIdx.x * SAMPLE_THREADS + threadIdx.x;
+    const float* qx = a.log_zoom ? a.qx : a.x;
+    const float* qy = a.log_zoom ? a.qy : a.y;
+    // ---- cull
+    long long n1 = 0, n2 = 0, n3 = 0;
+    for (long long c = gt; c < K2; c += T) a.counts[c] = 0;
+    for (long long i = gt; i < a.n; i += T) {
+        float px = a.x[i], py = a.y[i];
+        const double kt = a.kill_t[i];
+        const unsigned char ast = a.is_ast[i], inj = a.injected ? a.injected[i] : 0;
+        if (a.log_zoom) {
+            const float r = hypotf(px, py);
+            const float sk = r > 1e-9f ? __fdiv_rn(log1pf(r), __fmul_rn(LOG33F, fmaxf(r, 1e-30f))) : 0.0f;
+            px = __fmul_rn(px, sk);
+            py = __fmul_rn(py, sk);
+            a.qx[i] = px;
+            a.qy[i] = py;
+        }
+        unsigned char t = 0;
+        if ((kt > a.t_cut) & (px >= a.b.x0) & (px <= a.b.x1) & (py >= a.b.y0) & (py <= a.b.y1))
+            t = !ast ? 1 : (inj ? 3 : 2);
+        a.tier[i] = t;
+        a.keep[i] = 0;
+        n1 += t == 1;
+        n2 += t == 2;
+        n3 += t == 3;
+    }
+    n1 = block_sum_ll(n1, sm.red);
+    n2 = block_sum_ll(n2, sm.red);
+    n3 = block_sum_ll(n3, sm.red);
+    if (threadIdx.x == 0) {
+        if (n1) atomicAdd(a.ctl->tier_cnt + 1, (unsigned long long)n1);
+        if (n2) atomicAdd(a.ctl->tier_cnt + 2, (unsigned long long)n2);
+        if (n3) atomicAdd(a.ctl->tier_cnt + 3, (unsigned long long)n3);
+    }
+    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return;
+    // ---- plan (the reference's _lod_auswahl), identical in every block
+    const long long mm = (long long)__ldcg(a.ctl->tier_cnt + 1), ma = (long long)__ldcg(a.ctl->tier_cnt + 2),
+                    mi = (long long)__ldcg(a.ctl->tier_cnt + 3);
+    const long long m = mm + ma + mi;
+    const int T_ALL = (1 << 1) | (1 << 2) | (1 << 3), T_MASS = 1 << 1, T_AST = (1 << 2) | (1 << 3);
+    int all_mask = 0;
+    if (m <= a.budget) {
+        all_mask = T_ALL;
+    } else {
+        long long rest = a.budget - mm;
+        if (rest <= 0) {
+            if (mm > 200 && m > mm) {
+                // many massive bodies (a self-gravity cloud): they get half the budget, thinned
+                const long long m_budget = max(1LL, (long long)((double)a.budget * 0.5));
+                long long kept = mm;
+                if (mm <= m_budget) {
+                    all_mask |= T_MASS;
+                } else {
+                    if (!filter(a, qx, qy, T_MASS, m_budget, 0, epoch, sm)) return;
+                    kept = (long long)__ldcg(a.ctl->kept + 0);
+                }
+                rest = a.budget - kept;
+                if (rest > 0 && ma + mi > 0) {
+                    if (ma + mi <= rest) all_mask |= T_AST;
+                    else if (!filter(a, qx, qy, T_AST, rest, 1, epoch, sm)) return;
+                }
+            } else {
+                all_mask = T_MASS;
+            }
+        } else {
+            all_mask = T_MASS;
+            const long long sizes[2] = {ma, mi};
+            const int masks[2] = {1 << 2, 1 << 3};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (rest <= 0 || sizes[q] == 0) continue;
+                long long kept = sizes[q];
+                if (sizes[q] <= rest) {
+                    all_mask |= masks[q];
+                } else {
+                    if (!filter(a, qx, qy, masks[q], rest, q, epoch, sm)) return;
+                    kept = (long long)__ldcg(a.ctl->kept + q);
+                }
+                rest -= kept;
+            }
+        }
+    }
+    // ---- emit: block b owns bodies [b * chunk, (b + 1) * chunk)
+    const long long chunk = ((a.n + gridDim.x - 1) / gridDim.x + EMIT_SUB - 1) / EMIT_SUB * EMIT_SUB;
+    const long long c0 = (long long)blockIdx.x * chunk, c1 = min(c0 + chunk, a.n);
+    long long mine = 0;
+    for (long long i = c0 + threadIdx.x; i < c1; i += SAMPLE_THREADS)
+        mine += __ldcg(a.keep + i) | ((all_mask >> __ldcg(a.tier + i)) & 1);
+    mine = block_sum_ll(mine, sm.red);
+    if (threadIdx.x == 0) a.blockcnt[blockIdx.x] = mine;
+    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return;
+    long long before = 0;
+    for (int j = threadIdx.x; j < (int)blockIdx.x; j += SAMPLE_THREADS) before += __ldcg(a.blockcnt + j);
+    long long off = block_sum_ll(before, sm.red);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (long long s0 = c0; s0 < c1; s0 += EMIT_SUB) {
+        const long long i0 = s0 + (long long)threadIdx.x * 4;
+        unsigned bits = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const long long i = i0 + j;
+            if (i < c1 && (__ldcg(a.keep + i) | ((all_mask >> __ldcg(a.tier + i)) & 1))) bits |= 1u << j;
+        }
+        const int c = __popc(bits);
+        int inc = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (lane == 31) sm.wcnt[warp] = inc;
+        __syncthreads();
+        int wb = 0, all = 0;
+#pragma unroll
+        for (int w = 0; w < SAMPLE_WARPS; ++w) {
+            const int v = sm.wcnt[w];
+            wb += w < warp ? v : 0;
+            all += v;
+        }
+        long long q = off + wb + inc - c;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!((bits >> j) & 1)) continue;
+            const long long i = i0 + j;
+            a.sel[q] = (unsigned)i;
+            a.ox[q] = quant(__ldcg(qx + i), a.b.x0, a.b.sx);
+            a.oy[q] = quant(__ldcg(qy + i), a.b.y0, a.b.sy);
+            ++q;
+        }
+        off += all;
+        __syncthreads();                            // wcnt is rewritten by the next sub-range
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) a.ctl->total = off;
+}
+
 struct Work {
     float *qx, *qy;
     unsigned char *tier, *keep;
     int* counts;
-    double *w, *rate, *leaf, *lohi;
-    unsigned long long* cnt;           // [0..3] tier counts, [4] kept
-    long long *flags, *pos, *scan;
+    double *rate, *part;
+    long long* blockcnt;
+    Ctl* ctl;
 };
 
-// density filter of the masked tiers with `budget` points (the reference's
-// _dichte_filter); returns the number kept (all of them when under budget)
-int density_filter(sss_ctx* ctx, const Work& W, long long n, int mask, long long size, long long budget, Box b,
-                   cudaStream_t st, long long* kept) {
-    if (size <= budget) {
-        k_keep_all<<<nb(n), 256, 0, st>>>(W.tier, n, mask, W.keep);
-        SSS_LAUNCH_CHECK(ctx, "k_keep_all");
-        *kept = size;
-        return SSS_OK;
-    }
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.counts, 0, K2 * sizeof(int), st));
-    k_hist<<<nb(n), 256, 0, st>>>(W.qx, W.qy, W.tier, n, mask, b, W.counts);
-    SSS_LAUNCH_CHECK(ctx, "k_hist");
-    k_weights<<<K2 / 256, 256, 0, st>>>(W.counts, W.w);
-    const double lohi0[2] = {0.0, (double)budget};
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(W.lohi, lohi0, sizeof(lohi0), cudaMemcpyHostToDevice, st));
-    for (int it = 0; it < 40; ++it) {
-        k_leaf<<<LEAVES / 256, 256, 0, st>>>(W.counts, W.w, W.lohi, W.leaf);
-        k_tree<<<1, 1024, 0, st>>>(W.leaf, (double)budget, W.lohi);
-    }
-    k_rates<<<K2 / 256, 256, 0, st>>>(W.counts, W.w, W.lohi, W.rate);
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.cnt + 4, 0, 8, st));
-    k_keep<<<nb(n), 256, 0, st>>>(W.qx, W.qy, W.tier, n, mask, b, W.rate, W.keep, W.cnt + 4);
-    SSS_LAUNCH_CHECK(ctx, "k_keep");
-    unsigned long long k = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&k, W.cnt + 4, 8, cudaMemcpyDeviceToHost, st));
-    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    *kept = (long long)k;
-    return SSS_OK;
-}
-
-int make_work(sss_ctx* ctx, long long n, Work* W) {
+int make_work(sss_ctx* ctx, long long n, int grid, Work* W) {
     size_t off = 0;
     const size_t o_qx = off; off += al((size_t)n * 4);
     const size_t o_qy = off; off += al((size_t)n * 4);
     const size_t o_tier = off; off += al((size_t)n);
     const size_t o_keep = off; off += al((size_t)n);
     const size_t o_cnts = off; off += al((size_t)K2 * 4);
-    const size_t o_w = off; off += al((size_t)K2 * 8);
-    const size_t o_rate = off; off += al((size_t)K2 * 8);
-    const size_t o_leaf = off; off += al((size_t)LEAVES * 8);
-    const size_t o_lohi = off; off += al(16);
-    const size_t o_cnt = off; off += al(8 * 8);
-    const size_t o_flags = off; off += al((size_t)n * 8);
-    const size_t o_pos = off; off += al((size_t)n * 8);
-    const size_t o_scan = off; off += al(sss_dev::scan_scratch(n) * 8);
+    const size_t o_rate = off; off += al((size_t)K2 * 32);
+    const size_t o_part = off; off += al((size_t)2 * CAND * GROUPS * 8);
+    const size_t o_blk = off; off += al((size_t)grid * 8);
+    const size_t o_ctl = off; off += al(sizeof(Ctl));
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off, &scr);
     if (rc) return rc;
@@ -280,14 +600,24 @@ int make_work(sss_ctx* ctx, long long n, Work* W) {
     W->tier = (unsigned char*)(p + o_tier);
     W->keep = (unsigned char*)(p + o_keep);
     W->counts = (int*)(p + o_cnts);
-    W->w = (double*)(p + o_w);
     W->rate = (double*)(p + o_rate);
-    W->leaf = (double*)(p + o_leaf);
-    W->lohi = (double*)(p + o_lohi);
-    W->cnt = (unsigned long long*)(p + o_cnt);
-    W->flags = (long long*)(p + o_flags);
-    W->pos = (long long*)(p + o_pos);
-    W->scan = (long long*)(p + o_scan);
+    W->part = (double*)(p + o_part);
+    W->blockcnt = (long long*)(p + o_blk);
+    W->ctl = (Ctl*)(p + o_ctl);
+    return SSS_OK;
+}
+
+// blocks of one cooperative k_sample launch: every SM's resident blocks, at most 2 per SM
+int sample_grid(sss_ctx* ctx, int* grid) {
+    static int per_sm_of[64];                       // per device ordinal, 0 = not queried yet
+    const int dev = ctx->device;
+    int per_sm = dev >= 0 && dev < 64 ? per_sm_of[dev] : 0;
+    if (per_sm == 0) {
+        SSS_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sample, SAMPLE_THREADS, 0));
+        if (per_sm < 1) return sss_set_err(ctx, SSS_ERR_CUDA, "k_sample: no resident block per SM");
+        if (dev >= 0 && dev < 64) per_sm_of[dev] = per_sm;
+    }
+    *grid = ctx->num_sms * std::min(per_sm, 2);
     return SSS_OK;
 }
 
@@ -299,7 +629,7 @@ extern "C" int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const 
     if (n < 1 || !x || !y || !out4) return sss_set_err(ctx, SSS_ERR_ARG, "minmax: empty or NULL input");
     cudaStream_t st = (cudaStream_t)stream;
     Work W;
-    int rc = make_work(ctx, n, &W);
+    int rc = make_work(ctx, n, 1, &W);
     if (rc) return rc;
     const float* qx = x;
     const float* qy = y;
@@ -310,7 +640,7 @@ extern "C" int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const 
         qy = W.qy;
     }
     const int blocks = (int)std::min<long long>(nb(n), 256);
-    float* part = (float*)W.w;                   // 4 floats per block
+    float* part = (float*)W.rate;                // 4 floats per block
     k_minmax<<<blocks, 256, 0, st>>>(qx, qy, n, part);
     SSS_LAUNCH_CHECK(ctx, "k_minmax");
     float h[4 * 256];
@@ -336,81 +666,51 @@ extern "C" int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const 
     *n_sel = 0;
     if (n < 0 || budget < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
     if (n == 0) return SSS_OK;
+    if (n > 0xFFFFFFFFLL) return sss_set_err(ctx, SSS_ERR_ARG, "more than 2^32 bodies (u32 indices)");
     if (!x || !y || !kill_t || !is_ast || !sel || !qx_out || !qy_out)
         return sss_set_err(ctx, SSS_ERR_ARG, "NULL array");
     cudaStream_t st = (cudaStream_t)stream;
-    Work W;
-    int rc = make_work(ctx, n, &W);
+    int grid = 0;
+    int rc = sample_grid(ctx, &grid);
     if (rc) return rc;
-    Box b;
-    b.x0 = (float)box[0];
-    b.y0 = (float)box[1];
-    b.sx = (float)box[2];
-    b.sy = (float)box[3];
-    b.x1 = (float)(box[0] + box[2]);
-    b.y1 = (float)(box[1] + box[3]);
-    const float* qx = x;
-    const float* qy = y;
-    if (log_zoom) {
-        k_disp<<<nb(n), 256, 0, st>>>(x, y, n, W.qx, W.qy);
-        SSS_LAUNCH_CHECK(ctx, "k_disp");
-        qx = W.qx;
-        qy = W.qy;
-    }
-    W.qx = (float*)qx;
-    W.qy = (float*)qy;
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.cnt, 0, 8 * 8, st));
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.keep, 0, (size_t)n, st));
-    k_cull<<<nb(n), 256, 0, st>>>(qx, qy, kill_t, t_cut, is_ast, injected, n, b, W.tier, W.cnt);
-    SSS_LAUNCH_CHECK(ctx, "k_cull");
-    unsigned long long c[4] = {0, 0, 0, 0};
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(c, W.cnt, sizeof(c), cudaMemcpyDeviceToHost, st));
+    Work W;
+    rc = make_work(ctx, n, grid, &W);
+    if (rc) return rc;
+    SampleArgs a;
+    a.x = x;
+    a.y = y;
+    a.kill_t = kill_t;
+    a.is_ast = is_ast;
+    a.injected = injected;
+    a.t_cut = t_cut;
+    a.b.x0 = (float)box[0];
+    a.b.y0 = (float)box[1];
+    a.b.sx = (float)box[2];
+    a.b.sy = (float)box[3];
+    a.b.x1 = (float)(box[0] + box[2]);
+    a.b.y1 = (float)(box[1] + box[3]);
+    a.log_zoom = log_zoom ? 1 : 0;
+    a.n = n;
+    a.budget = budget;
+    a.qx = W.qx;
+    a.qy = W.qy;
+    a.tier = W.tier;
+    a.keep = W.keep;
+    a.counts = W.counts;
+    a.rate = W.rate;
+    a.part = W.part;
+    a.blockcnt = W.blockcnt;
+    a.sel = sel;
+    a.ox = qx_out;
+    a.oy = qy_out;
+    a.ctl = W.ctl;
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.ctl, 0, sizeof(Ctl), st));
+    void* params[] = {&a};
+    SSS_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void*)k_sample, dim3(grid), dim3(SAMPLE_THREADS), params, 0, st));
+    Ctl h;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
     SSS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    const long long mm = (long long)c[1], ma = (long long)c[2], mi = (long long)c[3];
-    const long long m = mm + ma + mi;
-    const int T_ALL = (1 << 1) | (1 << 2) | (1 << 3), T_MASS = 1 << 1, T_AST = (1 << 2) | (1 << 3);
-    long long kept = 0;
-    if (m <= budget) {
-        k_keep_all<<<nb(n), 256, 0, st>>>(W.tier, n, T_ALL, W.keep);
-        SSS_LAUNCH_CHECK(ctx, "k_keep_all");
-    } else {
-        long long rest = budget - mm;
-        if (rest <= 0) {
-            if (mm > 200 && m > mm) {
-                // many massive bodies (a self-gravity cloud): they get half the budget, thinned
-                const long long m_budget = std::max<long long>(1, (long long)((double)budget * 0.5));
-                rc = density_filter(ctx, W, n, T_MASS, mm, m_budget, b, st, &kept);
-                if (rc) return rc;
-                rest = budget - kept;
-                if (rest > 0 && ma + mi > 0) {
-                    rc = density_filter(ctx, W, n, T_AST, ma + mi, rest, b, st, &kept);
-                    if (rc) return rc;
-                }
-            } else {
-                k_keep_all<<<nb(n), 256, 0, st>>>(W.tier, n, T_MASS, W.keep);
-                SSS_LAUNCH_CHECK(ctx, "k_keep_all");
-            }
-        } else {
-            k_keep_all<<<nb(n), 256, 0, st>>>(W.tier, n, T_MASS, W.keep);
-            SSS_LAUNCH_CHECK(ctx, "k_keep_all");
-            const long long sizes[2] = {ma, mi};
-            const int masks[2] = {1 << 2, 1 << 3};
-            for (int q = 0; q < 2; ++q) {
-                if (rest <= 0 || sizes[q] == 0) continue;
-                rc = density_filter(ctx, W, n, masks[q], sizes[q], rest, b, st, &kept);
-                if (rc) return rc;
-                rest -= kept;
-            }
-        }
-    }
-    k_keep_flags<<<nb(n), 256, 0, st>>>(W.keep, n, W.flags);
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(W.flags, W.pos, n, W.scan, st));
-    k_emit<<<nb(n), 256, 0, st>>>(qx, qy, W.flags, W.pos, n, b, sel, qx_out, qy_out);
-    SSS_LAUNCH_CHECK(ctx, "k_emit");
-    long long tot = 0;
-    const long long tiles = (n + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&tot, W.scan + tiles, 8, cudaMemcpyDeviceToHost, st));
-    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    *n_sel = tot;
+    if (h.err) return sss_set_err(ctx, SSS_ERR_TIMEOUT, "k_sample: a grid barrier wait ran out");
+    *n_sel = h.total;
     return SSS_OK;
 }

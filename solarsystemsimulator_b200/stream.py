@@ -74,13 +74,19 @@ class StreamFrames:
         valid until the next call)."""
         x = x.contiguous()
         y = y.contiguous()
+        for v in (x, y):
+            if v.numel() != self.n or v.dtype != torch.float32 or v.device != self.dev:
+                raise ValueError(f"sample: x and y must be f32 tensors of {self.n} bodies on {self.dev}")
         b = (ctypes.c_double * 4)(*(float(v) for v in box))
         cnt = ctypes.c_int64()
-        with torch.cuda.device(self.device):
-            self.ctx.check(self.ctx.lib.sss_stream_sample(
-                self.ctx.ptr, self.n, x.data_ptr(), y.data_ptr(), self.kill_t.data_ptr(), float(t_i - raster_days),
+        args = (self.ctx.ptr, self.n, x.data_ptr(), y.data_ptr(), self.kill_t.data_ptr(), float(t_i - raster_days),
                 self.d_ast.data_ptr(), self.d_inj.data_ptr() if self.d_inj is not None else None, b,
                 int(bool(log_zoom)), int(budget), self.sel.data_ptr(), self.qx.data_ptr(), self.qy.data_ptr(),
-                ctypes.byref(cnt), self._s()))
+                ctypes.byref(cnt))
+        if torch.cuda.current_device() == self.device:
+            self.ctx.check(self.ctx.lib.sss_stream_sample(*args, self._s()))
+        else:
+            with torch.cuda.device(self.device):
+                self.ctx.check(self.ctx.lib.sss_stream_sample(*args, self._s()))
         m = cnt.value
         return self.sel[:m], self.qx[:m], self.qy[:m]
