@@ -16,20 +16,19 @@
 //   operations, so no fused multiply-add may appear), radii + 1e-6;
 // * ownership: min(x_a, x_b) < hi (f32); exact recheck in f64 of the f32
 //   values, again without contraction.
-// The candidate list is never materialised: one kernel walks the flattened
-// candidate index space (offset-major, then body, then range position — the
-// reference's expansion order) in contiguous chunks per warp, one candidate
-// per lane, tests each pair and appends hits; the partners' values are read
-// from records stored in sorted-key order (one gather per call), so the
-// lanes of a warp read consecutive records. The host
-// sorts the hits by (offset, a, b), which is the reference's output order.
+// The candidate list is never materialised: the sorted bodies are split
+// into runs of one cell; a run and a neighbour offset give a block of
+// candidates (the run's bodies x the bodies with the offset cell's key), cut
+// into tiles of 32 x 256 that warps take one by one, a run body per lane and
+// the partners streamed as broadcast loads from records stored in sorted-key
+// order. Hits are appended; the host sorts them by (offset, a, b), which is
+// the reference's output order.
 
 #include "devscan.cuh"
 
 namespace {
 
 constexpr int BP_NT = 256;
-constexpr int BP_CHUNK = 8192;   // consecutive candidates per warp
 
 __device__ __forceinline__ long long cell_key(long long cx, long long cy) {
     // int64 wrap-around multiply (the reference's `cx * int64(73856093) ^ cy * int64(19349663)`)
@@ -113,22 +112,6 @@ __device__ __forceinline__ long long upper_bound(const unsigned long long* a, lo
 
 __constant__ int c_off[5][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}, {1, -1}};   // film_producer.py:155
 
-// Key range of every (offset, body) segment: start in the sorted keys and length.
-__global__ void k_ranges(const long long* __restrict__ cx, const long long* __restrict__ cy, long long na,
-                         const unsigned long long* __restrict__ ks, long long* __restrict__ seg_lo,
-                         long long* __restrict__ seg_len) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 5 * na) return;
-    const int o = (int)(t / na);
-    const long long r = t - (long long)o * na;
-    const unsigned long long k2 =
-        (unsigned long long)cell_key(cx[r] + c_off[o][0], cy[r] + c_off[o][1]) ^ 0x8000000000000000ull;
-    const long long lo = lower_bound(ks, na, k2);
-    const long long hi = upper_bound(ks, na, k2);
-    seg_lo[t] = lo;
-    seg_len[t] = hi - lo;
-}
-
 struct Hit {
     int o;
     unsigned a, b;
@@ -184,14 +167,7 @@ __global__ void k_sorted_records(const float* __restrict__ x, const float* __res
     rec2[pos] = make_uint2(__float_as_uint(rr[b]), b);
 }
 
-struct CandArgs {
-    const float *x, *y, *vx, *vy, *rr;
-    const unsigned* ai;          // row -> body
-    const float4* rec;           // sorted position -> (x, y, vx, vy) of its body
-    const uint2* rec2;           // sorted position -> (rr bits, body)
-    const long long* seg_lo;     // [5*na]
-    const long long* seg_start;  // [5*na + 1] exclusive prefix of segment lengths
-    long long n_seg, total;
+struct TestParams {
     float dtf, hi;
     double dt;
     Hit* hits;
@@ -209,26 +185,9 @@ __device__ __forceinline__ long long find_segment(const long long* start, long l
     return lo;
 }
 
-// keep rule, f32 prefilter, ownership, f64 recheck, append (film_producer.py:241-314)
-// Pairs that provably fail the f32 test are skipped before it. For every t
-// in [-dt, dt], |dp + dv t| >= |dp| - (|dvx| + |dvy|) dt; if |dp| exceeds
-// twice reach = (|dvx| + |dvy|) dt + rsum, the closest approach is at least
-// 2 rsum. The f32 evaluation of the test errs by a few ulp of |dp|, below
-// 1e-7 AU while |dp| < 1 AU, while rsum >= 1e-6 AU (radii + 1e-6), so such
-// a pair can never pass it: the skip changes no result, only the work.
-__device__ __forceinline__ bool surely_apart(const Body& A, const Body& B, float dtf) {
-    const float dpx = B.x - A.x, dpy = B.y - A.y;
-    const float dp2 = dpx * dpx + dpy * dpy;
-    const float reach = (fabsf(B.vx - A.vx) + fabsf(B.vy - A.vy)) * dtf + (A.rr + B.rr + 1e-6f);
-    return dp2 < 1.0f && dp2 > 4.0001f * reach * reach;
-}
-
-__device__ __forceinline__ void test_pair(const CandArgs& a, int o, unsigned ab, const Body& A, uint2 q, float4 v) {
-    const unsigned bb = q.y;
-    const bool keep = (o == 0) ? (ab < bb) : (ab != bb);
-    if (!keep) return;
-    const Body B{v.x, v.y, v.z, v.w, __uint_as_float(q.x)};
-    if (surely_apart(A, B, a.dtf)) return;
+// ownership and the f64 recheck after the f32 test, then the append (film_producer.py:241-314)
+__device__ __forceinline__ void test_exact(const TestParams& a, int o, unsigned ab, const Body& A, unsigned bb,
+                                           const Body& B) {
     if (!ccd_f32(A, B, a.dtf)) return;
     if (!(fminf(A.x, B.x) < a.hi)) return;          // ownership (:296)
     if (!ccd_f64(A, B, a.dt)) return;
@@ -236,41 +195,298 @@ __device__ __forceinline__ void test_pair(const CandArgs& a, int o, unsigned ab,
     if ((long long)slot < a.cap) a.hits[slot] = Hit{o, ab, bb};
 }
 
-// A warp owns BP_CHUNK consecutive candidates of the flattened space and
-// walks them 32 at a time, lane l taking candidate base + l: the partners'
-// records of a step are consecutive (coalesced), the first body is shared
-// by the lanes of a segment (broadcast). Lane 0 finds the chunk's first
-// segment by binary search; every lane then moves forward through the
-// segment starts as its index grows.
-__global__ void __launch_bounds__(BP_NT) k_candidates(const CandArgs a) {
-    const int lane = threadIdx.x & 31;
-    const long long chunks = (a.total + BP_CHUNK - 1) / BP_CHUNK;
-    const long long na = a.n_seg / 5;
+// Cell runs: consecutive sorted positions whose bodies lie in the same cell
+// (the bodies of two cells with colliding keys interleave in the stable key
+// order; each stretch of one cell is its own run). All bodies of a run have,
+// per neighbour offset, the same partner range (the bodies whose key is the
+// offset cell's key), so the candidates of (run, offset) form a block of
+// run length x range length pairs. The candidate set, and with it the hit
+// set, is the reference's; the order of the hits is restored by sorting them
+// by (offset, a, b).
+__global__ void k_run_flags(const long long* __restrict__ cx, const long long* __restrict__ cy,
+                            const unsigned* __restrict__ order, long long na, long long* __restrict__ flags) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= na) return;
+    bool start = p == 0;
+    if (!start) {
+        const unsigned r = order[p], q = order[p - 1];
+        start = cx[r] != cx[q] || cy[r] != cy[q];
+    }
+    flags[p] = start ? 1 : 0;
+}
+
+__global__ void k_run_starts(const long long* __restrict__ flags, const long long* __restrict__ pos, long long na,
+                             long long* __restrict__ run_start) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < na && flags[p]) run_start[pos[p]] = p;
+}
+
+constexpr int TILE_B = 256;       // partners per tile; a tile is 32 run bodies (one per lane) x TILE_B partners
+
+// Item t = o * n_run + q: run q against the partner range of offset o (its
+// first position and length), its tile count, and the candidates summed per
+// block into n_cand.
+__global__ void __launch_bounds__(256) k_items(const long long* __restrict__ cx, const long long* __restrict__ cy,
+                                               const unsigned* __restrict__ order,
+                                               const unsigned long long* __restrict__ ks, long long na,
+                                               const long long* __restrict__ run_start, long long n_run,
+                                               long long* __restrict__ item_b0, long long* __restrict__ item_nb,
+                                               long long* __restrict__ tiles, unsigned long long* __restrict__ n_cand) {
+    __shared__ unsigned long long bs[8];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long cand = 0;
+    if (t < 5 * n_run) {
+        const int o = (int)(t / n_run);
+        const long long q = t - (long long)o * n_run;
+        const long long p0 = run_start[q], p1 = q + 1 < n_run ? run_start[q + 1] : na;
+        const unsigned r = order[p0];
+        const unsigned long long k2 =
+            (unsigned long long)cell_key(cx[r] + c_off[o][0], cy[r] + c_off[o][1]) ^ 0x8000000000000000ull;
+        const long long lo = lower_bound(ks, na, k2);
+        const long long nb = upper_bound(ks, na, k2) - lo;
+        item_b0[t] = lo;
+        item_nb[t] = nb;
+        tiles[t] = ((p1 - p0 + 31) / 32) * ((nb + TILE_B - 1) / TILE_B);
+        cand = (unsigned long long)(p1 - p0) * (unsigned long long)nb;
+    }
+    for (int d = 16; d; d >>= 1) cand += __shfl_down_sync(0xffffffffu, cand, d);
+    if ((threadIdx.x & 31) == 0) bs[threadIdx.x >> 5] = cand;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long sum = 0;
+        for (int w = 0; w < 8; ++w) sum += bs[w];
+        if (sum) atomicAdd(n_cand, sum);
+    }
+}
+
+struct TileArgs {
+    const float4* rec;           // sorted position -> (x, y, vx, vy)
+    const uint2* rec2;           // sorted position -> (rr bits, body)
+    const long long* run_start;  // [n_run]
+    const long long* item_b0;    // [5 n_run]
+    const long long* item_nb;    // [5 n_run]
+    const long long* tile_start; // [5 n_run + 1] exclusive prefix of the tile counts
+    const unsigned long long* ks; // sorted keys
+    long long na, n_run, n_tiles;
+    TestParams tp;
+};
+
+__device__ __forceinline__ float warp_max(float v) {
+    for (int d = 16; d; d >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d));
+    return v;
+}
+__device__ __forceinline__ float warp_min(float v) {
+    for (int d = 16; d; d >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, d));
+    return v;
+}
+
+// Pairs that provably fail the f32 test are skipped before it. That test
+// evaluates the closest approach |dp + dv t| at some t in [-dt, dt], from
+// the rounded dp = B - A, dv (the same subtractions). For every t,
+// |dp + dv t| >= |dp x dv| / |dv|, the distance of the relative motion's
+// line (dp x dv = dpx dvy - dpy dvx). So a pair is skipped when
+//   (|dp x dv| - E)^2 > 4.01 rs^2 |dv|^2,  rs = (rr_a + 1e-6) + rr_b,
+// i.e. its line passes farther than 2 rs. E bounds the f32 error of the
+// cross product: with |dpx|, |dpy| <= P and |dvx|, |dvy| <= V over the tile,
+// |dpx dvy| + |dpy dvx| <= 2 P V and the error is below 2^-22 of that;
+// E = 2 EPS_CROSS P V with EPS_CROSS = 4e-6 (>= 32 ulp). The skip is taken
+// only when P and V dt stay below 0.5 AU over the whole tile: then the f32
+// test's own rounding moves its distance by less than 1e-7 AU, while
+// rs >= 1e-6 AU, and 4.01 instead of 4 covers the rounding of the
+// comparison and of rs (a few ulp). A skipped pair can never pass the f32
+// test: the skips change no result, only the work.
+constexpr float EPS_CROSS = 4.0e-6f;
+constexpr int QCAP = 64;          // queued pairs per warp (flushed at 32)
+
+// Queue of pairs the line test could not skip (per warp, in shared memory):
+// push the lanes' pairs of this step, and once 32 are queued test them
+// exactly, one per lane (the run body fetched from its lane by shuffles).
+struct PairQueue {
+    int* j;
+    unsigned char* l;
+    int cnt;
+};
+
+__device__ __forceinline__ void queue_flush(PairQueue& q, int n, const TileArgs& a, int o, const Body& A,
+                                            unsigned ab, int lane) {
+    const int src = lane < n ? q.l[lane] : 0;
+    const int jj = lane < n ? q.j[lane] : 0;
+    const Body As{__shfl_sync(0xffffffffu, A.x, src), __shfl_sync(0xffffffffu, A.y, src),
+                  __shfl_sync(0xffffffffu, A.vx, src), __shfl_sync(0xffffffffu, A.vy, src),
+                  __shfl_sync(0xffffffffu, A.rr, src)};
+    const unsigned abs_ = __shfl_sync(0xffffffffu, ab, src);
+    if (lane < n) {
+        const float4 bv = a.rec[jj];
+        const uint2 bw = a.rec2[jj];
+        test_exact(a.tp, o, abs_, As, bw.y, Body{bv.x, bv.y, bv.z, bv.w, __uint_as_float(bw.x)});
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void queue_push(PairQueue& q, unsigned m, bool need, int j, const TileArgs& a, int o,
+                                           const Body& A, unsigned ab, int lane) {
+    if (need) {
+        const int at = q.cnt + __popc(m & ((1u << lane) - 1u));
+        q.j[at] = j;
+        q.l[at] = (unsigned char)lane;
+    }
+    q.cnt += __popc(m);
+    __syncwarp();
+    if (q.cnt >= 32) {
+        queue_flush(q, 32, a, o, A, ab, lane);
+        if (lane < q.cnt - 32) {
+            q.j[lane] = q.j[lane + 32];
+            q.l[lane] = q.l[lane + 32];
+        }
+        q.cnt -= 32;
+        __syncwarp();
+    }
+}
+
+// The tile's partners [j0, j0 + nj) against the lane's run body at sorted
+// position pa (valid = false: the lane has none). The keep rule on sorted
+// positions: within one key's range the stable sort keeps ascending body
+// order, so a < b is pa < j there. MODE 0: offset (0, 0), keep a < b;
+// MODE 1: another offset whose key differs from the run's own, all pairs
+// kept (the two ranges are disjoint); MODE 2: another offset whose cell
+// key equals the run's own (a hash collision), keep a != b. The line test
+// (see above) uses the tile's largest partner radius, which can only make
+// it skip less; it is written as c |c| > k dv^2 with c = |dp x dv| - E,
+// false for c <= 0.
+template <int MODE>
+__device__ __forceinline__ void tile_walk(const TileArgs& a, int o, const Body& A, unsigned ab, long long pa,
+                                          bool valid, long long j0, int nj, float E, float kl, bool skip_ok,
+                                          PairQueue& q, int lane) {
+    const float4* rp = a.rec + j0;
+    const long long rel = pa - j0;                     // the run body's position relative to j0
+    auto keep_of = [&](int k) { return MODE == 0 ? (long long)k > rel : (MODE == 1 ? true : (long long)k != rel); };
+    if (!skip_ok) {                                    // no skips in this tile: every kept pair is tested
+        for (int k = 0; k < nj; ++k) {
+            const bool need = valid && keep_of(k);
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            if (m) queue_push(q, m, need, (int)(j0 + k), a, o, A, ab, lane);
+        }
+        return;
+    }
+    int k = 0;
+    for (; k + 4 <= nj; k += 4) {
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = __ldg(rp + k + u);
+        bool need[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float dpx = v[u].x - A.x, dpy = v[u].y - A.y;
+            const float dvx = v[u].z - A.vx, dvy = v[u].w - A.vy;
+            const float c = fabsf(dpx * dvy - dpy * dvx) - E;
+            need[u] = valid && keep_of(k + u) && !(c * fabsf(c) > kl * (dvx * dvx + dvy * dvy));
+        }
+        const unsigned any = __ballot_sync(0xffffffffu, need[0] || need[1] || need[2] || need[3]);
+        if (any) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const unsigned m = __ballot_sync(0xffffffffu, need[u]);
+                if (m) queue_push(q, m, need[u], (int)(j0 + k + u), a, o, A, ab, lane);
+            }
+        }
+    }
+    for (; k < nj; ++k) {
+        const float4 v = __ldg(rp + k);
+        const float dpx = v.x - A.x, dpy = v.y - A.y;
+        const float dvx = v.z - A.vx, dvy = v.w - A.vy;
+        const float c = fabsf(dpx * dvy - dpy * dvx) - E;
+        const bool need = valid && keep_of(k) && !(c * fabsf(c) > kl * (dvx * dvx + dvy * dvy));
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) queue_push(q, m, need, (int)(j0 + k), a, o, A, ab, lane);
+    }
+}
+
+// A warp takes a contiguous range of tiles (one binary search per warp,
+// then forward). Per tile: lane l holds run body p0 + 32 i + l; the tile's
+// partner box and the run bodies' box give P and V; the warp streams the
+// partners — the same record for every lane, one broadcast load — through
+// the keep rule and the line test, and queues the pairs it cannot skip.
+__global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
+    __shared__ int q_j[BP_NT / 32][QCAP];
+    __shared__ unsigned char q_l[BP_NT / 32][QCAP];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    PairQueue q{q_j[wib], q_l[wib], 0};
     const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long c = warp0; c < chunks; c += warps) {
-        const long long base = c * BP_CHUNK;
-        const long long end = min(base + BP_CHUNK, a.total);
-        long long s0 = 0;
-        if (lane == 0) s0 = find_segment(a.seg_start, a.n_seg, base);
-        long long s = __shfl_sync(0xffffffffu, s0, 0);
-        long long cur = -1;
-        int o = 0;
-        unsigned ab = 0;
-        long long col0 = 0;
+    const long long per = (a.n_tiles + warps - 1) / warps;
+    const long long tb = warp0 * per, te = min(tb + per, a.n_tiles);
+    if (tb >= te) return;
+    const long long n_items = 5 * a.n_run;
+    long long t0 = 0;
+    if (lane == 0) t0 = find_segment(a.tile_start, n_items, tb);
+    long long t = __shfl_sync(0xffffffffu, t0, 0);
+    long long t_start = a.tile_start[t], t_end = a.tile_start[t + 1];
+    for (long long tid = tb; tid < te; ++tid) {
+        while (t_end <= tid) {
+            ++t;
+            t_start = t_end;
+            t_end = a.tile_start[t + 1];
+        }
+        const int o = (int)(t / a.n_run);
+        const long long qr = t - (long long)o * a.n_run;
+        const long long p0 = a.run_start[qr], p1 = qr + 1 < a.n_run ? a.run_start[qr + 1] : a.na;
+        const long long b0 = a.item_b0[t], nb = a.item_nb[t];
+        const long long n_bt = (nb + TILE_B - 1) / TILE_B;
+        const long long local = tid - t_start;
+        const long long ai = local / n_bt, bi = local - ai * n_bt;
+        const long long pa = p0 + ai * 32 + lane;
+        const bool valid = pa < p1;
         Body A{0.f, 0.f, 0.f, 0.f, 0.f};
-        for (long long idx = base + lane; idx < end; idx += 32) {
-            while (a.seg_start[s + 1] <= idx) ++s;
-            if (s != cur) {
-                cur = s;
-                o = (int)(s / na);
-                const long long r = s - (long long)o * na;
-                ab = a.ai[r];
-                A = Body{a.x[ab], a.y[ab], a.vx[ab], a.vy[ab], a.rr[ab]};
-                col0 = a.seg_lo[s] - a.seg_start[s];
-            }
-            const long long j = col0 + idx;
-            test_pair(a, o, ab, A, a.rec2[j], a.rec[j]);
+        unsigned ab = 0;
+        if (valid) {
+            const float4 v = a.rec[pa];
+            const uint2 w = a.rec2[pa];
+            A = Body{v.x, v.y, v.z, v.w, __uint_as_float(w.x)};
+            ab = w.y;
+        }
+        const long long jb = b0 + bi * TILE_B;
+        const int nj = (int)min((long long)TILE_B, b0 + nb - jb);
+        // boxes of the run bodies and of the partners -> P, V
+        float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+        float bu0 = INFINITY, bu1 = -INFINITY, bw0 = INFINITY, bw1 = -INFINITY, brr = 0.0f;
+        for (int k = lane; k < nj; k += 32) {
+            const float4 v = a.rec[jb + k];
+            bx0 = fminf(bx0, v.x); bx1 = fmaxf(bx1, v.x);
+            by0 = fminf(by0, v.y); by1 = fmaxf(by1, v.y);
+            bu0 = fminf(bu0, v.z); bu1 = fmaxf(bu1, v.z);
+            bw0 = fminf(bw0, v.w); bw1 = fmaxf(bw1, v.w);
+            const float r = __uint_as_float(a.rec2[jb + k].x);
+            brr = r > brr || r != r ? r : brr;        // a NaN radius poisons the tile's bound
+        }
+        const float ax0 = warp_min(valid ? A.x : INFINITY), ax1 = warp_max(valid ? A.x : -INFINITY);
+        const float ay0 = warp_min(valid ? A.y : INFINITY), ay1 = warp_max(valid ? A.y : -INFINITY);
+        const float au0 = warp_min(valid ? A.vx : INFINITY), au1 = warp_max(valid ? A.vx : -INFINITY);
+        const float aw0 = warp_min(valid ? A.vy : INFINITY), aw1 = warp_max(valid ? A.vy : -INFINITY);
+        bx0 = warp_min(bx0); bx1 = warp_max(bx1); by0 = warp_min(by0); by1 = warp_max(by1);
+        bu0 = warp_min(bu0); bu1 = warp_max(bu1); bw0 = warp_min(bw0); bw1 = warp_max(bw1);
+        for (int d = 16; d; d >>= 1) {
+            const float r = __shfl_xor_sync(0xffffffffu, brr, d);
+            brr = r > brr || r != r ? r : brr;
+        }
+        const float P = fmaxf(fmaxf(bx1 - ax0, ax1 - bx0), fmaxf(by1 - ay0, ay1 - by0)) * 1.0001f;
+        const float V = fmaxf(fmaxf(bu1 - au0, au1 - bu0), fmaxf(bw1 - aw0, aw1 - bw0)) * 1.0001f;
+        // a NaN radius or an unbounded box: no skips in the tile (warp-uniform;
+        // NaN coordinates need nothing here, as their line test never skips)
+        const bool skip_ok =
+            __all_sync(0xffffffffu, P < 0.5f && V * a.tp.dtf < 0.5f && brr == brr && (!valid || A.rr == A.rr));
+        const float E = 2.0f * EPS_CROSS * P * V;
+        const float rs = (A.rr + 1e-6f) + brr;
+        const float kl = 4.01f * rs * rs;
+        if (o == 0) {
+            tile_walk<0>(a, o, A, ab, pa, valid, jb, nj, E, kl, skip_ok, q, lane);
+        } else if (a.ks[b0] != a.ks[p0]) {
+            tile_walk<1>(a, o, A, ab, pa, valid, jb, nj, E, kl, skip_ok, q, lane);
+        } else {
+            tile_walk<2>(a, o, A, ab, pa, valid, jb, nj, E, kl, skip_ok, q, lane);
+        }
+        if (q.cnt > 0) {                               // the rest of the tile's queue
+            queue_flush(q, q.cnt, a, o, A, ab, lane);
+            q.cnt = 0;
         }
     }
 }
@@ -307,9 +523,10 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_k0 = take(nn), o_k1 = take(nn);
     const size_t o_v = take(nn);                  // v0 + v1 (unsigned, 2 per long long)
     const size_t o_ai = take((nn + 1) / 2 + 1);
-    const size_t o_seglo = take(5 * nn), o_segst = take(5 * nn + 1);
+    const size_t o_flag = take(nn), o_pos = take(nn), o_run = take(nn);
+    const size_t o_ib0 = take(5 * nn), o_inb = take(5 * nn), o_tst = take(5 * nn + 1);
     const size_t o_rec = take(2 * nn), o_rec2 = take(nn);      // float4 and uint2 per alive body
-    const size_t o_nh = take(1);
+    const size_t o_nh = take(2);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off * sizeof(long long), &scr);
     if (rc) return rc;
@@ -323,11 +540,16 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     unsigned* v0 = (unsigned*)(S + o_v);
     unsigned* v1 = v0 + nn;
     unsigned* ai = (unsigned*)(S + o_ai);
-    long long* seg_lo = S + o_seglo;
-    long long* seg_st = S + o_segst;
+    long long* flags = S + o_flag;
+    long long* pos = S + o_pos;
+    long long* run_start = S + o_run;
+    long long* item_b0 = S + o_ib0;
+    long long* item_nb = S + o_inb;
+    long long* tile_st = S + o_tst;
     float4* rec = (float4*)(S + o_rec);
     uint2* rec2 = (uint2*)(S + o_rec2);
     unsigned long long* d_nh = (unsigned long long*)(S + o_nh);
+    unsigned long long* d_ncand = d_nh + 1;
 
     // 1) alive compaction (ascending body order) + cells + keys
     k_alive_count<<<(unsigned)tiles, BP_NT, 0, s>>>(is_ast, vis, x, nn, lo, hi_halo, counts);
@@ -343,43 +565,57 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, na, scan_tmp, s));
     k_sorted_records<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, na, rec, rec2);
     SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
-    // 3) equal-key range of every (offset, body)
-    const long long nseg = 5 * na;
-    k_ranges<<<(unsigned)((nseg + 255) / 256), 256, 0, s>>>(cx, cy, na, k0, seg_lo, seg_st);
-    SSS_LAUNCH_CHECK(ctx, "k_ranges");
-    // 4) candidate offsets
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(seg_st, seg_st, nseg, scan_tmp, s));
-    const long long stiles = (nseg + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
-    long long total = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&total, scan_tmp + stiles, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(seg_st + nseg, scan_tmp + stiles, sizeof(long long), cudaMemcpyDeviceToDevice,
-                                      s));
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(d_nh, 0, sizeof(unsigned long long), s));
+    // 3) cell runs of the sorted order
+    const unsigned nb_a = (unsigned)((na + 255) / 256);
+    k_run_flags<<<nb_a, 256, 0, s>>>(cx, cy, v0, na, flags);
+    SSS_LAUNCH_CHECK(ctx, "k_run_flags");
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, na, scan_tmp, s));
+    k_run_starts<<<nb_a, 256, 0, s>>>(flags, pos, na, run_start);
+    SSS_LAUNCH_CHECK(ctx, "k_run_starts");
+    const long long atiles = (na + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    long long n_run = 0;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&n_run, scan_tmp + atiles, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(d_nh, 0, 2 * sizeof(unsigned long long), s));
     SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-    *n_cand = total;
-    if (total == 0) return SSS_OK;
-    // 5) fused candidate walk + tests
-    CandArgs ca;
-    ca.x = x; ca.y = y; ca.vx = vx; ca.vy = vy; ca.rr = rr;
-    ca.ai = ai;
-    ca.rec = rec;
-    ca.rec2 = rec2;
-    ca.seg_lo = seg_lo;
-    ca.seg_start = seg_st;
-    ca.n_seg = nseg;
-    ca.total = total;
-    ca.dtf = (float)dt_y;
-    ca.dt = dt_y;
-    ca.hi = hi;
-    ca.hits = (Hit*)out_hits;
-    ca.cap = capacity;
-    ca.n_hits = d_nh;
-    const long long chunks = (total + BP_CHUNK - 1) / BP_CHUNK;
-    long long blocks = (chunks + BP_NT / 32 - 1) / (BP_NT / 32);
+    // 4) (run, offset) items: partner ranges, tiles, candidates
+    const long long n_items = 5 * n_run;
+    k_items<<<(unsigned)((n_items + 255) / 256), 256, 0, s>>>(cx, cy, v0, k0, na, run_start, n_run, item_b0,
+                                                               item_nb, tile_st, d_ncand);
+    SSS_LAUNCH_CHECK(ctx, "k_items");
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(tile_st, tile_st, n_items, scan_tmp, s));
+    const long long itiles = (n_items + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    long long n_tiles = 0;
+    unsigned long long total = 0;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&n_tiles, scan_tmp + itiles, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tile_st + n_items, scan_tmp + itiles, sizeof(long long),
+                                      cudaMemcpyDeviceToDevice, s));
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&total, d_ncand, sizeof(total), cudaMemcpyDeviceToHost, s));
+    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    *n_cand = (int64_t)total;
+    if (n_tiles == 0) return SSS_OK;
+    // 5) tiles: keep rule + tests
+    TileArgs ta;
+    ta.rec = rec;
+    ta.rec2 = rec2;
+    ta.run_start = run_start;
+    ta.item_b0 = item_b0;
+    ta.item_nb = item_nb;
+    ta.tile_start = tile_st;
+    ta.ks = k0;
+    ta.na = na;
+    ta.n_run = n_run;
+    ta.n_tiles = n_tiles;
+    ta.tp.dtf = (float)dt_y;
+    ta.tp.dt = dt_y;
+    ta.tp.hi = hi;
+    ta.tp.hits = (Hit*)out_hits;
+    ta.tp.cap = capacity;
+    ta.tp.n_hits = d_nh;
+    long long blocks = (n_tiles + BP_NT / 32 - 1) / (BP_NT / 32);
     const long long max_blocks = (long long)ctx->num_sms * 32;
     if (blocks > max_blocks) blocks = max_blocks;
-    k_candidates<<<(unsigned)blocks, BP_NT, 0, s>>>(ca);
-    SSS_LAUNCH_CHECK(ctx, "k_candidates");
+    k_tiles<<<(unsigned)blocks, BP_NT, 0, s>>>(ta);
+    SSS_LAUNCH_CHECK(ctx, "k_tiles");
     unsigned long long nh = 0;
     SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&nh, d_nh, sizeof(nh), cudaMemcpyDeviceToHost, s));
     SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
