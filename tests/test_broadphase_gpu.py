@@ -124,3 +124,52 @@ def test_more_hits_than_the_first_buffer():
     res, cand = bp.bounce_hits(x, y, v, v, 0.001, 1e-3, 4e-3, rr=rr)
     ref, cref = obp.hits(x, y, v, v, rr, 0.001, 1e-3, 4e-3)
     assert cand == cref and _same(res, ref) and len(res[0]) > 4096
+
+
+def test_colliding_cell_keys():
+    """Cells (-34, 38) and (34, -38) have the same hash key at h = 0.01 AU,
+    so their bodies share one key range, interleaved in body order: runs of
+    a few bodies, tiles mixing two clusters 0.7 AU apart (where the line test
+    may not skip), a neighbour range that holds both, and many pairs through
+    the exact tests."""
+    bp = _bp()
+    A, B = np.int64(73856093), np.int64(19349663)
+    assert (np.int64(-34) * A) ^ (np.int64(38) * B) == (np.int64(34) * A) ^ (np.int64(-38) * B)
+    rng = np.random.default_rng(12)
+    n = 4000
+    h = 0.01
+    side = rng.integers(0, 2, n)                       # interleaved body indices
+    cx = np.where(side == 0, -34, 34) + 0.5
+    cy = np.where(side == 0, 38, -38) + 0.5
+    x = ((cx + rng.uniform(-0.45, 0.45, n)) * h).astype(np.float32)
+    y = ((cy + rng.uniform(-0.45, 0.45, n)) * h).astype(np.float32)
+    vx = rng.normal(0, 1e-2, n).astype(np.float32)
+    vy = rng.normal(0, 1e-2, n).astype(np.float32)
+    rr = np.full(n, 3e-5, np.float32)
+    dt = 0.05
+    halo = 2.0 * h + 2.0 * float(rr.max())
+    ref, cref = obp.hits(x, y, vx, vy, rr, dt, h, halo)
+    res, cand = bp.bounce_hits(x, y, vx, vy, dt, h, halo, rr=rr)
+    assert cand == cref and _same(res, ref)
+    assert ref is not None and len(ref[0]) > 0
+
+
+def test_non_finite_and_far_bodies():
+    """NaN positions and radii and bodies far from the origin: the line test
+    never skips what the exact tests would keep."""
+    bp = _bp()
+    x, y, vx, vy, rr = _scene(9, 20000, "clumps")
+    rng = np.random.default_rng(13)
+    bad = rng.choice(len(x), 40, replace=False)
+    x[bad[:10]] = np.nan
+    vy[bad[10:20]] = np.nan
+    rr[bad[20:30]] = np.nan
+    far = bad[30:]
+    x[far] = 3000.0 + rng.normal(0, 1e-3, len(far)).astype(np.float32)
+    dt = 0.5 / 365.25
+    v95 = float(np.nanpercentile(np.hypot(vx, vy), 95))
+    h = max(1e-4, 2.0 * v95 * dt)
+    halo = 2.0 * h + 2.0 * float(np.nanmax(rr))
+    ref, cref = obp.hits(x, y, vx, vy, rr, dt, h, halo)
+    res, cand = bp.bounce_hits(x, y, vx, vy, dt, h, halo, rr=rr)
+    assert cand == cref and _same(res, ref)
