@@ -198,7 +198,6 @@ __global__ void __launch_bounds__(SW_NT) k_run_write(long long n, const long lon
 // ------------------------------------------------------------- bounce
 
 constexpr int BF_NT = 256;
-constexpr int BF_CHUNK = 2048;
 
 __global__ void k_hit_keys(const int* __restrict__ hits, long long n_hits, unsigned long long* __restrict__ keys,
                            unsigned* __restrict__ vals) {
@@ -209,38 +208,98 @@ __global__ void k_hit_keys(const int* __restrict__ hits, long long n_hits, unsig
     vals[i] = (unsigned)i;
 }
 
-// Greedy one-hit-per-body filter over the sorted keys (one thread decides,
-// the block stages the keys); keep[i] = 1 for kept hits.
-__global__ void __launch_bounds__(BF_NT) k_bounce_filter(const unsigned long long* __restrict__ keys, long long n_hits,
-                                                         long long n_bodies, long long* __restrict__ keep) {
-    extern __shared__ unsigned used[];                  // n_bodies bits
-    __shared__ unsigned long long s_keys[BF_CHUNK];
-    __shared__ unsigned char s_keep[BF_CHUNK];
-    const long long words = (n_bodies + 31) / 32;
-    for (long long w = threadIdx.x; w < words; w += BF_NT) used[w] = 0u;
+// The one-hit-per-body rule (bounce_deltas: in (offset, a, b) order a hit
+// is kept when neither body is in a hit kept before it) is the
+// lexicographically first maximal matching of the hit graph, computed here
+// in rounds by one block: an undecided hit whose index is the smallest among
+// the undecided hits of both its bodies is kept; then every undecided hit
+// touching a body of a kept hit is dropped. Each kept hit is kept by the
+// sequential rule too (every earlier hit at its bodies was dropped, and a
+// hit is only ever dropped by a kept hit of smaller index, which keeps
+// before it), and each round keeps at least the smallest undecided hit.
+// After MATCH_ROUNDS rounds, whatever is still undecided is finished by the
+// sequential rule in order.
+constexpr int MATCH_NT = 1024;
+constexpr int MATCH_ROUNDS = 64;
+
+__device__ __forceinline__ void hit_bodies(unsigned long long key, unsigned& a, unsigned& b) {
+    a = (unsigned)((key >> 21) & 0x1FFFFFull);
+    b = (unsigned)(key & 0x1FFFFFull);
+}
+
+__global__ void __launch_bounds__(MATCH_NT) k_bounce_filter(const unsigned long long* __restrict__ keys,
+                                                            long long n_hits, int* __restrict__ min_hit,
+                                                            unsigned char* __restrict__ taken,
+                                                            unsigned char* __restrict__ state,
+                                                            long long* __restrict__ keep) {
+    __shared__ int s_left[MATCH_NT / 32];
+    for (long long i = threadIdx.x; i < n_hits; i += MATCH_NT) {
+        unsigned a, b;
+        hit_bodies(keys[i], a, b);
+        min_hit[a] = INT_MAX;
+        min_hit[b] = INT_MAX;
+        taken[a] = 0;
+        taken[b] = 0;
+        state[i] = 0;                                  // 0 undecided, 1 kept, 2 dropped
+    }
     __syncthreads();
-    for (long long c0 = 0; c0 < n_hits; c0 += BF_CHUNK) {
-        const int cnt = (int)min((long long)BF_CHUNK, n_hits - c0);
-        for (int i = threadIdx.x; i < cnt; i += BF_NT) s_keys[i] = keys[c0 + i];
+    int left = 1;
+    for (int round = 0; round < MATCH_ROUNDS && left > 0; ++round) {
+        for (long long i = threadIdx.x; i < n_hits; i += MATCH_NT) {
+            if (__ldcg(state + i)) continue;
+            unsigned a, b;
+            hit_bodies(keys[i], a, b);
+            atomicMin(min_hit + a, (int)i);
+            atomicMin(min_hit + b, (int)i);
+        }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int i = 0; i < cnt; ++i) {
-                const unsigned a = (unsigned)((s_keys[i] >> 21) & 0x1FFFFFull);
-                const unsigned b = (unsigned)(s_keys[i] & 0x1FFFFFull);
-                const bool ua = (used[a >> 5] >> (a & 31)) & 1u, ub = (used[b >> 5] >> (b & 31)) & 1u;
-                if (ua || ub) {
-                    s_keep[i] = 0;
-                } else {
-                    used[a >> 5] |= 1u << (a & 31);
-                    used[b >> 5] |= 1u << (b & 31);
-                    s_keep[i] = 1;
-                }
+        for (long long i = threadIdx.x; i < n_hits; i += MATCH_NT) {
+            if (__ldcg(state + i)) continue;
+            unsigned a, b;
+            hit_bodies(keys[i], a, b);
+            if (__ldcg(min_hit + a) == (int)i && __ldcg(min_hit + b) == (int)i) {
+                state[i] = 1;
+                taken[a] = 1;
+                taken[b] = 1;
             }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < cnt; i += BF_NT) keep[c0 + i] = s_keep[i];
+        int mine = 0;
+        for (long long i = threadIdx.x; i < n_hits; i += MATCH_NT) {
+            if (__ldcg(state + i)) continue;
+            unsigned a, b;
+            hit_bodies(keys[i], a, b);
+            if (__ldcg(taken + a) | __ldcg(taken + b)) {
+                state[i] = 2;
+            } else {
+                min_hit[a] = INT_MAX;
+                min_hit[b] = INT_MAX;
+                ++mine;
+            }
+        }
+        mine = __reduce_add_sync(0xffffffffu, mine);
+        if ((threadIdx.x & 31) == 0) s_left[threadIdx.x >> 5] = mine;
+        __syncthreads();
+        left = 0;
+        for (int w = 0; w < MATCH_NT / 32; ++w) left += s_left[w];
         __syncthreads();
     }
+    if (left > 0 && threadIdx.x == 0) {                // the sequential rule for the rest, in order
+        for (long long i = 0; i < n_hits; ++i) {
+            if (__ldcg(state + i)) continue;
+            unsigned a, b;
+            hit_bodies(keys[i], a, b);
+            if (__ldcg(taken + a) | __ldcg(taken + b)) {
+                state[i] = 2;
+            } else {
+                state[i] = 1;
+                taken[a] = 1;
+                taken[b] = 1;
+            }
+        }
+    }
+    __syncthreads();
+    for (long long i = threadIdx.x; i < n_hits; i += MATCH_NT) keep[i] = __ldcg(state + i) == 1;
 }
 
 struct BounceIn {
@@ -424,8 +483,7 @@ extern "C" int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const
     *n_act = 0;
     *n_touched = 0;
     if (n < 0 || n_hits < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
-    // body indices are packed in 21 bits of the sort key and the used-body bit
-    // set of the greedy filter lives in shared memory
+    // body indices are packed in 21 bits of the sort key
     if (n > SSS_COLLIDE_MAX_BODIES)
         return sss_set_err(ctx, SSS_ERR_ARG, "bounce: at most %d bodies", SSS_COLLIDE_MAX_BODIES);
     if (n_hits == 0 || n == 0) return SSS_OK;
@@ -447,6 +505,9 @@ extern "C" int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const
     const size_t o_tch = off; off += al((size_t)n * 8);
     const size_t o_tpos = off; off += al((size_t)n * 8);
     const size_t o_tscan = off; off += al(scan_scratch(n) * 8);
+    const size_t o_minh = off; off += al((size_t)n * 4);
+    const size_t o_taken = off; off += al((size_t)n);
+    const size_t o_state = off; off += al((size_t)n_hits);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off, &scr);
     if (rc) return rc;
@@ -466,10 +527,8 @@ extern "C" int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const
     k_hit_keys<<<nblk(n_hits, 256), 256, 0, st>>>(hits, n_hits, k0, v0);
     SSS_LAUNCH_CHECK(ctx, "k_hit_keys");
     SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n_hits, (long long*)(b + o_rs), st));
-    const size_t bits_bytes = (size_t)((n + 31) / 32) * 4;
-    SSS_CUDA_TRY(ctx, cudaFuncSetAttribute(k_bounce_filter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)std::max<size_t>(bits_bytes, 4)));
-    k_bounce_filter<<<1, BF_NT, std::max<size_t>(bits_bytes, 4), st>>>(k0, n_hits, n, keep);
+    k_bounce_filter<<<1, MATCH_NT, 0, st>>>(k0, n_hits, (int*)(b + o_minh), (unsigned char*)(b + o_taken),
+                                            (unsigned char*)(b + o_state), keep);
     SSS_LAUNCH_CHECK(ctx, "k_bounce_filter");
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(dd, 0, (size_t)n * 32, st));
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(tch, 0, (size_t)n * 8, st));

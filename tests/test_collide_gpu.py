@@ -157,3 +157,39 @@ def test_merges_match_oracle_and_reach_the_simulation():
     assert last
     for a, nx, ny, nvx, nvy, m, r in last.values():
         assert out[a] == nx and out[n + a] == ny and out[2 * n + a] == nvx and out[3 * n + a] == nvy
+
+
+def test_one_hit_rule_long_chains():
+    """The one-hit-per-body rule on a hit list with a 600-hit chain in index
+    order ((i, i+1): each round of the parallel filter settles one link, so
+    the sequential finish runs) and 3000 random hits among other bodies:
+    kept/active hits, touched bodies and deltas as the oracle's."""
+    from solarsystemsimulator_b200.collide import CollisionResponse
+    rng = np.random.default_rng(31)
+    n = 2000
+    x = np.arange(n) * 1e-5
+    y = rng.normal(0, 1e-7, n)
+    vx = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    vy = rng.normal(0, 0.1, n)
+    g = np.stack([x, y, vx, vy]).astype(np.float32)
+    rr = np.full(n, 6e-6)
+    mass = 10 ** rng.uniform(-14, -12, n)
+    ones = np.ones(n, np.uint8)
+    chain = {(i, i + 1) for i in range(600)}
+    extra = set()
+    while len(extra) < 3000:
+        a, b = sorted(rng.choice(np.arange(600, n), 2, replace=False).tolist())
+        extra.add((a, b))
+    pairs = sorted(chain | extra)
+    hits = np.array([(0, a, b) for a, b in pairs], np.int32)
+    cr = CollisionResponse(mass, rr, ones, ones, m_idx=np.zeros(0, np.int64))
+    res = cr.bounce_deltas(torch.as_tensor(g).cuda(), torch.as_tensor(hits).cuda(), len(hits), 0.5 / 365.25)
+    hi = np.array([a for a, b in pairs])
+    hj = np.array([b for a, b in pairs])
+    ref = oc.bounce_deltas(*g, rr, mass, hi, hj, 0.5 / 365.25)
+    assert res is not None and ref is not None
+    ghi, ghj, touched, d = (t.cpu().numpy() for t in res)
+    assert np.array_equal(ghi, ref[0]) and np.array_equal(ghj, ref[1])
+    assert np.array_equal(touched, ref[2])
+    assert np.allclose(d, ref[3], rtol=1e-12, atol=0.0, equal_nan=True)
+    assert len(ghi) > 300
