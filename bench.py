@@ -164,16 +164,21 @@ def run_reference(args, rank, world):
     rates = []
     cores = os.cpu_count() or 1
     desc = ""
-    for _ in range(max(1, args.warmup_cpu)):
-        pass
-    for _ in range(max(1, min(args.steps, 2))):
-        r, cores, desc = cpu_sample(w, seconds_target=args.cpu_seconds, threads=cores)
+    # W warm-up samples and K timed samples, each a bounded sample of the
+    # step (a strided target subset x all sources), sized so that the whole
+    # run stays within about three minutes
+    steps, warmup = max(1, args.steps), max(0, args.warmup)
+    per_sample = min(args.cpu_seconds, 180.0 / (steps + warmup))
+    for _ in range(warmup):
+        cpu_sample(w, seconds_target=per_sample, threads=cores)
+    for _ in range(steps):
+        r, cores, desc = cpu_sample(w, seconds_target=per_sample, threads=cores)
         rates.append(r)
     rate = statistics.median(rates)
     value = rate / 1e9
     sec_per_step = pairs_per_step(n_src, n_tgt) / rate
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": len(rates),
-            "warmup": 0, "ms_per_step": sec_per_step * 1e3, "higher_is_better": True,
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": warmup, "ms_per_step": sec_per_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference", "config": config_block(n_src, n_tgt),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
