@@ -111,24 +111,29 @@ struct Targets {
     long long n;
 };
 
-// the factor f(r) of one pair, a = -G m f d (see the file comment)
+// the factor f(r) of one pair, a = -G m f d (see the file comment). The
+// powers of r come from one reciprocal square root (CUDA's double rsqrt,
+// 1 ulp) instead of a square root and two divisions.
 __device__ __forceinline__ double ewald_pair(double r2, double alpha, double eps2, double rc2, double small2) {
     const double sp = 1.1283791670955126;   // 2 / sqrt(pi)
-    const double r = sqrt(r2);
-    const double inv_r3 = 1.0 / (r2 * r);
+    const double rinv = rsqrt(r2);
+    const double inv_r2 = rinv * rinv;
+    const double inv_r3 = inv_r2 * rinv;
+    const double r = r2 * rinv;
     if (r2 < small2) {
         const double x = alpha * r;
         const double s2 = r2 + eps2;
-        return (-erf(x) + sp * x * exp(-x * x)) * inv_r3 + 1.0 / (s2 * sqrt(s2));
+        const double si = rsqrt(s2);
+        return (-erf(x) + sp * x * exp(-x * x)) * inv_r3 + si * si * si;
     }
-    const double u = eps2 / r2;
+    const double u = eps2 * inv_r2;
     double soft;
     if (u < 1e-3) {
         // (1 + u)^{-3/2} - 1 = -3/2 u + 15/8 u^2 - 35/16 u^3 + 315/128 u^4 - ...
         soft = u * (-1.5 + u * (1.875 + u * (-2.1875 + u * 2.4609375)));
     } else {
-        const double s2 = r2 + eps2;
-        soft = (r2 * r) / (s2 * sqrt(s2)) - 1.0;
+        const double t = r * rsqrt(r2 + eps2);   // r / sqrt(r^2 + eps2)
+        soft = t * t * t - 1.0;
     }
     double f = soft * inv_r3;
     if (r2 < rc2) {

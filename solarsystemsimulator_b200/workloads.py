@@ -83,13 +83,15 @@ SEED_PERIODIC = 20260505
 
 
 def periodic_structure(n_side: int = 128, mesh_n: int = 256, sigma_mesh: float = 0.5, index: float = -2.0,
-                       softening: float = 1e-3, seed: int = SEED_PERIODIC):
-    """Particle-mesh workload: n_side^3 equal-mass particles (total mass 1,
-    G = 1) in the periodic unit box, a lattice displaced by Zel'dovich
-    displacements from P(k) ~ k^index normalised to rms density contrast
-    sigma_mesh on the particle lattice (the mesh scale of a mesh twice as
-    fine), wrapped into [0, 1); cold start. 128^3 = 1,048,576 particles on a
-    256^3 mesh is the full configuration.
+                       softening: float = 1e-3, seed: int = SEED_PERIODIC, fcc: bool = True):
+    """Particle-mesh workload: equal-mass particles (total mass 1, G = 1) in
+    the periodic unit box on a lattice displaced by Zel'dovich displacements
+    from P(k) ~ k^index normalised to rms density contrast sigma_mesh on the
+    n_side^3 lattice (the mesh scale of a mesh twice as fine), wrapped into
+    [0, 1); cold start. fcc keeps the lattice sites with i + j + k even (a
+    face-centred cubic sublattice, n_side^3 / 2 particles, displaced by the
+    same field): n_side = 128 gives the full configuration of 1,048,576
+    particles on a 256^3 mesh. fcc = False keeps all n_side^3 sites.
 
     Returns dict with pos (n,3), vel (n,3), mass (scalar per particle),
     mesh_n, softening."""
@@ -98,6 +100,9 @@ def periodic_structure(n_side: int = 128, mesh_n: int = 256, sigma_mesh: float =
     qx, qy, qz = np.meshgrid(g, g, g, indexing="ij")
     q = np.stack([qx.ravel(), qy.ravel(), qz.ravel()], 1)
     pos = q + np.stack([psi[c].ravel() for c in range(3)], 1)
+    if fcc:
+        i, j, k = np.meshgrid(*(np.arange(n_side),) * 3, indexing="ij")
+        pos = pos[((i + j + k) % 2 == 0).ravel()]
     pos -= np.floor(pos)
     n = len(pos)
     return {"pos": pos, "vel": np.zeros_like(pos), "mass": 1.0 / n, "mesh_n": mesh_n, "softening": softening}

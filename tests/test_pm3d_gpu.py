@@ -226,7 +226,7 @@ def test_training_reduces_the_loss(mods):
 def test_learned_run_gains_and_judge_reverts(mods):
     _lib, pm3d, mlp, _ = mods
     from solarsystemsimulator_b200.workloads import periodic_structure
-    w = periodic_structure(n_side=32, mesh_n=64, seed=21)
+    w = periodic_structure(n_side=32, mesh_n=64, seed=21, fcc=False)
     sim = pm3d.NBodyPMLearned(0, mesh_n=64, softening=w["softening"], check_every=10, samples=4096,
                               iters=400, batch=1024, lr=2e-3, seed=1)
     st = sim.load_state(w["pos"], w["vel"], w["mass"])
