@@ -390,6 +390,11 @@ int sss_ewald_accel(sss_ctx* ctx, const sss_pm3_particles* src, const double* co
                     const int64_t* self_idx, int64_t n_tgt, double G, double box, double alpha,
                     double r_cut, double eps2, const int* hvec, const double* coef, const double* sc,
                     int nk, double* const* out, void* stream);
+/* sss_ewald_gtab: the host-built table of g(x) = erfc(x) + 2 x exp(-x^2) / sqrt(pi)
+ * that the real-space sum evaluates (*n_int intervals of width *h over [0, n_int h],
+ * 6 Taylor coefficients about each interval's centre, lowest order first) into
+ * out (host, capacity cap doubles); host code only, no device call. */
+int sss_ewald_gtab(double* out, int64_t cap, int* n_int, double* h);
 
 /* ------------------------------------------- learned short-range correction
  *

@@ -139,6 +139,7 @@ SIGNATURES = {
     "sss_ewald_accel": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.POINTER(_dp), _dp, _c_i64,
                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, _dp, _dp, _dp, ctypes.c_int, ctypes.POINTER(_dp), _vp]),
+    "sss_ewald_gtab": (ctypes.c_int, [_dp, _c_i64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "sss_mlp_pack": (ctypes.c_int, [_vp, _dp, _dp, _vp]),
     "sss_mlp_features": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(Pm3Particles), _dp, _c_i64, ctypes.c_double,
                                         _dp, _vp]),

@@ -421,3 +421,11 @@ extern "C" int sss_ewald_accel(sss_ctx* ctx, const sss_pm3_particles* src, const
     SSS_LAUNCH_CHECK(ctx, "k_ewald_final");
     return SSS_OK;
 }
+
+extern "C" int sss_ewald_gtab(double* out, int64_t cap, int* n_int, double* h) {
+    if (!out || !n_int || !h || cap < (int64_t)G_NI * (G_DEG + 1)) return SSS_ERR_ARG;
+    build_gtab(out);
+    *n_int = G_NI;
+    *h = G_H;
+    return SSS_OK;
+}
