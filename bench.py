@@ -765,10 +765,15 @@ def measure_stream(dev, stream, samples=200):
             host[6 * m:8 * m].view(torch.int16).copy_(qy, non_blocking=True)
             kept[0] = m
 
+        def batch8():
+            sf.sample_batch([xd] * 8, [yd] * 8, [0.5] * 8, 0.5, box, log_zoom, LOD_MAX)
+
         for _ in range(3):
             one_e2e()
+            batch8()
         t = _ev_time(one, stream, samples)
         te = _ev_time(one_e2e, stream, samples)
+        tb = _ev_time(batch8, stream, max(1, samples // 8)) / 8
         m = kept[0]
         alg = n * (4 + 4 + 8 + 1 + 1) + m * 8           # sample, kill times, flags in; the kept payload out
         qxs, qys = ofr.display_coords(x, y, log_zoom)
@@ -777,6 +782,7 @@ def measure_stream(dev, stream, samples=200):
         ofr.sample_frame(x, y, kill_t > 0.0, a, inj, cpu_box, log_zoom, LOD_MAX)
         tc = time.perf_counter() - t0
         out[mode] = {"samples_per_s": 1.0 / t, "ms_per_sample": t * 1e3, "kept": int(m),
+                     "batch_of_8": {"samples_per_s": 1.0 / tb, "ms_per_sample": tb * 1e3},
                      "e2e": {"samples_per_s": 1.0 / te, "d2h_bytes_per_sample": 8 * m},
                      "algorithmic_bytes_per_sample": alg, "achieved_gbs": alg / t / 1e9,
                      "frac_of_measured_hbm": alg / t / 1e9 / peak,

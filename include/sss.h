@@ -316,6 +316,15 @@ int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const float* y, c
                       int64_t budget, unsigned* sel, uint16_t* qx, uint16_t* qy, int64_t* n_sel, void* stream);
 int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const float* y, int log_zoom, float* out4,
                       void* stream);
+/* sss_stream_sample_batch: k samples of the same bodies at once, as build_frame
+ * packs the samples of one frame (server.py:378-537): x[i], y[i] (host arrays of
+ * k device pointers) and t_cut[i] (host) per sample, the other inputs shared;
+ * sample i's output at sel/qx/qy + i n (capacity k n each), its count in
+ * n_sel[i] (host). One readback and one synchronisation for the batch. */
+int sss_stream_sample_batch(sss_ctx* ctx, int64_t n, int k, const float* const* x, const float* const* y,
+                            const double* kill_t, const double* t_cut, const unsigned char* is_ast,
+                            const unsigned char* injected, const double* box, int log_zoom, int64_t budget,
+                            unsigned* sel, uint16_t* qx, uint16_t* qy, int64_t* n_sel, void* stream);
 
 /* ------------------------------------------------ particle mesh, 3-D periodic
  *

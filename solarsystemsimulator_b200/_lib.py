@@ -124,6 +124,10 @@ SIGNATURES = {
     "sss_stream_sample": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, ctypes.c_double, _dp, _dp,
                                          ctypes.POINTER(ctypes.c_double), ctypes.c_int, _c_i64, _dp, _dp, _dp,
                                          ctypes.POINTER(_c_i64), _vp]),
+    "sss_stream_sample_batch": (ctypes.c_int, [_vp, _c_i64, ctypes.c_int, ctypes.POINTER(_dp), ctypes.POINTER(_dp),
+                                               _dp, ctypes.POINTER(ctypes.c_double), _dp, _dp,
+                                               ctypes.POINTER(ctypes.c_double), ctypes.c_int, _c_i64, _dp, _dp, _dp,
+                                               ctypes.POINTER(_c_i64), _vp]),
     "sss_stream_minmax": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), _vp]),
     "sss_pm3_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),
     "sss_pm3_destroy": (None, [_vp]),

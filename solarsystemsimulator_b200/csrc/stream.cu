@@ -580,7 +580,9 @@ struct Work {
     Ctl* ctl;
 };
 
-int make_work(sss_ctx* ctx, long long n, int grid, Work* W) {
+// scratch of a sample (reused by the samples of a batch, which run in
+// stream order) and n_ctl control blocks (one per sample of a batch)
+int make_work(sss_ctx* ctx, long long n, int grid, int n_ctl, Work* W) {
     size_t off = 0;
     const size_t o_qx = off; off += al((size_t)n * 4);
     const size_t o_qy = off; off += al((size_t)n * 4);
@@ -590,7 +592,7 @@ int make_work(sss_ctx* ctx, long long n, int grid, Work* W) {
     const size_t o_rate = off; off += al((size_t)K2 * 32);
     const size_t o_part = off; off += al((size_t)2 * CAND * GROUPS * 8);
     const size_t o_blk = off; off += al((size_t)grid * 8);
-    const size_t o_ctl = off; off += al(sizeof(Ctl));
+    const size_t o_ctl = off; off += al(sizeof(Ctl) * (size_t)n_ctl);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off, &scr);
     if (rc) return rc;
@@ -629,7 +631,7 @@ extern "C" int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const 
     if (n < 1 || !x || !y || !out4) return sss_set_err(ctx, SSS_ERR_ARG, "minmax: empty or NULL input");
     cudaStream_t st = (cudaStream_t)stream;
     Work W;
-    int rc = make_work(ctx, n, 1, &W);
+    int rc = make_work(ctx, n, 1, 1, &W);
     if (rc) return rc;
     const float* qx = x;
     const float* qy = y;
@@ -657,32 +659,35 @@ extern "C" int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const 
     return SSS_OK;
 }
 
-extern "C" int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const float* y, const double* kill_t,
-                                 double t_cut, const unsigned char* is_ast, const unsigned char* injected,
-                                 const double* box, int log_zoom, int64_t budget, unsigned* sel, uint16_t* qx_out,
-                                 uint16_t* qy_out, int64_t* n_sel, void* stream) {
+namespace {
+
+// k samples of the same bodies, one cooperative launch each in stream
+// order, one readback of the k counts at the end
+int sample_batch(sss_ctx* ctx, int64_t n, int k, const float* const* x, const float* const* y,
+                 const double* kill_t, const double* t_cut, const unsigned char* is_ast,
+                 const unsigned char* injected, const double* box, int log_zoom, int64_t budget, unsigned* sel,
+                 uint16_t* qx_out, uint16_t* qy_out, int64_t* n_sel, void* stream) {
     if (!ctx) return SSS_ERR_ARG;
-    if (!n_sel || !box) return sss_set_err(ctx, SSS_ERR_ARG, "NULL box or count");
-    *n_sel = 0;
+    if (!n_sel || !box || (k > 0 && (!x || !y || !t_cut))) return sss_set_err(ctx, SSS_ERR_ARG, "NULL host array");
+    if (k < 0 || k > 4096) return sss_set_err(ctx, SSS_ERR_ARG, "batch of 0..4096 samples");
+    for (int i = 0; i < k; ++i) n_sel[i] = 0;
     if (n < 0 || budget < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
-    if (n == 0) return SSS_OK;
+    if (n == 0 || k == 0) return SSS_OK;
     if (n > 0xFFFFFFFFLL) return sss_set_err(ctx, SSS_ERR_ARG, "more than 2^32 bodies (u32 indices)");
-    if (!x || !y || !kill_t || !is_ast || !sel || !qx_out || !qy_out)
-        return sss_set_err(ctx, SSS_ERR_ARG, "NULL array");
+    if (!kill_t || !is_ast || !sel || !qx_out || !qy_out) return sss_set_err(ctx, SSS_ERR_ARG, "NULL array");
+    for (int i = 0; i < k; ++i)
+        if (!x[i] || !y[i]) return sss_set_err(ctx, SSS_ERR_ARG, "NULL sample %d", i);
     cudaStream_t st = (cudaStream_t)stream;
     int grid = 0;
     int rc = sample_grid(ctx, &grid);
     if (rc) return rc;
     Work W;
-    rc = make_work(ctx, n, grid, &W);
+    rc = make_work(ctx, n, grid, k, &W);
     if (rc) return rc;
     SampleArgs a;
-    a.x = x;
-    a.y = y;
     a.kill_t = kill_t;
     a.is_ast = is_ast;
     a.injected = injected;
-    a.t_cut = t_cut;
     a.b.x0 = (float)box[0];
     a.b.y0 = (float)box[1];
     a.b.sx = (float)box[2];
@@ -700,17 +705,53 @@ extern "C" int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const 
     a.rate = W.rate;
     a.part = W.part;
     a.blockcnt = W.blockcnt;
-    a.sel = sel;
-    a.ox = qx_out;
-    a.oy = qy_out;
-    a.ctl = W.ctl;
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.ctl, 0, sizeof(Ctl), st));
-    void* params[] = {&a};
-    SSS_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void*)k_sample, dim3(grid), dim3(SAMPLE_THREADS), params, 0, st));
-    Ctl h;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&h, W.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    if (h.err) return sss_set_err(ctx, SSS_ERR_TIMEOUT, "k_sample: a grid barrier wait ran out");
-    *n_sel = h.total;
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.ctl, 0, sizeof(Ctl) * (size_t)k, st));
+    for (int i = 0; i < k; ++i) {
+        a.x = x[i];
+        a.y = y[i];
+        a.t_cut = t_cut[i];
+        a.sel = sel + (size_t)i * n;
+        a.ox = qx_out + (size_t)i * n;
+        a.oy = qy_out + (size_t)i * n;
+        a.ctl = W.ctl + i;
+        void* params[] = {&a};
+        SSS_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void*)k_sample, dim3(grid), dim3(SAMPLE_THREADS), params,
+                                                      0, st));
+    }
+    Ctl hbuf[16];
+    Ctl* h = k <= 16 ? hbuf : new Ctl[k];
+    cudaError_t e = cudaMemcpyAsync(h, W.ctl, sizeof(Ctl) * (size_t)k, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    int bad = -1;
+    if (e == cudaSuccess)
+        for (int i = 0; i < k; ++i) {
+            if (h[i].err && bad < 0) bad = i;
+            n_sel[i] = h[i].total;
+        }
+    if (h != hbuf) delete[] h;
+    if (e != cudaSuccess) return sss_cuda_err(ctx, e, "stream sample readback");
+    if (bad >= 0) {
+        for (int i = 0; i < k; ++i) n_sel[i] = 0;
+        return sss_set_err(ctx, SSS_ERR_TIMEOUT, "k_sample (sample %d): a grid barrier wait ran out", bad);
+    }
     return SSS_OK;
+}
+
+}  // namespace
+
+extern "C" int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const float* y, const double* kill_t,
+                                 double t_cut, const unsigned char* is_ast, const unsigned char* injected,
+                                 const double* box, int log_zoom, int64_t budget, unsigned* sel, uint16_t* qx_out,
+                                 uint16_t* qy_out, int64_t* n_sel, void* stream) {
+    return sample_batch(ctx, n, 1, &x, &y, kill_t, &t_cut, is_ast, injected, box, log_zoom, budget, sel, qx_out,
+                        qy_out, n_sel, stream);
+}
+
+extern "C" int sss_stream_sample_batch(sss_ctx* ctx, int64_t n, int k, const float* const* x, const float* const* y,
+                                       const double* kill_t, const double* t_cut, const unsigned char* is_ast,
+                                       const unsigned char* injected, const double* box, int log_zoom,
+                                       int64_t budget, unsigned* sel, uint16_t* qx_out, uint16_t* qy_out,
+                                       int64_t* n_sel, void* stream) {
+    return sample_batch(ctx, n, k, x, y, kill_t, t_cut, is_ast, injected, box, log_zoom, budget, sel, qx_out, qy_out,
+                        n_sel, stream);
 }

@@ -9,6 +9,7 @@ log1p on the device).
     box = sf.box(x_dev, y_dev, view, log_zoom)              # the session's box rule
     sel, qx, qy = sf.sample(x_dev, y_dev, t_i, raster_days, box, log_zoom, budget)
     sf.kill(idx, t)                                         # the event stream's kill times
+    frame = sf.sample_batch([x0, x1], [y0, y1], [t0, t1], raster_days, box, log_zoom, budget)
 
 The frame bytes around it (header, events, sub-sample chains, the unchanged
 index list flag) stay with the server's own packing code.
@@ -45,6 +46,7 @@ class StreamFrames:
         self.sel = torch.empty(self.n, dtype=torch.int32, device=self.dev)
         self.qx = torch.empty(self.n, dtype=torch.int16, device=self.dev)
         self.qy = torch.empty(self.n, dtype=torch.int16, device=self.dev)
+        self._bsel = self._bqx = self._bqy = None       # batch outputs, grown on demand
 
     def _s(self):
         return ctypes.c_void_p(_lib.stream_handle(self.device))
@@ -90,3 +92,39 @@ class StreamFrames:
                 self.ctx.check(self.ctx.lib.sss_stream_sample(*args, self._s()))
         m = cnt.value
         return self.sel[:m], self.qx[:m], self.qy[:m]
+
+    def sample_batch(self, xs, ys, t_is, raster_days: float, box, log_zoom: bool, budget: int):
+        """The samples of one frame at once (build_frame's list of ring
+        slots): xs, ys sequences of f32 device tensors, t_is their sample
+        times. A list of (sel u32, qx u16, qy u16) device views per sample,
+        valid until the next batch call."""
+        k = len(xs)
+        if len(ys) != k or len(t_is) != k:
+            raise ValueError("sample_batch: xs, ys and t_is must have the same length")
+        if k == 0:
+            return []
+        xs = [x.contiguous() for x in xs]
+        ys = [y.contiguous() for y in ys]
+        for v in xs + ys:
+            if v.numel() != self.n or v.dtype != torch.float32 or v.device != self.dev:
+                raise ValueError(f"sample_batch: samples must be f32 tensors of {self.n} bodies on {self.dev}")
+        if self._bsel is None or self._bsel.numel() < k * self.n:
+            self._bsel = torch.empty(k * self.n, dtype=torch.int32, device=self.dev)
+            self._bqx = torch.empty(k * self.n, dtype=torch.int16, device=self.dev)
+            self._bqy = torch.empty(k * self.n, dtype=torch.int16, device=self.dev)
+        px = (ctypes.c_void_p * k)(*(x.data_ptr() for x in xs))
+        py = (ctypes.c_void_p * k)(*(y.data_ptr() for y in ys))
+        tc = (ctypes.c_double * k)(*(float(t) - float(raster_days) for t in t_is))
+        b = (ctypes.c_double * 4)(*(float(v) for v in box))
+        cnt = (ctypes.c_int64 * k)()
+        args = (self.ctx.ptr, self.n, k, px, py, self.kill_t.data_ptr(), tc, self.d_ast.data_ptr(),
+                self.d_inj.data_ptr() if self.d_inj is not None else None, b, int(bool(log_zoom)), int(budget),
+                self._bsel.data_ptr(), self._bqx.data_ptr(), self._bqy.data_ptr(), cnt)
+        with torch.cuda.device(self.device):
+            self.ctx.check(self.ctx.lib.sss_stream_sample_batch(*args, self._s()))
+        out = []
+        for i in range(k):
+            o = i * self.n
+            m = cnt[i]
+            out.append((self._bsel[o:o + m], self._bqx[o:o + m], self._bqy[o:o + m]))
+        return out

@@ -132,3 +132,49 @@ def test_kill_times():
     assert len(sel) == len(x) and 7 in sel                  # t_cut 0.0 < 0.25
     sel = sf.sample(xd, yd, 1.0, 0.5, box, False, 10**6)[0].cpu().numpy()
     assert len(sel) == len(x) - 3 and not {7, 9, 11} & set(sel.tolist())
+
+
+@pytest.mark.parametrize("scene", SCENES)
+def test_batch_equals_single_samples(load_golden, scene):
+    """sample_batch (both samples of the golden frame in one call) gives the
+    golden frames and the single-sample results."""
+    from solarsystemsimulator_b200.stream import StreamFrames
+    g = load_golden(f"server_frame_{scene}.npz")
+    log_zoom = bool(g["log_zoom"])
+    sf = StreamFrames(g["is_ast"], g["injected"])
+    sf.kill_t = torch.as_tensor(g["kill_t"]).cuda()
+    box = tuple(float(v) for v in g["box"])
+    rd = float(g["raster_days"])
+    xs = [torch.as_tensor(g[f"x{k}"]).cuda() for k in range(2)]
+    ys = [torch.as_tensor(g[f"y{k}"]).cuda() for k in range(2)]
+    ts = [float(g["t0"]) + (k + 1) * rd for k in range(2)]
+    batch = [tuple(t.cpu().numpy() for t in r) for r in sf.sample_batch(xs, ys, ts, rd, box, log_zoom, int(g["budget"]))]
+    for k in range(2):
+        single = tuple(t.cpu().numpy() for t in sf.sample(xs[k], ys[k], ts[k], rd, box, log_zoom, int(g["budget"])))
+        for a, b in zip(batch[k], single):
+            assert np.array_equal(a, b)
+        if not log_zoom:
+            assert np.array_equal(batch[k][0].view(np.uint32), g[f"sel{k}"])
+            assert np.array_equal(batch[k][1].view(np.uint16), g[f"qx{k}"])
+
+
+def test_batch_of_twenty():
+    """A batch longer than the stack buffer of control blocks (20 samples of
+    110,000 bodies moving between samples, LOD active): every sample as its
+    single-sample call."""
+    from solarsystemsimulator_b200.stream import StreamFrames
+    x, y, a, inj, kill_t = _scene(20, 100_000, 10_000, seed=4)
+    sf = StreamFrames(a, inj)
+    sf.kill_t = torch.as_tensor(kill_t).cuda()
+    rng = np.random.default_rng(5)
+    xs, ys = [], []
+    for k in range(20):
+        xs.append(torch.as_tensor((x + rng.normal(0, 1e-3, len(x))).astype(np.float32)).cuda())
+        ys.append(torch.as_tensor((y + rng.normal(0, 1e-3, len(y))).astype(np.float32)).cuda())
+    ts = [0.1 * (k + 1) for k in range(20)]
+    box = sf.box(xs[0], ys[0], (0.0, 0.0, 2.0, 2.0), False)
+    batch = [tuple(t.cpu().numpy() for t in r) for r in sf.sample_batch(xs, ys, ts, 0.1, box, False, 20_000)]
+    for k in range(20):
+        single = [t.cpu().numpy() for t in sf.sample(xs[k], ys[k], ts[k], 0.1, box, False, 20_000)]
+        assert all(np.array_equal(p, q) for p, q in zip(batch[k], single))
+        assert 0 < len(single[0]) <= 25_000
