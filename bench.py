@@ -194,7 +194,7 @@ def run_reference(args, rank, world):
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
-    from solarsystemsimulator_b200 import _lib
+    from solarsystemsimulator_b200 import _lib, replicas
     from solarsystemsimulator_b200 import selfgrav_kernel as sg
 
     torch.cuda.set_device(local_rank)
@@ -241,11 +241,7 @@ def run_ours(args, rank, world, local_rank):
         return total
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device=f"cuda:{dev}")
 
     # ---- peaks measured in this run (the roofline denominators)
     peak = {}
