@@ -137,7 +137,13 @@ struct Ctl {                                        // zeroed before every launc
     unsigned long long tier_cnt[4];
     unsigned long long kept[2];
     long long total;
+    int value_over;                                 // more distinct cell counts than the value table holds
+    int fast_steps;                                 // halvings decided from the value histogram
+    double lohi[2];                                 // the bisection interval after them
 };
+
+constexpr int VALUE_SLOTS = 8192;                   // distinct nonzero cell counts (open addressing)
+constexpr int VALUE_MAX = 4096;                     // at most this many are sorted by one block
 
 struct SampleArgs {
     const float* x;
@@ -161,6 +167,9 @@ struct SampleArgs {
     unsigned short* ox;
     unsigned short* oy;
     Ctl* ctl;
+    int* vkey;                                      // VALUE_SLOTS: count value, -1 empty
+    unsigned* vmul;                                 // VALUE_SLOTS: cells holding it
+    double* vpre;                                   // 2 VALUE_MAX: prefix sums of the sorted values
 };
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -232,6 +241,7 @@ struct Smem {
     } u;
     double leaf[GROUP_LEAVES][32];
     double tot[32];
+    double dred[SAMPLE_WARPS];
     long long red[SAMPLE_WARPS];
     int wcnt[SAMPLE_WARPS];
     int bad;
@@ -331,7 +341,7 @@ __device__ void phase_group_sums(const SampleArgs& a, double lo, double hi, doub
 // shuffle levels pair lanes (l, l + d) for d = 1, 2, 4, 8, 16), then the
 // BISECT_D decisions, taken alike by every block
 static_assert(GROUPS == 4 * 32, "four group sums per lane");
-__device__ void phase_walk(const double* part, double budget, double& lo, double& hi, Smem& sm) {
+__device__ void phase_walk(const double* part, double budget, double& lo, double& hi, int levels, Smem& sm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int c = warp; c < CAND; c += SAMPLE_WARPS) {
         const double2 p0 = __ldcg((const double2*)(part + c * GROUPS + 4 * lane));
@@ -346,7 +356,7 @@ __device__ void phase_walk(const double* part, double budget, double& lo, double
     }
     __syncthreads();
     int node = 1;
-    for (int d = 0; d < BISECT_D; ++d) {
+    for (int d = 0; d < levels; ++d) {
         const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
         if (sm.tot[node - 1] > budget) {
             hi = s;
@@ -358,6 +368,233 @@ __device__ void phase_walk(const double* part, double budget, double& lo, double
     }
 }
 
+__device__ __forceinline__ long long block_excl_scan_ll(long long v, Smem& sm, long long* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    __syncthreads();
+    if (lane == 31) sm.red[warp] = inc;
+    __syncthreads();
+    long long before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < SAMPLE_WARPS; ++w) {
+        const long long x = sm.red[w];
+        before += w < warp ? x : 0;
+        all += x;
+    }
+    *total = all;
+    return before + inc - v;
+}
+
+__device__ __forceinline__ double block_excl_scan_d(double v, Smem& sm, double* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    __syncthreads();
+    if (lane == 31) sm.dred[warp] = inc;
+    __syncthreads();
+    double before = 0.0, all = 0.0;
+#pragma unroll
+    for (int w = 0; w < SAMPLE_WARPS; ++w) {
+        const double x = sm.dred[w];
+        if (w < warp) before += x;
+        all += x;
+    }
+    *total = all;
+    return before + (inc - v);
+}
+
+__device__ __forceinline__ void value_insert(const SampleArgs& a, int v, unsigned m) {
+    unsigned h = ((unsigned)v * 2654435761u) >> 19;                  // Fibonacci hash to 13 bits
+    for (int probe = 0; probe < VALUE_SLOTS; ++probe) {
+        const int prev = atomicCAS(a.vkey + h, -1, v);
+        if (prev == -1 || prev == v) {
+            atomicAdd(a.vmul + h, m);
+            return;
+        }
+        h = (h + 1) & (VALUE_SLOTS - 1);
+    }
+    atomicExch(&a.ctl->value_over, 1);
+}
+static_assert(VALUE_SLOTS == 1 << 13, "13-bit hash");
+
+// The histogram of the nonzero cell counts (how many cells hold each count):
+// each block takes a contiguous range of cells, merges its values in a
+// shared-memory table and adds them to the global table. A global table that
+// runs out of slots sets value_over (the bisection then takes the exact path).
+__device__ void phase_values(const SampleArgs& a, Smem& sm) {
+    for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS) {
+        sm.u.h.key[j] = -1;
+        sm.u.h.val[j] = 0;
+    }
+    __syncthreads();
+    const long long per = (K2 + gridDim.x - 1) / gridDim.x;
+    const long long c0 = (long long)blockIdx.x * per, c1 = min(c0 + per, (long long)K2);
+    for (long long c = c0 + threadIdx.x; c < c1; c += SAMPLE_THREADS) {
+        const int v = __ldcg(a.counts + c);
+        if (v <= 0) continue;
+        unsigned h = ((unsigned)v * 2654435761u) >> 20;              // 12 bits
+        bool done = false;
+        for (int probe = 0; probe < HIST_SLOTS; ++probe) {
+            const int prev = atomicCAS(sm.u.h.key + h, -1, v);
+            if (prev == -1 || prev == v) {
+                atomicAdd(sm.u.h.val + h, 1);
+                done = true;
+                break;
+            }
+            h = (h + 1) & (HIST_SLOTS - 1);
+        }
+        if (!done) value_insert(a, v, 1u);                           // a full block table: straight to the global one
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS)
+        if (sm.u.h.key[j] >= 0) value_insert(a, sm.u.h.key[j], (unsigned)sm.u.h.val[j]);
+    __syncthreads();
+}
+
+// The bisection from the count histogram (block 0). With the D distinct
+// counts v_i sorted ascending, n_i the cells holding each, w_i = v_i ** 0.5
+// and s the midpoint, the reference's sum over the cells of min(v, s w) is,
+// up to rounding, F(s) = A_k + s (W - W_k), k the number of values with
+// v_i <= s^2, A_k = sum_{i<k} n_i v_i (exact: integers below 2^53), W_k =
+// sum_{i<k} n_i w_i, W = W_D. A halving is taken only where the decision
+// F(s) > budget is certain: the reference's pairwise f64 sum differs from
+// the exact sum of its terms by less than 30 ulp of it (leaves of 128 with
+// 8 partial sums: 16 + 3 additions, 11 pairwise levels), the terms differ
+// from those of F by less than 2 ulp of max(v, s w) (the classification
+// at v = s^2 included), and the prefix sums here err by less than 30 ulp of
+// W; so |f(s) - F(s)| < 1e-13 (F + s W + budget) with a wide margin. At the
+// first step inside that margin the walk stops; the exact rounds finish it.
+__device__ void block_fast_bisection(const SampleArgs& a, double budget, Smem& sm) {
+    int* sv = sm.u.h.key;                                            // sorted values (VALUE_MAX)
+    int* sn = sm.u.h.val;                                            // their cell counts
+    static_assert(HIST_SLOTS >= VALUE_MAX, "sort space");
+    constexpr int PER = VALUE_SLOTS / SAMPLE_THREADS;
+    int cnt = 0;
+    for (int q = 0; q < PER; ++q) cnt += __ldcg(a.vkey + threadIdx.x * PER + q) >= 0;
+    long long total = 0;
+    const long long off = block_excl_scan_ll(cnt, sm, &total);
+    if (__ldcg(&a.ctl->value_over) != 0 || total > VALUE_MAX || total < 1) {
+        if (threadIdx.x == 0) {
+            a.ctl->lohi[0] = 0.0;
+            a.ctl->lohi[1] = budget;
+            a.ctl->fast_steps = 0;
+        }
+        return;
+    }
+    const int D = (int)total;
+    int Dp = 1;
+    while (Dp < D) Dp <<= 1;
+    int w = (int)off;
+    for (int q = 0; q < PER; ++q) {
+        const int slot = threadIdx.x * PER + q;
+        const int v = __ldcg(a.vkey + slot);
+        if (v >= 0) {
+            sv[w] = v;
+            sn[w] = (int)__ldcg(a.vmul + slot);
+            ++w;
+        }
+    }
+    for (int i = D + threadIdx.x; i < Dp; i += SAMPLE_THREADS) {
+        sv[i] = INT_MAX;
+        sn[i] = 0;
+    }
+    __syncthreads();
+    // bitonic sort of (value, cells) by value, ascending (the values are distinct)
+    for (int size = 2; size <= Dp; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < Dp / 2; i += SAMPLE_THREADS) {
+                const int l = 2 * i - (i & (stride - 1)), r = l + stride;
+                const bool up = (l & size) == 0;
+                if ((sv[l] > sv[r]) == up) {
+                    const int tv = sv[l], tn = sn[l];
+                    sv[l] = sv[r];
+                    sn[l] = sn[r];
+                    sv[r] = tv;
+                    sn[r] = tn;
+                }
+            }
+            __syncthreads();
+        }
+    // prefix sums over chunks of consecutive values, then across the chunks
+    const int ch = (D + SAMPLE_THREADS - 1) / SAMPLE_THREADS;
+    const int i0 = threadIdx.x * ch, i1 = min(i0 + ch, D);
+    double la = 0.0, lw = 0.0;
+    for (int i = i0; i < i1; ++i) {
+        la += (double)sn[i] * (double)sv[i];
+        lw += (double)sn[i] * cell_weight(sv[i]);
+    }
+    double tot_a = 0.0, tot_w = 0.0;
+    double ea = block_excl_scan_d(la, sm, &tot_a);
+    double ew = block_excl_scan_d(lw, sm, &tot_w);
+    for (int i = i0; i < i1; ++i) {
+        a.vpre[2 * i] = ea;
+        a.vpre[2 * i + 1] = ew;
+        ea += (double)sn[i] * (double)sv[i];
+        ew += (double)sn[i] * cell_weight(sv[i]);
+    }
+    if (threadIdx.x == 0) {
+        a.vpre[2 * D] = tot_a;
+        a.vpre[2 * D + 1] = tot_w;
+    }
+    __syncthreads();
+    // warp 0: BISECT_D halvings per round, lane c evaluating the midpoint of
+    // node c + 1 of the halving tree below (lo, hi) (node_mid: the same
+    // arithmetic as the sequential halving), the decisions read off the
+    // path by shuffles; the walk stops at the first uncertain node
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const double W = tot_w;
+        double lo = 0.0, hi = budget;
+        int steps = 0;
+        bool stop = false;
+        while (steps < 40 && !stop) {
+            double F = 0.0, margin = 0.0;
+            if (lane < CAND) {
+                const double s = node_mid(lane + 1, lo, hi);
+                const double s2 = s * s;
+                int l = 0, r = D;                                    // k = #values <= s^2
+                while (l < r) {
+                    const int m = (l + r) >> 1;
+                    if ((double)sv[m] <= s2) l = m + 1;
+                    else r = m;
+                }
+                F = a.vpre[2 * l] + s * (W - a.vpre[2 * l + 1]);
+                margin = 1e-13 * (F + s * W + budget);
+            }
+            const int levels = min(BISECT_D, 40 - steps);
+            int node = 1;
+            for (int d = 0; d < levels; ++d) {
+                const double Fn = __shfl_sync(0xffffffffu, F, node - 1);
+                const double Mn = __shfl_sync(0xffffffffu, margin, node - 1);
+                const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
+                if (Fn > budget + Mn) {
+                    hi = s;
+                    node = 2 * node;
+                } else if (Fn < budget - Mn) {
+                    lo = s;
+                    node = 2 * node + 1;
+                } else {
+                    stop = true;
+                    break;
+                }
+                ++steps;
+            }
+        }
+        if (lane == 0) {
+            a.ctl->lohi[0] = lo;
+            a.ctl->lohi[1] = hi;
+            a.ctl->fast_steps = steps;
+        }
+    }
+}
+
 // The reference's _dichte_filter over the tiers in mask with `budget`
 // points (size > budget); keep[i] = 1 for the kept bodies, their number in
 // ctl->kept[slot]. Returns false when a barrier gave up.
@@ -365,12 +602,20 @@ __device__ bool filter(const SampleArgs& a, const float* qx, const float* qy, in
                        unsigned& epoch, Smem& sm) {
     phase_hist(a, qx, qy, mask, sm);
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
-    double lo = 0.0, hi = (double)budget;
-    for (int round = 0; round < 40 / BISECT_D; ++round) {
+    phase_values(a, sm);
+    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
+    if (blockIdx.x == 0) block_fast_bisection(a, (double)budget, sm);
+    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
+    double lo = __ldcg(&a.ctl->lohi[0]), hi = __ldcg(&a.ctl->lohi[1]);
+    // the halvings the histogram could not decide (normally none): exact rounds
+    int left = 40 - __ldcg(&a.ctl->fast_steps);
+    for (int round = 0; left > 0; ++round) {
         double* part = a.part + (round & 1) * CAND * GROUPS;
         phase_group_sums(a, lo, hi, part, sm);
         if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
-        phase_walk(part, (double)budget, lo, hi, sm);
+        const int levels = min(BISECT_D, left);
+        phase_walk(part, (double)budget, lo, hi, levels, sm);
+        left -= levels;
     }
     const long long T = (long long)gridDim.x * SAMPLE_THREADS;
     const long long gt = (long long)blockIdx.x * SAMPLE_THREADS + threadIdx.x;
@@ -427,6 +672,11 @@ __device__ bool filter(const SampleArgs& a, const float* qx, const float* qy, in
     // the cell counts are dead now (the rates hold what the keep decisions
     // need): clear them for a following filter
     for (long long c = gt; c < K2; c += T) a.counts[c] = 0;
+    for (long long c = gt; c < VALUE_SLOTS; c += T) {
+        a.vkey[c] = -1;
+        a.vmul[c] = 0;
+    }
+    if (gt == 0) a.ctl->value_over = 0;
     kept = block_sum_ll(kept, sm.red);
     if (threadIdx.x == 0 && kept) atomicAdd(a.ctl->kept + slot, (unsigned long long)kept);
     return grid_barrier(a.ctl, epoch, &sm.bad);
@@ -442,6 +692,11 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     // ---- cull
     long long n1 = 0, n2 = 0, n3 = 0;
     for (long long c = gt; c < K2; c += T) a.counts[c] = 0;
+    for (long long c = gt; c < VALUE_SLOTS; c += T) {
+        a.vkey[c] = -1;
+        a.vmul[c] = 0;
+    }
+    if (gt == 0) a.ctl->value_over = 0;
     for (long long i = gt; i < a.n; i += T) {
         float px = a.x[i], py = a.y[i];
         const double kt = a.kill_t[i];
@@ -576,6 +831,9 @@ struct Work {
     unsigned char *tier, *keep;
     int* counts;
     double *rate, *part;
+    int* vkey;
+    unsigned* vmul;
+    double* vpre;
     long long* blockcnt;
     Ctl* ctl;
 };
@@ -591,6 +849,9 @@ int make_work(sss_ctx* ctx, long long n, int grid, int n_ctl, Work* W) {
     const size_t o_cnts = off; off += al((size_t)K2 * 4);
     const size_t o_rate = off; off += al((size_t)K2 * 32);
     const size_t o_part = off; off += al((size_t)2 * CAND * GROUPS * 8);
+    const size_t o_vkey = off; off += al((size_t)VALUE_SLOTS * 4);
+    const size_t o_vmul = off; off += al((size_t)VALUE_SLOTS * 4);
+    const size_t o_vpre = off; off += al((size_t)2 * (VALUE_MAX + 1) * 8);
     const size_t o_blk = off; off += al((size_t)grid * 8);
     const size_t o_ctl = off; off += al(sizeof(Ctl) * (size_t)n_ctl);
     void* scr = nullptr;
@@ -604,6 +865,9 @@ int make_work(sss_ctx* ctx, long long n, int grid, int n_ctl, Work* W) {
     W->counts = (int*)(p + o_cnts);
     W->rate = (double*)(p + o_rate);
     W->part = (double*)(p + o_part);
+    W->vkey = (int*)(p + o_vkey);
+    W->vmul = (unsigned*)(p + o_vmul);
+    W->vpre = (double*)(p + o_vpre);
     W->blockcnt = (long long*)(p + o_blk);
     W->ctl = (Ctl*)(p + o_ctl);
     return SSS_OK;
@@ -705,6 +969,9 @@ int sample_batch(sss_ctx* ctx, int64_t n, int k, const float* const* x, const fl
     a.rate = W.rate;
     a.part = W.part;
     a.blockcnt = W.blockcnt;
+    a.vkey = W.vkey;
+    a.vmul = W.vmul;
+    a.vpre = W.vpre;
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(W.ctl, 0, sizeof(Ctl) * (size_t)k, st));
     for (int i = 0; i < k; ++i) {
         a.x = x[i];
