@@ -178,3 +178,31 @@ def test_batch_of_twenty():
         single = [t.cpu().numpy() for t in sf.sample(xs[k], ys[k], ts[k], 0.1, box, False, 20_000)]
         assert all(np.array_equal(p, q) for p, q in zip(batch[k], single))
         assert 0 < len(single[0]) <= 25_000
+
+
+def test_many_distinct_cell_counts_take_the_exact_rounds():
+    """4,200 distinct cell counts (cell i of the box holds i + 1 bodies,
+    8,822,100 asteroids): more than the count histogram holds, so the
+    bisection runs entirely in the exact pairwise rounds; bit-exact against
+    the oracle."""
+    from oracle import frames as ofr
+    from solarsystemsimulator_b200.stream import StreamFrames
+    k, cells = 512, 4200
+    reps = np.arange(1, cells + 1)
+    cid = np.repeat(np.arange(cells), reps)
+    rng = np.random.default_rng(17)
+    x = ((cid % k + 0.5 + rng.uniform(-0.3, 0.3, len(cid))) / k).astype(np.float32)
+    y = ((cid // k + 0.5 + rng.uniform(-0.3, 0.3, len(cid))) / k).astype(np.float32)
+    n = len(x)
+    a = np.ones(n, bool)
+    inj = np.zeros(n, bool)
+    view = (0.5, 0.5, 0.25, 0.25)                     # box (0, 0, 1, 1): one LOD cell per grid cell
+    box = ofr.make_box(x, y, view)
+    sf = StreamFrames(a, inj)
+    xd, yd = torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda()
+    assert sf.box(xd, yd, view, False) == box
+    sel, qx, qy = (t.cpu().numpy() for t in sf.sample(xd, yd, 0.5, 0.5, box, False, 120_000))
+    rs, rx, ry = ofr.sample_frame(x, y, np.ones(n, bool), a, inj, box, False, 120_000)
+    assert np.array_equal(sel.view(np.uint32), rs)
+    assert np.array_equal(qx.view(np.uint16), rx) and np.array_equal(qy.view(np.uint16), ry)
+    assert 100_000 < len(rs) < 140_000
