@@ -16,11 +16,13 @@
 //   operations, so no fused multiply-add may appear), radii + 1e-6;
 // * ownership: min(x_a, x_b) < hi (f32); exact recheck in f64 of the f32
 //   values, again without contraction.
-// The candidate list is never materialised: the sorted bodies are split
-// into runs of one cell; a run and a neighbour offset give a block of
-// candidates (the run's bodies x the bodies with the offset cell's key), cut
-// into tiles of 32 x 256 that warps take one by one, a run body per lane and
-// the partners streamed as broadcast loads from records stored in sorted-key
+// The candidate list is never materialised: the bodies are sorted by cell
+// key and, inside a cell, by sub-cell, and split into runs of one cell; a run
+// and a neighbour offset give a block of candidates (the run's bodies x the
+// bodies with the offset cell's key), counted exactly and cut into tiles of
+// 32 run bodies x up to 992 partners. A warp skips each aligned chunk of 32
+// partners whose bounding box is provably out of reach of the run bodies' box
+// and streams the others as broadcast loads from records stored in sorted
 // order. Hits are appended; the host sorts them by (offset, a, b), which is
 // the reference's output order.
 
@@ -195,6 +197,81 @@ __device__ __forceinline__ void test_exact(const TestParams& a, int o, unsigned 
     if ((long long)slot < a.cap) a.hits[slot] = Hit{o, ab, bb};
 }
 
+// Position inside the cell: a 12-bit Morton code of the 64 x 64 sub-cell,
+// the secondary sort key, so that consecutive bodies of a run (and of a
+// partner range) lie close together and their bounding boxes are small.
+__device__ __forceinline__ unsigned spread2(unsigned v) {
+    v &= 0x3Fu;
+    v = (v | (v << 4)) & 0x0F0Fu;
+    v = (v | (v << 2)) & 0x3333u;
+    v = (v | (v << 1)) & 0x5555u;
+    return v;
+}
+
+__global__ void k_sub_keys(const float* __restrict__ x, const float* __restrict__ y, const unsigned* __restrict__ ai,
+                           const long long* __restrict__ cx, const long long* __restrict__ cy, long long na,
+                           double h, unsigned long long* __restrict__ sk, unsigned* __restrict__ sv) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= na) return;
+    const unsigned b = ai[r];
+    const double fx = __ddiv_rn((double)x[b], h) - (double)cx[r];
+    const double fy = __ddiv_rn((double)y[b], h) - (double)cy[r];
+    const int ix = fx >= 0.0 ? min((int)(fx * 64.0), 63) : 0;      // NaN and below: sub-cell 0
+    const int iy = fy >= 0.0 ? min((int)(fy * 64.0), 63) : 0;
+    sk[r] = spread2((unsigned)ix) | (spread2((unsigned)iy) << 1);
+    sv[r] = (unsigned)r;
+}
+
+__global__ void k_gather_keys(const unsigned long long* __restrict__ rowkey, const unsigned* __restrict__ order,
+                              long long na, unsigned long long* __restrict__ keys) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < na) keys[p] = rowkey[order[p]];
+}
+
+// Bounding box of every aligned chunk of 32 sorted records: x, y, vx, vy
+// ranges and the largest radius (NaN when a radius is NaN).
+struct ChunkBox {
+    float4 pos;   // xmin, xmax, ymin, ymax
+    float4 vel;   // vxmin, vxmax, vymin, vymax
+    float4 rad;   // rrmax, -, -, -
+};
+
+__device__ __forceinline__ float nan_max(float a, float b) { return (b > a || b != b) ? b : a; }
+
+__global__ void k_chunk_boxes(const float4* __restrict__ rec, const uint2* __restrict__ rec2, long long na,
+                              ChunkBox* __restrict__ boxes) {
+    const int lane = threadIdx.x & 31;
+    const long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nc = (na + 31) / 32;
+    if (c >= nc) return;
+    const long long j = c * 32 + lane;
+    float4 v = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+    float4 w = make_float4(-INFINITY, -INFINITY, -INFINITY, -INFINITY);
+    float r = 0.0f;
+    if (j < na) {
+        const float4 q = rec[j];
+        v = q;
+        w = q;
+        r = __uint_as_float(rec2[j].x);
+    }
+    for (int d = 16; d; d >>= 1) {
+        v.x = fminf(v.x, __shfl_xor_sync(0xffffffffu, v.x, d));
+        v.y = fminf(v.y, __shfl_xor_sync(0xffffffffu, v.y, d));
+        v.z = fminf(v.z, __shfl_xor_sync(0xffffffffu, v.z, d));
+        v.w = fminf(v.w, __shfl_xor_sync(0xffffffffu, v.w, d));
+        w.x = fmaxf(w.x, __shfl_xor_sync(0xffffffffu, w.x, d));
+        w.y = fmaxf(w.y, __shfl_xor_sync(0xffffffffu, w.y, d));
+        w.z = fmaxf(w.z, __shfl_xor_sync(0xffffffffu, w.z, d));
+        w.w = fmaxf(w.w, __shfl_xor_sync(0xffffffffu, w.w, d));
+        r = nan_max(r, __shfl_xor_sync(0xffffffffu, r, d));
+    }
+    if (lane == 0) {
+        boxes[c].pos = make_float4(v.x, w.x, v.y, w.y);
+        boxes[c].vel = make_float4(v.z, w.z, v.w, w.w);
+        boxes[c].rad = make_float4(r, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 // Cell runs: consecutive sorted positions whose bodies lie in the same cell
 // (the bodies of two cells with colliding keys interleave in the stable key
 // order; each stretch of one cell is its own run). All bodies of a run have,
@@ -221,7 +298,7 @@ __global__ void k_run_starts(const long long* __restrict__ flags, const long lon
     if (p < na && flags[p]) run_start[pos[p]] = p;
 }
 
-constexpr int TILE_B = 256;       // partners per tile; a tile is 32 run bodies (one per lane) x TILE_B partners
+constexpr int TILE_B = 992;       // partners per tile (at most 32 aligned chunks of 32); 32 run bodies per tile
 
 // Item t = o * n_run + q: run q against the partner range of offset o (its
 // first position and length), its tile count, and the candidates summed per
@@ -267,6 +344,7 @@ struct TileArgs {
     const long long* item_nb;    // [5 n_run]
     const long long* tile_start; // [5 n_run + 1] exclusive prefix of the tile counts
     const unsigned long long* ks; // sorted keys
+    const ChunkBox* boxes;       // [ceil(na / 32)] boxes of the aligned chunks of 32 records
     long long na, n_run, n_tiles;
     TestParams tp;
 };
@@ -343,24 +421,27 @@ __device__ __forceinline__ void queue_push(PairQueue& q, unsigned m, bool need, 
     }
 }
 
-// The tile's partners [j0, j0 + nj) against the lane's run body at sorted
-// position pa (valid = false: the lane has none). The keep rule on sorted
-// positions: within one key's range the stable sort keeps ascending body
-// order, so a < b is pa < j there. MODE 0: offset (0, 0), keep a < b;
-// MODE 1: another offset whose key differs from the run's own, all pairs
-// kept (the two ranges are disjoint); MODE 2: another offset whose cell
-// key equals the run's own (a hash collision), keep a != b. The line test
-// (see above) uses the tile's largest partner radius, which can only make
-// it skip less; it is written as c |c| > k dv^2 with c = |dp x dv| - E,
-// false for c <= 0.
+// The partners [j0, j0 + nj) of one surviving chunk against the lane's run
+// body (valid = false: the lane has none). Keep rule on body indices:
+// MODE 0: offset (0, 0), keep a < b; MODE 1: another offset whose key
+// differs from the run's own, all pairs kept (the two ranges are disjoint);
+// MODE 2: another offset whose cell key equals the run's own (a hash
+// collision), keep a != b. The line test (see above) uses the chunk's
+// largest radius (kl = 4.01 (rr_a + 1e-6 + rr_max)^2), which can only make it
+// skip less; it is written as c |c| > kl dv^2 with c = |dp x dv| - E, false
+// for c <= 0.
 template <int MODE>
-__device__ __forceinline__ void tile_walk(const TileArgs& a, int o, const Body& A, unsigned ab, long long pa,
-                                          bool valid, long long j0, int nj, float E, float kl, bool skip_ok,
-                                          PairQueue& q, int lane) {
+__device__ __forceinline__ void span_walk(const TileArgs& a, int o, const Body& A, unsigned ab, bool valid,
+                                          long long j0, int nj, float E, float kl, bool skip_ok, PairQueue& q,
+                                          int lane) {
     const float4* rp = a.rec + j0;
-    const long long rel = pa - j0;                     // the run body's position relative to j0
-    auto keep_of = [&](int k) { return MODE == 0 ? (long long)k > rel : (MODE == 1 ? true : (long long)k != rel); };
-    if (!skip_ok) {                                    // no skips in this tile: every kept pair is tested
+    const uint2* rp2 = a.rec2 + j0;
+    auto keep_of = [&](int k) {
+        if (MODE == 1) return true;
+        const unsigned bb = __ldg(&rp2[k].y);
+        return MODE == 0 ? ab < bb : ab != bb;
+    };
+    if (!skip_ok) {                                    // no skips in this chunk: every kept pair is tested
         for (int k = 0; k < nj; ++k) {
             const bool need = valid && keep_of(k);
             const unsigned m = __ballot_sync(0xffffffffu, need);
@@ -379,7 +460,7 @@ __device__ __forceinline__ void tile_walk(const TileArgs& a, int o, const Body& 
             const float dpx = v[u].x - A.x, dpy = v[u].y - A.y;
             const float dvx = v[u].z - A.vx, dvy = v[u].w - A.vy;
             const float c = fabsf(dpx * dvy - dpy * dvx) - E;
-            need[u] = valid && keep_of(k + u) && !(c * fabsf(c) > kl * (dvx * dvx + dvy * dvy));
+            need[u] = valid && !(c * fabsf(c) > kl * (dvx * dvx + dvy * dvy)) && keep_of(k + u);
         }
         const unsigned any = __ballot_sync(0xffffffffu, need[0] || need[1] || need[2] || need[3]);
         if (any) {
@@ -395,7 +476,7 @@ __device__ __forceinline__ void tile_walk(const TileArgs& a, int o, const Body& 
         const float dpx = v.x - A.x, dpy = v.y - A.y;
         const float dvx = v.z - A.vx, dvy = v.w - A.vy;
         const float c = fabsf(dpx * dvy - dpy * dvx) - E;
-        const bool need = valid && keep_of(k) && !(c * fabsf(c) > kl * (dvx * dvx + dvy * dvy));
+        const bool need = valid && !(c * fabsf(c) > kl * (dvx * dvx + dvy * dvy)) && keep_of(k);
         const unsigned m = __ballot_sync(0xffffffffu, need);
         if (m) queue_push(q, m, need, (int)(j0 + k), a, o, A, ab, lane);
     }
@@ -403,9 +484,20 @@ __device__ __forceinline__ void tile_walk(const TileArgs& a, int o, const Body& 
 
 // A warp takes a contiguous range of tiles (one binary search per warp,
 // then forward). Per tile: lane l holds run body p0 + 32 i + l; the tile's
-// partner box and the run bodies' box give P and V; the warp streams the
-// partners — the same record for every lane, one broadcast load — through
-// the keep rule and the line test, and queues the pairs it cannot skip.
+// partners span at most 32 aligned chunks of 32 records, and lane c tests
+// chunk c against the box of the run bodies: the chunk is skipped when every
+// pair of it is provably apart (below); the warp walks the surviving chunks
+// one by one, streaming their partners as broadcast loads through the keep
+// rule and the line test, and queues the pairs it cannot skip.
+//
+// Chunk skip: over all pairs of the run bodies and the chunk, |dp| is at
+// least the distance d of the two boxes and every (|dvx| + |dvy|) dt + rs is
+// at most reach = (Vx + Vy) dt + (rr_a,max + 1e-6 + rr_b,max) (Vx, Vy the
+// largest velocity differences of the boxes). If d > 2 reach, each pair has
+// |dp| > 2 ((|dvx| + |dvy|) dt + rs), so its closest approach over t in
+// [-dt, dt] exceeds 2 rs: the f32 test rejects it (its own rounding below
+// 1e-7 AU while the boxes' extents P and V dt stay below 0.5 AU, rs >= 1e-6
+// AU); 4.01 for 4 covers the rounding of the box arithmetic.
 __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
     __shared__ int q_j[BP_NT / 32][QCAP];
     __shared__ unsigned char q_l[BP_NT / 32][QCAP];
@@ -421,6 +513,7 @@ __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
     if (lane == 0) t0 = find_segment(a.tile_start, n_items, tb);
     long long t = __shfl_sync(0xffffffffu, t0, 0);
     long long t_start = a.tile_start[t], t_end = a.tile_start[t + 1];
+    const float dtf = a.tp.dtf;
     for (long long tid = tb; tid < te; ++tid) {
         while (t_end <= tid) {
             ++t;
@@ -444,45 +537,52 @@ __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
             A = Body{v.x, v.y, v.z, v.w, __uint_as_float(w.x)};
             ab = w.y;
         }
-        const long long jb = b0 + bi * TILE_B;
-        const int nj = (int)min((long long)TILE_B, b0 + nb - jb);
-        // boxes of the run bodies and of the partners -> P, V
-        float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
-        float bu0 = INFINITY, bu1 = -INFINITY, bw0 = INFINITY, bw1 = -INFINITY, brr = 0.0f;
-        for (int k = lane; k < nj; k += 32) {
-            const float4 v = a.rec[jb + k];
-            bx0 = fminf(bx0, v.x); bx1 = fmaxf(bx1, v.x);
-            by0 = fminf(by0, v.y); by1 = fmaxf(by1, v.y);
-            bu0 = fminf(bu0, v.z); bu1 = fmaxf(bu1, v.z);
-            bw0 = fminf(bw0, v.w); bw1 = fmaxf(bw1, v.w);
-            const float r = __uint_as_float(a.rec2[jb + k].x);
-            brr = r > brr || r != r ? r : brr;        // a NaN radius poisons the tile's bound
-        }
         const float ax0 = warp_min(valid ? A.x : INFINITY), ax1 = warp_max(valid ? A.x : -INFINITY);
         const float ay0 = warp_min(valid ? A.y : INFINITY), ay1 = warp_max(valid ? A.y : -INFINITY);
         const float au0 = warp_min(valid ? A.vx : INFINITY), au1 = warp_max(valid ? A.vx : -INFINITY);
         const float aw0 = warp_min(valid ? A.vy : INFINITY), aw1 = warp_max(valid ? A.vy : -INFINITY);
-        bx0 = warp_min(bx0); bx1 = warp_max(bx1); by0 = warp_min(by0); by1 = warp_max(by1);
-        bu0 = warp_min(bu0); bu1 = warp_max(bu1); bw0 = warp_min(bw0); bw1 = warp_max(bw1);
-        for (int d = 16; d; d >>= 1) {
-            const float r = __shfl_xor_sync(0xffffffffu, brr, d);
-            brr = r > brr || r != r ? r : brr;
+        float arr = valid ? A.rr : 0.0f;
+        for (int d = 16; d; d >>= 1) arr = nan_max(arr, __shfl_xor_sync(0xffffffffu, arr, d));
+        const long long jb = b0 + bi * TILE_B;
+        const long long je = min(jb + TILE_B, b0 + nb);
+        const long long c0 = jb >> 5;
+        const int nch = (int)(((je - 1) >> 5) - c0 + 1);
+        // lane c: chunk c0 + c
+        bool near = false;
+        float Pc = 0.0f, Vc = 0.0f, brr = 0.0f;
+        if (lane < nch) {
+            const ChunkBox bx = a.boxes[c0 + lane];
+            const float dxb = fmaxf(0.0f, fmaxf(bx.pos.x - ax1, ax0 - bx.pos.y));
+            const float dyb = fmaxf(0.0f, fmaxf(bx.pos.z - ay1, ay0 - bx.pos.w));
+            const float Vx = fmaxf(bx.vel.y - au0, au1 - bx.vel.x), Vy = fmaxf(bx.vel.w - aw0, aw1 - bx.vel.z);
+            Pc = fmaxf(fmaxf(bx.pos.y - ax0, ax1 - bx.pos.x), fmaxf(bx.pos.w - ay0, ay1 - bx.pos.z)) * 1.0001f;
+            Vc = fmaxf(Vx, Vy) * 1.0001f;
+            brr = bx.rad.x;
+            const float reach = (Vx + Vy) * 1.0001f * dtf + ((arr + 1e-6f) + brr);
+            const float d2 = dxb * dxb + dyb * dyb;
+            const bool far = Pc < 0.5f && Vc * dtf < 0.5f && reach < 1.0f && d2 > 4.01f * reach * reach;
+            near = !far;
         }
-        const float P = fmaxf(fmaxf(bx1 - ax0, ax1 - bx0), fmaxf(by1 - ay0, ay1 - by0)) * 1.0001f;
-        const float V = fmaxf(fmaxf(bu1 - au0, au1 - bu0), fmaxf(bw1 - aw0, aw1 - bw0)) * 1.0001f;
-        // a NaN radius or an unbounded box: no skips in the tile (warp-uniform;
-        // NaN coordinates need nothing here, as their line test never skips)
-        const bool skip_ok =
-            __all_sync(0xffffffffu, P < 0.5f && V * a.tp.dtf < 0.5f && brr == brr && (!valid || A.rr == A.rr));
-        const float E = 2.0f * EPS_CROSS * P * V;
-        const float rs = (A.rr + 1e-6f) + brr;
-        const float kl = 4.01f * rs * rs;
-        if (o == 0) {
-            tile_walk<0>(a, o, A, ab, pa, valid, jb, nj, E, kl, skip_ok, q, lane);
-        } else if (a.ks[b0] != a.ks[p0]) {
-            tile_walk<1>(a, o, A, ab, pa, valid, jb, nj, E, kl, skip_ok, q, lane);
-        } else {
-            tile_walk<2>(a, o, A, ab, pa, valid, jb, nj, E, kl, skip_ok, q, lane);
+        unsigned nm = __ballot_sync(0xffffffffu, near);
+        const int mode = o == 0 ? 0 : (a.ks[b0] != a.ks[p0] ? 1 : 2);
+        const float rsa = A.rr + 1e-6f;
+        while (nm) {
+            const int c = __ffs(nm) - 1;
+            nm &= nm - 1;
+            const float P = __shfl_sync(0xffffffffu, Pc, c), V = __shfl_sync(0xffffffffu, Vc, c);
+            const float br = __shfl_sync(0xffffffffu, brr, c);
+            // a NaN radius or an unbounded box: no line-test skips in the chunk (warp-uniform;
+            // NaN coordinates need nothing here, as their line test never skips)
+            const bool skip_ok =
+                __all_sync(0xffffffffu, P < 0.5f && V * dtf < 0.5f && br == br && (!valid || A.rr == A.rr));
+            const float E = 2.0f * EPS_CROSS * P * V;
+            const float rs = rsa + br;
+            const float kl = 4.01f * rs * rs;
+            const long long cs = (c0 + c) << 5;
+            const long long js = max(cs, jb), jn = min(cs + 32, je);
+            if (mode == 0) span_walk<0>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
+            else if (mode == 1) span_walk<1>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
+            else span_walk<2>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
         }
         if (q.cnt > 0) {                               // the rest of the tile's queue
             queue_flush(q, q.cnt, a, o, A, ab, lane);
@@ -526,6 +626,8 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_flag = take(nn), o_pos = take(nn), o_run = take(nn);
     const size_t o_ib0 = take(5 * nn), o_inb = take(5 * nn), o_tst = take(5 * nn + 1);
     const size_t o_rec = take(2 * nn), o_rec2 = take(nn);      // float4 and uint2 per alive body
+    const size_t o_rowkey = take(nn);                          // cell key per alive row
+    const size_t o_box = take((nn + 31) / 32 * (sizeof(ChunkBox) / 8));
     const size_t o_nh = take(2);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off * sizeof(long long), &scr);
@@ -549,6 +651,8 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     float4* rec = (float4*)(S + o_rec);
     uint2* rec2 = (uint2*)(S + o_rec2);
     unsigned long long* d_nh = (unsigned long long*)(S + o_nh);
+    unsigned long long* rowkey = (unsigned long long*)(S + o_rowkey);
+    ChunkBox* boxes = (ChunkBox*)(S + o_box);
     unsigned long long* d_ncand = d_nh + 1;
 
     // 1) alive compaction (ascending body order) + cells + keys
@@ -559,12 +663,22 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     if (na < 2) return SSS_OK;
     k_alive_scatter<<<(unsigned)tiles, BP_NT, 0, s>>>(is_ast, vis, x, y, nn, lo, hi_halo, h, counts, ai, cx, cy,
-                                                       k0, v0);
+                                                       rowkey, v0);
     SSS_LAUNCH_CHECK(ctx, "k_alive_scatter");
-    // 2) stable sort of the keys (ascending signed order)
+    // 2) sort by the position inside the cell, then stably by the cell key
+    //    (ascending signed order): key, then sub-cell, then body order
+    const unsigned nb_r = (unsigned)((na + 255) / 256);
+    k_sub_keys<<<nb_r, 256, 0, s>>>(x, y, ai, cx, cy, na, h, k0, v0);
+    SSS_LAUNCH_CHECK(ctx, "k_sub_keys");
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, na, scan_tmp, s, 12));
+    k_gather_keys<<<nb_r, 256, 0, s>>>(rowkey, v0, na, k0);
+    SSS_LAUNCH_CHECK(ctx, "k_gather_keys");
     SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, na, scan_tmp, s));
-    k_sorted_records<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, na, rec, rec2);
+    k_sorted_records<<<nb_r, 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, na, rec, rec2);
     SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
+    const long long n_chunks = (na + 31) / 32;
+    k_chunk_boxes<<<(unsigned)((n_chunks * 32 + 255) / 256), 256, 0, s>>>(rec, rec2, na, boxes);
+    SSS_LAUNCH_CHECK(ctx, "k_chunk_boxes");
     // 3) cell runs of the sorted order
     const unsigned nb_a = (unsigned)((na + 255) / 256);
     k_run_flags<<<nb_a, 256, 0, s>>>(cx, cy, v0, na, flags);
@@ -602,6 +716,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     ta.item_nb = item_nb;
     ta.tile_start = tile_st;
     ta.ks = k0;
+    ta.boxes = boxes;
     ta.na = na;
     ta.n_run = n_run;
     ta.n_tiles = n_tiles;

@@ -185,15 +185,19 @@ inline size_t radix_scratch(long long n) {
     return (size_t)(tiles * RS_BINS) + scan_scratch(tiles * RS_BINS);
 }
 
-// Stable ascending sort of unsigned 64-bit keys with values. keys/vals are
-// sorted through the alternate buffers; the result ends in (k0, v0).
+// Stable ascending sort of unsigned 64-bit keys with values, on the low
+// `bits` bits of the keys (the higher bits must be zero; rounded up to an
+// even number of 8-bit passes). keys/vals are sorted through the alternate
+// buffers; the result ends in (k0, v0).
 inline cudaError_t radix_sort(unsigned long long* k0, unsigned* v0, unsigned long long* k1, unsigned* v1,
-                              long long n, long long* scratch, cudaStream_t s) {
+                              long long n, long long* scratch, cudaStream_t s, int bits = 64) {
     if (n <= 1) return cudaSuccess;
     const int tiles = (int)((n + RS_TILE - 1) / RS_TILE);
     long long* hist = scratch;
     long long* scan_tmp = scratch + (size_t)tiles * RS_BINS;
-    for (int pass = 0; pass < 64 / RS_BITS; ++pass) {
+    const int want = (bits + 2 * RS_BITS - 1) / (2 * RS_BITS) * 2;
+    const int passes = want < 64 / RS_BITS ? want : 64 / RS_BITS;
+    for (int pass = 0; pass < passes; ++pass) {
         const int shift = pass * RS_BITS;
         unsigned long long* kin = (pass & 1) ? k1 : k0;
         unsigned* vin = (pass & 1) ? v1 : v0;
@@ -204,7 +208,7 @@ inline cudaError_t radix_sort(unsigned long long* k0, unsigned* v0, unsigned lon
         if (e != cudaSuccess) return e;
         k_rs_scatter<<<tiles, RS_NT, 0, s>>>(kin, vin, n, shift, hist, tiles, kout, vout);
     }
-    return cudaGetLastError();   // 8 passes: the result is back in (k0, v0)
+    return cudaGetLastError();   // an even number of passes: the result is back in (k0, v0)
 }
 
 }  // namespace
