@@ -3,7 +3,8 @@
 Tolerances: positions and velocities within 1e-9 of their scale after 50
 steps (f64, different rsqrt/FMA rounding only); every team mapping, the
 graph replay and one-launch-per-system give bit-identical states (each body
-sums its partners in the same order in all of them).
+sums its partners in the same order in all of them); the block-per-system
+mappings (partial sums over source chunks) agree to 1e-12 of the scale.
 """
 import numpy as np
 import pytest
@@ -32,26 +33,47 @@ def test_matches_oracle_per_system():
         assert np.abs(v - rv).max() <= 1e-9 * max(np.abs(rv).max(), 1e-30)
 
 
+def _state(ens):
+    return np.concatenate([np.concatenate([p, v], 1) for p, v in ens.export()], 1)
+
+
 def test_mappings_graph_and_single_launches_agree():
+    """Team mappings (shuffles, one lane per target), the graph replay and
+    one launch per system sum every body's partners in the same order:
+    bit-identical states. The block-per-system mappings add the partial sums
+    of their source chunks, and the autotuner may pick them: within 1e-12 of
+    the scale."""
     from solarsystemsimulator_b200 import batched
     systems = _ens(120, 12, seed=5)
-    runs = []
-    for variant in range(4):
-        ens = batched.BatchedSystems(systems, device=0, autotune=(variant == 0))
-        if variant == 1:
+    steps = 30
+
+    def run(variant, maps=None):
+        ens = batched.BatchedSystems(systems, device=0, autotune=(variant == "tuned"))
+        if maps is not None:
             for g in ens.groups:
-                g["map"] = batched.candidates(g["max_n"])[-1]        # largest team
-        if variant == 2:
-            ens.capture(30)
+                g["map"] = maps(g)
+        if variant == "graph":
+            ens.capture(steps)
             ens.replay()
-        elif variant == 3:
-            ens.run_one_launch_per_system(30)
+        elif variant == "single":
+            ens.run_one_launch_per_system(steps)
         else:
-            ens.run(30)
+            ens.run(steps)
         torch.cuda.synchronize()
-        runs.append(np.concatenate([np.concatenate([p, v], 1) for p, v in ens.export()], 1))
-    for r in runs[1:]:
-        assert np.array_equal(r, runs[0])
+        return _state(ens)
+
+    base = run("default")
+    widest_team = lambda g: [m for m in batched.candidates(g["max_n"]) if m[0] <= 32][-1]
+    for r in (run("default", widest_team), run("graph"), run("single")):
+        assert np.array_equal(r, base)
+    scale = np.abs(base).max(axis=0, keepdims=True)
+    for k in range(3):
+        blocks = lambda g, k=k: (batched.BLOCK_MAPS[32 if g["max_n"] <= 32 else 64][k] if g["max_n"] > 16
+                                 else g["map"])
+        r = run("default", blocks)
+        assert np.all(np.abs(r - base) <= 1e-12 * np.maximum(scale, 1e-30))
+    r = run("tuned")
+    assert np.all(np.abs(r - base) <= 1e-12 * np.maximum(scale, 1e-30))
 
 
 def test_figure8_conserves_energy_over_a_period():
