@@ -9,7 +9,7 @@ group runs in one persistent kernel (sss_batched_launch) with the team
 mapping that `autotune` measured fastest on this device: a team of T <= 32
 lanes with B bodies per lane (positions by warp shuffles), or for the larger
 groups a block of T threads per system that splits each body's sources
-over T / 32 or T / 64 threads. `run` launches every group concurrently, and
+over T / 16, T / 32 or T / 64 threads. `run` launches every group concurrently, and
 `capture(steps)` records those launches once into a CUDA graph that `replay`
 re-launches with one call.
 """
@@ -27,8 +27,12 @@ TEAMS = (1, 2, 4, 8, 16, 32)
 PER_LANE = (1, 2, 4, 8)
 SUPPORTED = {(1, 1), (1, 2), (1, 4), (1, 8), (2, 1), (2, 2), (2, 4), (2, 8), (4, 1), (4, 2), (4, 4), (4, 8),
              (8, 1), (8, 2), (8, 4), (8, 8), (16, 1), (16, 2), (16, 4), (32, 1), (32, 2)}
-# a block per system (T > 32 threads, B = 1): 32 or 64 targets x T / 32 or T / 64 source chunks
-BLOCK_MAPS = {32: ((64, 1), (128, 1), (256, 1)), 64: ((128, 1), (256, 1), (512, 1))}
+# a block per system (T > 32 threads, B = 1): 16, 32 or 64 targets x T / 16, T / 32 or T / 64 source chunks
+BLOCK_MAPS = {16: ((64, 1), (128, 1)), 32: ((64, 1), (128, 1), (256, 1)), 64: ((128, 1), (256, 1), (512, 1))}
+
+
+def block_bucket(max_n: int) -> int:
+    return 16 if max_n <= 16 else (32 if max_n <= 32 else 64)
 
 _tuned: dict = {}
 
@@ -40,8 +44,8 @@ def candidates(max_n: int):
         for b in PER_LANE:
             if (t, b) in SUPPORTED and t * b >= max_n and (t * b) // 2 < max_n:
                 out.append((t, b))
-    if max_n > 16:
-        out.extend(BLOCK_MAPS[32 if max_n <= 32 else 64])
+    if max_n > 8:
+        out.extend(BLOCK_MAPS[block_bucket(max_n)])
     return out
 
 

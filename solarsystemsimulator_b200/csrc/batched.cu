@@ -127,7 +127,8 @@ __global__ void __launch_bounds__(128) k_batched(const BatchArgs a) {
     }
 }
 
-// Block per system, for the larger groups: thread (t, c) of NT * S takes
+// Block per system, for the larger groups (NT = 16, 32 or 64 targets):
+// thread (t, c) of NT * S takes
 // target t and the sources j = c, c + S, c + 2S, ...; positions and masses
 // in shared memory, the S partial forces of a target added in chunk order.
 // A force evaluation is n / S dependent pair iterations instead of n, with
@@ -221,7 +222,8 @@ __global__ void __launch_bounds__(NT * S) k_batched_blk(const BatchArgs a) {
 template <int D>
 void* pick_blk(int NT, int S) {
 #define SSS_BLK(nt, s) if (NT == nt && S == s) return (void*)k_batched_blk<D, nt, s>;
-    SSS_BLK(32, 2) SSS_BLK(32, 4) SSS_BLK(32, 8) SSS_BLK(64, 2) SSS_BLK(64, 4) SSS_BLK(64, 8)
+    SSS_BLK(16, 4) SSS_BLK(16, 8) SSS_BLK(32, 2) SSS_BLK(32, 4) SSS_BLK(32, 8) SSS_BLK(64, 2) SSS_BLK(64, 4)
+    SSS_BLK(64, 8)
 #undef SSS_BLK
     return nullptr;
 }
@@ -250,9 +252,9 @@ extern "C" int sss_batched_launch(sss_ctx* ctx, int dim, double* const* x, doubl
     if (n_list < 0 || steps < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative count");
     if (n_list == 0 || steps == 0) return SSS_OK;
     if (!x || !v || !m || !off || !G || !dt || !sys_list) return sss_set_err(ctx, SSS_ERR_ARG, "NULL argument");
-    // team > 32: a block per system, NT = 32 or 64 targets (by max_n) x S = team / NT source chunks
+    // team > 32: a block per system, NT = 16, 32 or 64 targets (by max_n) x S = team / NT source chunks
     const bool blk = team > 32;
-    const int nt = max_n <= 32 ? 32 : 64;
+    const int nt = max_n <= 16 ? 16 : (max_n <= 32 ? 32 : 64);
     void* fn = nullptr;
     if (blk) {
         if (per_lane == 1 && team % nt == 0)

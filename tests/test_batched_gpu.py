@@ -68,8 +68,11 @@ def test_mappings_graph_and_single_launches_agree():
         assert np.array_equal(r, base)
     scale = np.abs(base).max(axis=0, keepdims=True)
     for k in range(3):
-        blocks = lambda g, k=k: (batched.BLOCK_MAPS[32 if g["max_n"] <= 32 else 64][k] if g["max_n"] > 16
-                                 else g["map"])
+        def blocks(g, k=k):
+            if g["max_n"] <= 8:
+                return g["map"]
+            maps = batched.BLOCK_MAPS[batched.block_bucket(g["max_n"])]
+            return maps[k % len(maps)]
         r = run("default", blocks)
         assert np.all(np.abs(r - base) <= 1e-12 * np.maximum(scale, 1e-30))
     r = run("tuned")
