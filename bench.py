@@ -566,6 +566,13 @@ def measure_batched(dev, stream, steps=10_000):
         ob.yoshida(s["pos"], s["vel"], s["mass"], s["G"], s["dt"], 10)
     tc = (time.perf_counter() - t0) / 10 / max(share, 1e-12)
     maps = {str(g["max_n"]): list(g["map"]) for g in ens.groups}
+    # FP64 roofline: pairs x 20 flop (the reference's convention) against a DFMA chain probe of this run
+    import ctypes
+    from solarsystemsimulator_b200 import _lib
+    ctx = _lib.context(dev)
+    probe = ctypes.c_double()
+    ctx.check(ctx.lib.sss_probe_fma(ctx.ptr, 0, 4096, ctypes.byref(probe)))
+    achieved = pairs * FLOP_PER_PAIR / t / 1e12
     return {"workload": "4096 systems (512 figure-8 + planetary 3-64 bodies), f64 Yoshida-4, dt = 1e-3 "
                         f"innermost period, {steps} steps in one captured graph",
             "steps_per_s": steps / t, "system_steps_per_s": len(systems) * steps / t,
@@ -573,6 +580,9 @@ def measure_batched(dev, stream, steps=10_000):
             "one_launch_per_system_steps_per_s_est": steps / t1_full,
             "speedup_vs_one_launch_per_system": t1_full / t,
             "team_mapping_by_group_max_n": maps,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": probe.value, "unit": "TFLOP/s",
+                         "frac": achieved / probe.value, "flop_per_pair": FLOP_PER_PAIR,
+                         "peak_source": "DFMA-chain probe measured in this run (sss_probe_fma)"},
             "cpu_baseline": {"value": 1.0 / tc, "unit": "ensemble steps/s", "cores": 1, "kind": "port",
                              "sample": "oracle/batched.py, 64 systems x 10 steps, scaled by pair share"}}
 
