@@ -16,10 +16,13 @@
 // bodies are compacted in ascending order (the reference's np.sort of the
 // concatenated tiers) and quantised in the same pass.
 //
-// The bisection resolves 5 halvings per round: the sum is monotone in s
-// (every term is, and rounded addition is monotone), so the 31 midpoints of
-// the next 5 levels of the halving tree can be summed at once and the 5
-// decisions read off them afterwards, each midpoint formed by the same
+// The bisection uses that the sum is monotone in s (every term is, and
+// rounded addition is monotone): its 40 decisions are those of the crossing
+// point. Normally all of them come from the histogram of the cell counts
+// (how many cells hold each count), with a certified error bound; where the
+// bound cannot decide, rounds resolve 5 halvings each by summing the 31
+// midpoints of the next 5 levels of the halving tree over all cells at once
+// and reading the 5 decisions off them, each midpoint formed by the same
 // arithmetic as the sequential halving.
 
 #include "sss_internal.cuh"
@@ -106,14 +109,16 @@ unsigned nb(long long n) { return (unsigned)((n + 255) / 256); }
 // ---------------------------------------------------------------- one sample
 // The whole sample is one cooperative launch of SAMPLE_THREADS-thread blocks,
 // all resident at once; its phases are separated by grid barriers:
-//   cull      display coordinates, tier per body (keep = 0), tier counts
+//   cull      display coordinates, tier per body (keep = 0), tier counts of
+//             the whole sample and of each block's range of bodies
 //   (plan)    every block reads the tier counts and takes the reference's
 //             branch of _lod_auswahl; the plan is uniform over the grid
-//   filter    per thinned tier: cell counts (hist), 8 bisection rounds of
-//             5 halvings each (group sums, then every block adds the top
-//             levels and walks the same decisions), rates, keep decisions
-//   emit      per-block kept counts, then each block places its contiguous
-//             range of bodies in ascending order
+//   filter    per thinned tier: cell counts (hist), the histogram of those
+//             counts (values), the 40 halvings from it (block 0; rounds of
+//             group sums over all cells for those it cannot decide), the
+//             rate of every cell, keep decisions and kept counts per block
+//   emit      each block places its range of bodies in ascending order
+//             after those of the blocks before it
 // A barrier wait polls at most BARRIER_POLLS times; when it runs out the
 // block records SSS_ERR_TIMEOUT and every block returns at its next barrier.
 constexpr int SAMPLE_THREADS = 512;
@@ -121,7 +126,7 @@ constexpr int SAMPLE_WARPS = SAMPLE_THREADS / 32;
 constexpr unsigned BARRIER_POLLS = 1u << 21;        // about a second with the 32 ns back-off
 constexpr int HIST_CHUNK = SAMPLE_THREADS * 4;      // bodies per shared-memory table fill
 constexpr int HIST_SLOTS = 2 * HIST_CHUNK;          // 4096: the hash yields 12 bits
-constexpr int EMIT_SUB = SAMPLE_THREADS * 4;        // bodies per block scan in the emit phase
+constexpr int EMIT_SUB = SAMPLE_THREADS * 8;        // bodies per block scan in the emit phase
 constexpr int BISECT_D = 5;                         // halvings per round
 constexpr int CAND = (1 << BISECT_D) - 1;           // 31 midpoints per round, lanes 0..30
 constexpr int GROUP_LEAVES = SAMPLE_WARPS;          // 16 leaves of 128 cells per group (warp = leaf)
@@ -137,13 +142,21 @@ struct Ctl {                                        // zeroed before every launc
     unsigned long long tier_cnt[4];
     unsigned long long kept[2];
     long long total;
-    int value_over;                                 // more distinct cell counts than the value table holds
+    int value_over[2];                              // per filter slot: more large distinct counts than vkey holds
     int fast_steps;                                 // halvings decided from the value histogram
     double lohi[2];                                 // the bisection interval after them
 };
 
-constexpr int VALUE_SLOTS = 8192;                   // distinct nonzero cell counts (open addressing)
-constexpr int VALUE_MAX = 4096;                     // at most this many are sorted by one block
+constexpr int VDIR = 4096;                          // cell counts below this: a table indexed by the count
+constexpr int LSLOTS = 2048;                        // a block's larger distinct counts (open addressing)
+constexpr int VALUE_SLOTS = 8192;                   // the grid's larger distinct counts (open addressing)
+constexpr int VALUE_MAX = 4096;                     // at most this many distinct counts take the fast path
+constexpr int SPRE_MAX = 1024;                      // fewer: their prefix sums are kept in shared memory
+
+// the per-block record of blk: [1..3] bodies of tiers 1..3, [4 + slot] kept
+// by the filter of that slot (a block of bodies: the contiguous range
+// body_range gives it in the cull, keep and emit phases)
+constexpr int BLK = 8;
 
 struct SampleArgs {
     const float* x;
@@ -159,18 +172,42 @@ struct SampleArgs {
     float* qy;
     unsigned char* tier;                            // n
     unsigned char* keep;                            // n
-    int* counts;                                    // K2 cell counts (cleared in the cull phase)
-    double* rate;                                   // K2 rate quads (4 doubles per cell)
+    int* counts;                                    // 2 x K2 cell counts, one table per filter slot
+    double* rate;                                   // K2 keep rates per cell
     double* part;                                   // 2 x CAND x GROUPS group sums
-    long long* blockcnt;                            // gridDim.x
+    long long* blk;                                 // BLK x gridDim.x: per block of bodies, its tier counts, kept counts
     unsigned* sel;
     unsigned short* ox;
     unsigned short* oy;
     Ctl* ctl;
-    int* vkey;                                      // VALUE_SLOTS: count value, -1 empty
-    unsigned* vmul;                                 // VALUE_SLOTS: cells holding it
+    unsigned* vdir;                                 // 2 x VDIR: cells holding each count below VDIR
+    int* vkey;                                      // 2 x VALUE_SLOTS: count value >= VDIR, -1 empty
+    unsigned* vmul;                                 // 2 x VALUE_SLOTS: cells holding it
     double* vpre;                                   // 2 VALUE_MAX: prefix sums of the sorted values
 };
+
+// the count tables of one filter slot (each filter of a launch has its own,
+// all cleared in the cull phase)
+struct Tables {
+    int* counts;
+    unsigned* vdir;
+    int* vkey;
+    unsigned* vmul;
+    int* over;
+};
+
+__device__ __forceinline__ Tables tables(const SampleArgs& a, int slot) {
+    return Tables{a.counts + (size_t)slot * K2, a.vdir + slot * VDIR, a.vkey + slot * VALUE_SLOTS,
+                  a.vmul + slot * VALUE_SLOTS, a.ctl->value_over + slot};
+}
+
+// bodies [c0, c1) of this block in the cull, keep and emit phases (c0 a
+// multiple of 8)
+__device__ __forceinline__ void body_range(long long n, long long& c0, long long& c1) {
+    const long long chunk = ((n + gridDim.x - 1) / gridDim.x + 7) / 8 * 8;
+    c0 = min((long long)blockIdx.x * chunk, n);
+    c1 = min(c0 + chunk, n);
+}
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
@@ -234,6 +271,11 @@ struct Smem {
             int key[HIST_SLOTS];
             int val[HIST_SLOTS];
         } h;
+        struct {                                    // values phase
+            unsigned dir[VDIR];                     // cells per count below VDIR
+            int lkey[LSLOTS];                       // larger counts
+            unsigned lval[LSLOTS];
+        } v;
         struct {                                    // bisection: one group's cells
             double c[GROUP_CELLS];
             double w[GROUP_CELLS];
@@ -252,20 +294,28 @@ struct Smem {
 // put many bodies of a chunk into a few cells) and adds every distinct cell
 // to the global counts once. The table has twice the chunk's slots, so a
 // probe ends within HIST_SLOTS steps.
-__device__ void phase_hist(const SampleArgs& a, const float* qx, const float* qy, int mask, Smem& sm) {
+__device__ void phase_hist(const SampleArgs& a, const Tables& tb, const float* qx, const float* qy, int mask,
+                           Smem& sm) {
     for (long long c0 = (long long)blockIdx.x * HIST_CHUNK; c0 < a.n; c0 += (long long)gridDim.x * HIST_CHUNK) {
         for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS) {
             sm.u.h.key[j] = -1;
             sm.u.h.val[j] = 0;
         }
         __syncthreads();
+        constexpr int R = HIST_CHUNK / SAMPLE_THREADS;
+        int cells[R];                                            // -1: not in this filter's tiers
 #pragma unroll
-        for (int r = 0; r < HIST_CHUNK / SAMPLE_THREADS; ++r) {
+        for (int r = 0; r < R; ++r) {                           // all loads first: one latency for the chunk
             const long long i = c0 + (long long)r * SAMPLE_THREADS + threadIdx.x;
-            if (i >= a.n) break;
-            const unsigned char t = __ldcg(a.tier + i);
-            if (!((mask >> t) & 1)) continue;
-            const int c = cell_of(__ldcg(qy + i), a.b.y0, a.b.sy) * K + cell_of(__ldcg(qx + i), a.b.x0, a.b.sx);
+            const bool ok = i < a.n;
+            const unsigned char t = ok ? __ldcg(a.tier + i) : 0;
+            const float px = ok ? __ldcg(qx + i) : 0.0f, py = ok ? __ldcg(qy + i) : 0.0f;
+            cells[r] = (mask >> t) & 1 ? cell_of(py, a.b.y0, a.b.sy) * K + cell_of(px, a.b.x0, a.b.sx) : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int c = cells[r];
+            if (c < 0) continue;
             unsigned h = ((unsigned)c * 2654435761u) >> 20;       // Fibonacci hash to 12 bits
             for (int probe = 0; probe < HIST_SLOTS; ++probe) {
                 const int prev = atomicCAS(sm.u.h.key + h, -1, c);
@@ -278,7 +328,7 @@ __device__ void phase_hist(const SampleArgs& a, const float* qx, const float* qy
         }
         __syncthreads();
         for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS)
-            if (sm.u.h.key[j] >= 0) atomicAdd(a.counts + sm.u.h.key[j], sm.u.h.val[j]);
+            if (sm.u.h.key[j] >= 0) atomicAdd(tb.counts + sm.u.h.key[j], sm.u.h.val[j]);
         __syncthreads();
     }
 }
@@ -290,13 +340,13 @@ __device__ void phase_hist(const SampleArgs& a, const float* qx, const float* qy
 // empty cells sums to +0 for every midpoint, as its terms min(0, s * 0) = +0
 // do; in a leaf with occupied cells the +0 terms of its empty cells are added
 // like the others (exactly).
-__device__ void phase_group_sums(const SampleArgs& a, double lo, double hi, double* part, Smem& sm) {
+__device__ void phase_group_sums(const Tables& tb, double lo, double hi, double* part, Smem& sm) {
     const int leaf = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int g = blockIdx.x; g < GROUPS; g += gridDim.x) {
         constexpr int PER_T = GROUP_CELLS / SAMPLE_THREADS;
         int cv[PER_T];
 #pragma unroll
-        for (int k = 0; k < PER_T; ++k) cv[k] = __ldcg(a.counts + g * GROUP_CELLS + k * SAMPLE_THREADS + threadIdx.x);
+        for (int k = 0; k < PER_T; ++k) cv[k] = __ldcg(tb.counts + g * GROUP_CELLS + k * SAMPLE_THREADS + threadIdx.x);
 #pragma unroll
         for (int k = 0; k < PER_T; ++k) {
             sm.u.g.c[k * SAMPLE_THREADS + threadIdx.x] = (double)cv[k];
@@ -410,51 +460,90 @@ __device__ __forceinline__ double block_excl_scan_d(double v, Smem& sm, double* 
     return before + (inc - v);
 }
 
-__device__ __forceinline__ void value_insert(const SampleArgs& a, int v, unsigned m) {
+__device__ __forceinline__ void value_insert(const Tables& tb, int v, unsigned m) {
     unsigned h = ((unsigned)v * 2654435761u) >> 19;                  // Fibonacci hash to 13 bits
     for (int probe = 0; probe < VALUE_SLOTS; ++probe) {
-        const int prev = atomicCAS(a.vkey + h, -1, v);
+        const int prev = atomicCAS(tb.vkey + h, -1, v);
         if (prev == -1 || prev == v) {
-            atomicAdd(a.vmul + h, m);
+            atomicAdd(tb.vmul + h, m);
             return;
         }
         h = (h + 1) & (VALUE_SLOTS - 1);
     }
-    atomicExch(&a.ctl->value_over, 1);
+    atomicExch(tb.over, 1);
 }
 static_assert(VALUE_SLOTS == 1 << 13, "13-bit hash");
 
 // The histogram of the nonzero cell counts (how many cells hold each count):
-// each block takes a contiguous range of cells, merges its values in a
-// shared-memory table and adds them to the global table. A global table that
-// runs out of slots sets value_over (the bisection then takes the exact path).
-__device__ void phase_values(const SampleArgs& a, Smem& sm) {
-    for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS) {
-        sm.u.h.key[j] = -1;
-        sm.u.h.val[j] = 0;
+// each block takes a contiguous range of cells and merges them in shared
+// memory, the counts below VDIR in a table indexed by the count and the
+// larger ones in an open-addressing table, then adds them to the global
+// tables (vdir, and vkey/vmul for the larger counts). A global table of
+// larger counts that runs out of slots sets value_over (the bisection then
+// takes the exact path).
+__device__ void phase_values(const Tables& tb, Smem& sm) {
+    for (int j = threadIdx.x; j < VDIR; j += SAMPLE_THREADS) sm.u.v.dir[j] = 0;
+    for (int j = threadIdx.x; j < LSLOTS; j += SAMPLE_THREADS) {
+        sm.u.v.lkey[j] = -1;
+        sm.u.v.lval[j] = 0;
     }
     __syncthreads();
     const long long per = (K2 + gridDim.x - 1) / gridDim.x;
     const long long c0 = (long long)blockIdx.x * per, c1 = min(c0 + per, (long long)K2);
     for (long long c = c0 + threadIdx.x; c < c1; c += SAMPLE_THREADS) {
-        const int v = __ldcg(a.counts + c);
+        const int v = __ldcg(tb.counts + c);
         if (v <= 0) continue;
-        unsigned h = ((unsigned)v * 2654435761u) >> 20;              // 12 bits
+        if (v < VDIR) {
+            atomicAdd(sm.u.v.dir + v, 1u);
+            continue;
+        }
+        unsigned h = ((unsigned)v * 2654435761u) >> 21;              // 11 bits
         bool done = false;
-        for (int probe = 0; probe < HIST_SLOTS; ++probe) {
-            const int prev = atomicCAS(sm.u.h.key + h, -1, v);
+        for (int probe = 0; probe < LSLOTS; ++probe) {
+            const int prev = atomicCAS(sm.u.v.lkey + h, -1, v);
             if (prev == -1 || prev == v) {
-                atomicAdd(sm.u.h.val + h, 1);
+                atomicAdd(sm.u.v.lval + h, 1u);
                 done = true;
                 break;
             }
-            h = (h + 1) & (HIST_SLOTS - 1);
+            h = (h + 1) & (LSLOTS - 1);
         }
-        if (!done) value_insert(a, v, 1u);                           // a full block table: straight to the global one
+        if (!done) value_insert(tb, v, 1u);                          // a full block table: straight to the global one
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < HIST_SLOTS; j += SAMPLE_THREADS)
-        if (sm.u.h.key[j] >= 0) value_insert(a, sm.u.h.key[j], (unsigned)sm.u.h.val[j]);
+    for (int j = threadIdx.x; j < VDIR; j += SAMPLE_THREADS)
+        if (sm.u.v.dir[j]) atomicAdd(tb.vdir + j, sm.u.v.dir[j]);
+    for (int j = threadIdx.x; j < LSLOTS; j += SAMPLE_THREADS)
+        if (sm.u.v.lkey[j] >= 0) value_insert(tb, sm.u.v.lkey[j], sm.u.v.lval[j]);
+    __syncthreads();
+}
+static_assert(LSLOTS == 1 << 11, "11-bit hash");
+static_assert(VDIR == 8 * SAMPLE_THREADS, "eight direct counts per thread");
+
+// Ascending bitonic sort of n (a power of two) (value, cells) pairs in
+// shared memory by the block. A stage of stride <= 32 pairs positions inside
+// the 64 that one warp's 32 pairs cover (pair i of a stage: positions
+// 2 i - (i mod stride) and that + stride), so between two such stages a
+// warp synchronises only itself.
+__device__ void block_bitonic(int* sv, int* sn, int n) {
+    for (int size = 2; size <= n; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < n / 2; i += SAMPLE_THREADS) {
+                const int l = 2 * i - (i & (stride - 1)), r = l + stride;
+                const bool up = (l & size) == 0;
+                const int vl = sv[l], vr = sv[r];
+                if ((vl > vr) == up) {
+                    const int nl = sn[l];
+                    sv[l] = vr;
+                    sv[r] = vl;
+                    sn[l] = sn[r];
+                    sn[r] = nl;
+                }
+            }
+            const int next = stride > 1 ? stride >> 1 : size;      // the following stage's stride
+            if (stride > 32 || next > 32) __syncthreads();
+            else __syncwarp();
+        }
     __syncthreads();
 }
 
@@ -471,16 +560,43 @@ __device__ void phase_values(const SampleArgs& a, Smem& sm) {
 // at v = s^2 included), and the prefix sums here err by less than 30 ulp of
 // W; so |f(s) - F(s)| < 1e-13 (F + s W + budget) with a wide margin. At the
 // first step inside that margin the walk stops; the exact rounds finish it.
-__device__ void block_fast_bisection(const SampleArgs& a, double budget, Smem& sm) {
+// The counts below VDIR come sorted from their direct table (thread t holds
+// counts 8 t .. 8 t + 7); only the larger ones are sorted here.
+__device__ void block_fast_bisection(const SampleArgs& a, const Tables& tb, double budget, Smem& sm) {
     int* sv = sm.u.h.key;                                            // sorted values (VALUE_MAX)
     int* sn = sm.u.h.val;                                            // their cell counts
     static_assert(HIST_SLOTS >= VALUE_MAX, "sort space");
+    static_assert(2 * SPRE_MAX * sizeof(double) <= HIST_SLOTS * sizeof(int) && SPRE_MAX <= 2 * SAMPLE_THREADS,
+                  "shared prefix sums fit the counts' space, two values per thread");
     constexpr int PER = VALUE_SLOTS / SAMPLE_THREADS;
-    int cnt = 0;
-    for (int q = 0; q < PER; ++q) cnt += __ldcg(a.vkey + threadIdx.x * PER + q) >= 0;
-    long long total = 0;
-    const long long off = block_excl_scan_ll(cnt, sm, &total);
-    if (__ldcg(&a.ctl->value_over) != 0 || total > VALUE_MAX || total < 1) {
+    static_assert(PER % 4 == 0 && PER <= 32, "int4 loads of the large-count slots, one mask word");
+    // the tables were filled by every block before the last grid barrier,
+    // whose acquire orders those writes before these (L1-cached) loads
+    const int* lkey = tb.vkey + threadIdx.x * PER;
+    unsigned dn[8], lmask = 0;
+    {
+        const uint4 d0 = *(const uint4*)(tb.vdir + 8 * threadIdx.x);
+        const uint4 d1 = *(const uint4*)(tb.vdir + 8 * threadIdx.x + 4);
+        dn[0] = d0.x; dn[1] = d0.y; dn[2] = d0.z; dn[3] = d0.w;
+        dn[4] = d1.x; dn[5] = d1.y; dn[6] = d1.z; dn[7] = d1.w;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; q += 4) {
+        const int4 k4 = *(const int4*)(lkey + q);
+        lmask |= (k4.x >= 0 ? 1u : 0u) << q | (k4.y >= 0 ? 2u : 0u) << q | (k4.z >= 0 ? 4u : 0u) << q |
+                 (k4.w >= 0 ? 8u : 0u) << q;
+    }
+    int cs = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) cs += dn[q] != 0;
+    const int cl = __popc(lmask);
+    long long total = 0;                                             // (small << 32) + large, both < 2^14
+    const long long off = block_excl_scan_ll(((long long)cs << 32) + cl, sm, &total);
+    const int Ds = (int)(total >> 32), Dl = (int)(total & 0xffffffffLL);
+    const int D = Ds + Dl;
+    int Dlp = Dl > 0 ? 1 : 0;
+    while (Dlp < Dl) Dlp <<= 1;
+    if (__ldcg(tb.over) != 0 || D > VALUE_MAX || D < 1 || Ds + Dlp > HIST_SLOTS) {
         if (threadIdx.x == 0) {
             a.ctl->lohi[0] = 0.0;
             a.ctl->lohi[1] = budget;
@@ -488,97 +604,178 @@ __device__ void block_fast_bisection(const SampleArgs& a, double budget, Smem& s
         }
         return;
     }
-    const int D = (int)total;
-    int Dp = 1;
-    while (Dp < D) Dp <<= 1;
-    int w = (int)off;
-    for (int q = 0; q < PER; ++q) {
-        const int slot = threadIdx.x * PER + q;
-        const int v = __ldcg(a.vkey + slot);
-        if (v >= 0) {
-            sv[w] = v;
-            sn[w] = (int)__ldcg(a.vmul + slot);
+    {
+        int w = (int)(off >> 32);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (dn[q]) {
+                sv[w] = 8 * threadIdx.x + q;
+                sn[w] = (int)dn[q];
+                ++w;
+            }
+        w = Ds + (int)(off & 0xffffffffLL);
+        for (unsigned m = lmask; m; m &= m - 1) {
+            const int q = __ffs(m) - 1;
+            sv[w] = lkey[q];
+            sn[w] = (int)tb.vmul[threadIdx.x * PER + q];
             ++w;
         }
     }
-    for (int i = D + threadIdx.x; i < Dp; i += SAMPLE_THREADS) {
+    for (int i = Ds + Dl + threadIdx.x; i < Ds + Dlp; i += SAMPLE_THREADS) {
         sv[i] = INT_MAX;
         sn[i] = 0;
     }
     __syncthreads();
-    // bitonic sort of (value, cells) by value, ascending (the values are distinct)
-    for (int size = 2; size <= Dp; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < Dp / 2; i += SAMPLE_THREADS) {
-                const int l = 2 * i - (i & (stride - 1)), r = l + stride;
-                const bool up = (l & size) == 0;
-                if ((sv[l] > sv[r]) == up) {
-                    const int tv = sv[l], tn = sn[l];
-                    sv[l] = sv[r];
-                    sn[l] = sn[r];
-                    sv[r] = tv;
-                    sn[r] = tn;
-                }
-            }
-            __syncthreads();
+    if (Dl > 1 && Dl <= SAMPLE_THREADS) {
+        // the larger counts (all >= VDIR, distinct): each of Dl threads
+        // counts the smaller ones, then places its own
+        int v = 0, c = 0, rank = 0;
+        if ((int)threadIdx.x < Dl) {
+            v = sv[Ds + threadIdx.x];
+            c = sn[Ds + threadIdx.x];
+            for (int j = 0; j < Dl; ++j) rank += sv[Ds + j] < v;
         }
-    // prefix sums over chunks of consecutive values, then across the chunks
+        __syncthreads();
+        if ((int)threadIdx.x < Dl) {
+            sv[Ds + rank] = v;
+            sn[Ds + rank] = c;
+        }
+        __syncthreads();
+    } else if (Dl > 1) {
+        block_bitonic(sv + Ds, sn + Ds, Dlp);
+    }
+    // prefix sums over chunks of consecutive values, then across the chunks.
+    // With D < SPRE_MAX (at most 2 values per thread) they replace the cell
+    // counts in shared memory (each thread keeps its own counts in
+    // registers), else they go to global memory.
     const int ch = (D + SAMPLE_THREADS - 1) / SAMPLE_THREADS;
     const int i0 = threadIdx.x * ch, i1 = min(i0 + ch, D);
+    const bool in_smem = D < SPRE_MAX;
+    double* pre = in_smem ? (double*)sn : a.vpre;
+    int n0 = 0, n1 = 0;
     double la = 0.0, lw = 0.0;
     for (int i = i0; i < i1; ++i) {
-        la += (double)sn[i] * (double)sv[i];
-        lw += (double)sn[i] * cell_weight(sv[i]);
+        const int c = sn[i];
+        if (i == i0) n0 = c;
+        else n1 = c;
+        la += (double)c * (double)sv[i];
+        lw += (double)c * cell_weight(sv[i]);
     }
     double tot_a = 0.0, tot_w = 0.0;
-    double ea = block_excl_scan_d(la, sm, &tot_a);
+    double ea = block_excl_scan_d(la, sm, &tot_a);                   // (the scans' barriers end the reads of sn)
     double ew = block_excl_scan_d(lw, sm, &tot_w);
     for (int i = i0; i < i1; ++i) {
-        a.vpre[2 * i] = ea;
-        a.vpre[2 * i + 1] = ew;
-        ea += (double)sn[i] * (double)sv[i];
-        ew += (double)sn[i] * cell_weight(sv[i]);
+        const int c = !in_smem ? sn[i] : (i == i0 ? n0 : n1);
+        pre[2 * i] = ea;
+        pre[2 * i + 1] = ew;
+        ea += (double)c * (double)sv[i];
+        ew += (double)c * cell_weight(sv[i]);
     }
     if (threadIdx.x == 0) {
-        a.vpre[2 * D] = tot_a;
-        a.vpre[2 * D + 1] = tot_w;
+        pre[2 * D] = tot_a;
+        pre[2 * D + 1] = tot_w;
     }
     __syncthreads();
-    // warp 0: BISECT_D halvings per round, lane c evaluating the midpoint of
-    // node c + 1 of the halving tree below (lo, hi) (node_mid: the same
-    // arithmetic as the sequential halving), the decisions read off the
-    // path by shuffles; the walk stops at the first uncertain node
+    // warp 0. F at the breakpoints b_i = v_i ** 0.5 (where k = i + 1) grows
+    // with i: a 32-way search finds the piece on which F crosses the budget,
+    // and that piece's line gives an estimate s_est of the crossing. The
+    // reference's sum grows with s (each term min(c, s w) does, and so does a
+    // rounded sum), so its halvings go up exactly where the midpoint lies
+    // above its crossing: the 40 halvings the estimate predicts are checked
+    // at once (step j on lane j and lane j - 32), each taken when F at its
+    // midpoint certainly lies on the predicted side of the budget, up to the
+    // first that is not. Where that leaves steps, rounds of BISECT_D
+    // halvings go on from there, lane c evaluating the midpoint of node c + 1
+    // of the halving tree below (lo, hi) (node_mid: the same arithmetic as
+    // the sequential halving), the certain decisions in two ballots, up to
+    // the first uncertain node. k(s) grows with s, so inside [lo, hi] it
+    // lies between the k of the nodes that set lo and hi.
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         const double W = tot_w;
-        double lo = 0.0, hi = budget;
-        int steps = 0;
+        int bl = -1, bh = D;                                         // F(b_bl) <= budget < F(b_bh), virtual ends
+        while (bh - bl > 1) {
+            const int step = (bh - bl + 31) / 32;
+            const int i = bl + (lane + 1) * step;
+            bool le = false;
+            if (i < bh) le = pre[2 * i + 2] + cell_weight(sv[i]) * (W - pre[2 * i + 3]) <= budget;
+            const int c = __popc(__ballot_sync(0xffffffffu, le));
+            bh = min(bh, bl + (c + 1) * step);
+            bl += c * step;
+        }
+        const double den = W - pre[2 * (bl + 1) + 1];
+        const double s_est = den > 0.0 ? (budget - pre[2 * (bl + 1)]) / den : budget;
+        double lo = 0.0, hi = budget, s0 = 0.0, s1 = 0.0;
+        bool p0 = false, p1 = false;
+        for (int j = 0; j < 40; ++j) {
+            const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
+            const bool up = s > s_est;
+            if (j == lane) {
+                s0 = s;
+                p0 = up;
+            }
+            if (j == lane + 32) {
+                s1 = s;
+                p1 = up;
+            }
+            if (up) hi = s;
+            else lo = s;
+        }
+        auto certain = [&](double s, bool up) {
+            const double s2 = s * s;
+            int l = 0, r = D;                                        // k = #values <= s^2
+            while (l < r) {
+                const int m = (l + r) >> 1;
+                if ((double)sv[m] <= s2) l = m + 1;
+                else r = m;
+            }
+            const double F = pre[2 * l] + s * (W - pre[2 * l + 1]);
+            const double margin = 1e-13 * (F + s * W + budget);
+            return up ? F > budget + margin : F < budget - margin;
+        };
+        const unsigned ok0 = __ballot_sync(0xffffffffu, certain(s0, p0));
+        const unsigned ok1 = __ballot_sync(0xffffffffu, lane >= 8 || certain(s1, p1));
+        const unsigned long long bad = (unsigned long long)~ok0 | ((unsigned long long)(~ok1 & 0xffu) << 32);
+        int steps = bad ? __ffsll((long long)bad) - 1 : 40;
+        lo = 0.0;
+        hi = budget;
+        for (int j = 0; j < steps; ++j) {
+            const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
+            if (s > s_est) hi = s;
+            else lo = s;
+        }
+        int klo = 0, khi = D;
         bool stop = false;
         while (steps < 40 && !stop) {
-            double F = 0.0, margin = 0.0;
+            int k = 0;
+            bool up = false, down = false;
             if (lane < CAND) {
                 const double s = node_mid(lane + 1, lo, hi);
                 const double s2 = s * s;
-                int l = 0, r = D;                                    // k = #values <= s^2
+                int l = klo, r = khi;                                // k = #values <= s^2
                 while (l < r) {
                     const int m = (l + r) >> 1;
                     if ((double)sv[m] <= s2) l = m + 1;
                     else r = m;
                 }
-                F = a.vpre[2 * l] + s * (W - a.vpre[2 * l + 1]);
-                margin = 1e-13 * (F + s * W + budget);
+                k = l;
+                const double F = pre[2 * l] + s * (W - pre[2 * l + 1]);
+                const double margin = 1e-13 * (F + s * W + budget);
+                up = F > budget + margin;
+                down = F < budget - margin;
             }
+            const unsigned b_up = __ballot_sync(0xffffffffu, up), b_down = __ballot_sync(0xffffffffu, down);
             const int levels = min(BISECT_D, 40 - steps);
-            int node = 1;
+            int node = 1, n_lo = 0, n_hi = 0;
             for (int d = 0; d < levels; ++d) {
-                const double Fn = __shfl_sync(0xffffffffu, F, node - 1);
-                const double Mn = __shfl_sync(0xffffffffu, margin, node - 1);
                 const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
-                if (Fn > budget + Mn) {
+                if ((b_up >> (node - 1)) & 1) {
                     hi = s;
+                    n_hi = node;
                     node = 2 * node;
-                } else if (Fn < budget - Mn) {
+                } else if ((b_down >> (node - 1)) & 1) {
                     lo = s;
+                    n_lo = node;
                     node = 2 * node + 1;
                 } else {
                     stop = true;
@@ -586,6 +783,10 @@ __device__ void block_fast_bisection(const SampleArgs& a, double budget, Smem& s
                 }
                 ++steps;
             }
+            const int k_lo = __shfl_sync(0xffffffffu, k, max(n_lo - 1, 0));
+            const int k_hi = __shfl_sync(0xffffffffu, k, max(n_hi - 1, 0));
+            if (n_lo) klo = k_lo;
+            if (n_hi) khi = k_hi;
         }
         if (lane == 0) {
             a.ctl->lohi[0] = lo;
@@ -597,21 +798,23 @@ __device__ void block_fast_bisection(const SampleArgs& a, double budget, Smem& s
 
 // The reference's _dichte_filter over the tiers in mask with `budget`
 // points (size > budget); keep[i] = 1 for the kept bodies, their number in
-// ctl->kept[slot]. Returns false when a barrier gave up.
+// ctl->kept[slot] and, per block of bodies, in its record. Returns false
+// when a barrier gave up.
 __device__ bool filter(const SampleArgs& a, const float* qx, const float* qy, int mask, long long budget, int slot,
                        unsigned& epoch, Smem& sm) {
-    phase_hist(a, qx, qy, mask, sm);
+    const Tables tb = tables(a, slot);
+    phase_hist(a, tb, qx, qy, mask, sm);
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
-    phase_values(a, sm);
+    phase_values(tb, sm);
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
-    if (blockIdx.x == 0) block_fast_bisection(a, (double)budget, sm);
+    if (blockIdx.x == 0) block_fast_bisection(a, tb, (double)budget, sm);
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
     double lo = __ldcg(&a.ctl->lohi[0]), hi = __ldcg(&a.ctl->lohi[1]);
     // the halvings the histogram could not decide (normally none): exact rounds
     int left = 40 - __ldcg(&a.ctl->fast_steps);
     for (int round = 0; left > 0; ++round) {
         double* part = a.part + (round & 1) * CAND * GROUPS;
-        phase_group_sums(a, lo, hi, part, sm);
+        phase_group_sums(tb, lo, hi, part, sm);
         if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
         const int levels = min(BISECT_D, left);
         phase_walk(part, (double)budget, lo, hi, levels, sm);
@@ -619,66 +822,70 @@ __device__ bool filter(const SampleArgs& a, const float* qx, const float* qy, in
     }
     const long long T = (long long)gridDim.x * SAMPLE_THREADS;
     const long long gt = (long long)blockIdx.x * SAMPLE_THREADS + threadIdx.x;
-    // rate quad of cell (iy, ix): the rates of (iy, ix), (iy, ix1), (iy1, ix),
-    // (iy1, ix1), the four a body's bilinear rate reads, in one 32-byte sector
+    // the keep rate of every cell: min(k, lo k ** 0.5) / k, 0 for an empty cell
     for (long long c = gt; c < K2; c += T) {
-        const int ix = (int)(c % K), iy = (int)(c / K);
-        const int ix1 = min(ix + 1, K - 1), iy1 = min(iy + 1, K - 1);
-        const int cells[4] = {iy * K + ix, iy * K + ix1, iy1 * K + ix, iy1 * K + ix1};
-        double r[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = __ldcg(a.counts + cells[q]);
-            r[q] = k > 0 ? __ddiv_rn(fmin((double)k, __dmul_rn(lo, cell_weight(k))), (double)k) : 0.0;
-        }
-        double2* dst = (double2*)(a.rate + 4 * c);
-        dst[0] = make_double2(r[0], r[1]);
-        dst[1] = make_double2(r[2], r[3]);
+        const int k = __ldcg(tb.counts + c);
+        a.rate[c] = k > 0 ? __ddiv_rn(fmin((double)k, __dmul_rn(lo, cell_weight(k))), (double)k) : 0.0;
     }
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
     const unsigned char* __restrict__ tier = a.tier;
     unsigned char* __restrict__ keep = a.keep;
+    const double* __restrict__ rate = a.rate;
+    long long c0, c1;
+    body_range(a.n, c0, c1);
     long long kept = 0;
-    for (long long i0 = gt; i0 < a.n; i0 += 2 * T) {
-        unsigned char t[2];
-        float px[2], py[2];
+    // two bodies per thread and pass, in three stages (loads, rate gathers,
+    // decisions) so that both bodies' gathers are in flight together. A body
+    // reads the rates of cells (iy, ix), (iy, ix1), (iy1, ix), (iy1, ix1)
+    // for its bilinear rate. The gathers are plain (L1-cached) loads: a dense
+    // cloud puts many bodies into the same few cells, and L2-only loads of
+    // those rates queue at their L2 slices. The rates were written by other
+    // blocks before the last grid barrier, whose acquire orders them before
+    // these loads.
+    for (long long i0 = c0 + threadIdx.x; i0 < c1; i0 += 2 * SAMPLE_THREADS) {
+        bool in[2];
+        float fx[2], fy[2];
+        int ix[2], iy[2];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-            const long long i = i0 + u * T;
-            t[u] = i < a.n ? __ldcg(tier + i) : 0;
-            px[u] = i < a.n ? __ldcg(qx + i) : 0.0f;
-            py[u] = i < a.n ? __ldcg(qy + i) : 0.0f;
+            const long long i = i0 + u * SAMPLE_THREADS;
+            const bool ok = i < c1;
+            const unsigned char t = ok ? __ldcg(tier + i) : 0;
+            const float px = ok ? __ldcg(qx + i) : 0.0f, py = ok ? __ldcg(qy + i) : 0.0f;
+            in[u] = (mask >> t) & 1;
+            fx[u] = frac_coord(px, a.b.x0, a.b.sx);
+            fy[u] = frac_coord(py, a.b.y0, a.b.sy);
+            ix[u] = (int)floorf(fx[u]);
+            iy[u] = (int)floorf(fy[u]);
+        }
+        double r[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int x1 = min(ix[u] + 1, K - 1), y1 = min(iy[u] + 1, K - 1);
+            const int cells[4] = {iy[u] * K + ix[u], iy[u] * K + x1, y1 * K + ix[u], y1 * K + x1};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r[u][q] = in[u] ? rate[cells[q]] : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-            if (!((mask >> t[u]) & 1)) continue;
-            const long long i = i0 + u * T;
-            const float fx = frac_coord(px[u], a.b.x0, a.b.sx), fy = frac_coord(py[u], a.b.y0, a.b.sy);
-            const int ix = (int)floorf(fx), iy = (int)floorf(fy);
-            const double2* rq = (const double2*)(a.rate + 4 * (iy * K + ix));
-            const double2 r0 = __ldcg(rq), r1 = __ldcg(rq + 1);
-            const double tx = __dsub_rn((double)fx, (double)ix), ty = __dsub_rn((double)fy, (double)iy);
+            const long long i = i0 + u * SAMPLE_THREADS;
+            const double tx = __dsub_rn((double)fx[u], (double)ix[u]), ty = __dsub_rn((double)fy[u], (double)iy[u]);
             const double ux = __dsub_rn(1.0, tx), uy = __dsub_rn(1.0, ty);
-            double rp = __dmul_rn(__dmul_rn(r0.x, ux), uy);
-            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r0.y, tx), uy));
-            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r1.x, ux), ty));
-            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r1.y, tx), ty));
-            if (index_hash((unsigned long long)i) < rp) {
+            double rp = __dmul_rn(__dmul_rn(r[u][0], ux), uy);
+            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r[u][1], tx), uy));
+            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r[u][2], ux), ty));
+            rp = __dadd_rn(rp, __dmul_rn(__dmul_rn(r[u][3], tx), ty));
+            if (in[u] && index_hash((unsigned long long)i) < rp) {
                 keep[i] = 1;
                 ++kept;
             }
         }
     }
-    // the cell counts are dead now (the rates hold what the keep decisions
-    // need): clear them for a following filter
-    for (long long c = gt; c < K2; c += T) a.counts[c] = 0;
-    for (long long c = gt; c < VALUE_SLOTS; c += T) {
-        a.vkey[c] = -1;
-        a.vmul[c] = 0;
-    }
-    if (gt == 0) a.ctl->value_over = 0;
     kept = block_sum_ll(kept, sm.red);
-    if (threadIdx.x == 0 && kept) atomicAdd(a.ctl->kept + slot, (unsigned long long)kept);
+    if (threadIdx.x == 0) {
+        a.blk[(size_t)blockIdx.x * BLK + 4 + slot] = kept;
+        if (kept) atomicAdd(a.ctl->kept + slot, (unsigned long long)kept);
+    }
     return grid_barrier(a.ctl, epoch, &sm.bad);
 }
 
@@ -689,34 +896,52 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     const long long gt = (long long)blockIdx.x * SAMPLE_THREADS + threadIdx.x;
     const float* qx = a.log_zoom ? a.qx : a.x;
     const float* qy = a.log_zoom ? a.qy : a.y;
-    // ---- cull
+    // ---- cull (and clear both filter slots' count tables)
     long long n1 = 0, n2 = 0, n3 = 0;
-    for (long long c = gt; c < K2; c += T) a.counts[c] = 0;
-    for (long long c = gt; c < VALUE_SLOTS; c += T) {
+    for (long long c = gt; c < 2 * K2; c += T) a.counts[c] = 0;
+    for (long long c = gt; c < 2 * VALUE_SLOTS; c += T) {
         a.vkey[c] = -1;
         a.vmul[c] = 0;
     }
-    if (gt == 0) a.ctl->value_over = 0;
-    for (long long i = gt; i < a.n; i += T) {
-        float px = a.x[i], py = a.y[i];
-        const double kt = a.kill_t[i];
-        const unsigned char ast = a.is_ast[i], inj = a.injected ? a.injected[i] : 0;
-        if (a.log_zoom) {
-            const float r = hypotf(px, py);
-            const float sk = r > 1e-9f ? __fdiv_rn(log1pf(r), __fmul_rn(LOG33F, fmaxf(r, 1e-30f))) : 0.0f;
-            px = __fmul_rn(px, sk);
-            py = __fmul_rn(py, sk);
-            a.qx[i] = px;
-            a.qy[i] = py;
+    for (long long c = gt; c < 2 * VDIR; c += T) a.vdir[c] = 0;
+    long long c0, c1;
+    body_range(a.n, c0, c1);
+    for (long long i0 = c0 + threadIdx.x; i0 < c1; i0 += 4 * SAMPLE_THREADS) {
+        float bx[4], by[4];
+        double kt[4];
+        unsigned char ast[4], inj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {                           // all loads first: one latency per pass
+            const long long i = i0 + u * SAMPLE_THREADS;
+            const bool ok = i < c1;
+            bx[u] = ok ? a.x[i] : 0.0f;
+            by[u] = ok ? a.y[i] : 0.0f;
+            kt[u] = ok ? a.kill_t[i] : 0.0;
+            ast[u] = ok ? a.is_ast[i] : 0;
+            inj[u] = ok && a.injected ? a.injected[i] : 0;
         }
-        unsigned char t = 0;
-        if ((kt > a.t_cut) & (px >= a.b.x0) & (px <= a.b.x1) & (py >= a.b.y0) & (py <= a.b.y1))
-            t = !ast ? 1 : (inj ? 3 : 2);
-        a.tier[i] = t;
-        a.keep[i] = 0;
-        n1 += t == 1;
-        n2 += t == 2;
-        n3 += t == 3;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long i = i0 + u * SAMPLE_THREADS;
+            if (i >= c1) break;
+            float px = bx[u], py = by[u];
+            if (a.log_zoom) {
+                const float r = hypotf(px, py);
+                const float sk = r > 1e-9f ? __fdiv_rn(log1pf(r), __fmul_rn(LOG33F, fmaxf(r, 1e-30f))) : 0.0f;
+                px = __fmul_rn(px, sk);
+                py = __fmul_rn(py, sk);
+                a.qx[i] = px;
+                a.qy[i] = py;
+            }
+            unsigned char t = 0;
+            if ((kt[u] > a.t_cut) & (px >= a.b.x0) & (px <= a.b.x1) & (py >= a.b.y0) & (py <= a.b.y1))
+                t = !ast[u] ? 1 : (inj[u] ? 3 : 2);
+            a.tier[i] = t;
+            a.keep[i] = 0;
+            n1 += t == 1;
+            n2 += t == 2;
+            n3 += t == 3;
+        }
     }
     n1 = block_sum_ll(n1, sm.red);
     n2 = block_sum_ll(n2, sm.red);
@@ -725,6 +950,12 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         if (n1) atomicAdd(a.ctl->tier_cnt + 1, (unsigned long long)n1);
         if (n2) atomicAdd(a.ctl->tier_cnt + 2, (unsigned long long)n2);
         if (n3) atomicAdd(a.ctl->tier_cnt + 3, (unsigned long long)n3);
+        long long* rec = a.blk + (size_t)blockIdx.x * BLK;
+        rec[1] = n1;
+        rec[2] = n2;
+        rec[3] = n3;
+        rec[4] = 0;
+        rec[5] = 0;
     }
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return;
     // ---- plan (the reference's _lod_auswahl), identical in every block
@@ -774,26 +1005,60 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
             }
         }
     }
-    // ---- emit: block b owns bodies [b * chunk, (b + 1) * chunk)
-    const long long chunk = ((a.n + gridDim.x - 1) / gridDim.x + EMIT_SUB - 1) / EMIT_SUB * EMIT_SUB;
-    const long long c0 = (long long)blockIdx.x * chunk, c1 = min(c0 + chunk, a.n);
-    long long mine = 0;
-    for (long long i = c0 + threadIdx.x; i < c1; i += SAMPLE_THREADS)
-        mine += __ldcg(a.keep + i) | ((all_mask >> __ldcg(a.tier + i)) & 1);
-    mine = block_sum_ll(mine, sm.red);
-    if (threadIdx.x == 0) a.blockcnt[blockIdx.x] = mine;
-    if (!grid_barrier(a.ctl, epoch, &sm.bad)) return;
+    // ---- emit: block b places its bodies [c0, c1) after those of blocks
+    // 0 .. b - 1. A block emits its kept bodies and its bodies of the tiers
+    // in all_mask (never a filtered tier): its record holds both numbers.
     long long before = 0;
-    for (int j = threadIdx.x; j < (int)blockIdx.x; j += SAMPLE_THREADS) before += __ldcg(a.blockcnt + j);
+    for (int j = threadIdx.x; j < (int)blockIdx.x; j += SAMPLE_THREADS) {
+        const long long* rec = a.blk + (size_t)j * BLK;
+        long long e = __ldcg(rec + 4) + __ldcg(rec + 5);
+#pragma unroll
+        for (int t = 1; t <= 3; ++t)
+            if ((all_mask >> t) & 1) e += __ldcg(rec + t);
+        before += e;
+    }
     long long off = block_sum_ll(before, sm.red);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // 8 consecutive bodies per thread: flags in one 8-byte load each, the
+    // coordinates in float4 loads where both arrays are 16-byte aligned (the
+    // ranges start at multiples of 8)
+    const bool vec = ((reinterpret_cast<unsigned long long>(qx) | reinterpret_cast<unsigned long long>(qy)) & 15) == 0;
     for (long long s0 = c0; s0 < c1; s0 += EMIT_SUB) {
-        const long long i0 = s0 + (long long)threadIdx.x * 4;
-        unsigned bits = 0;
+        const long long i0 = s0 + (long long)threadIdx.x * 8;
+        unsigned bits = 0, oq[8];                                // oq: the quantised (x, y) of each body
+        auto put = [&](int j, unsigned kp, unsigned t, float px, float py) {
+            if (kp | ((all_mask >> t) & 1)) bits |= 1u << j;
+            oq[j] = (unsigned)quant(px, a.b.x0, a.b.sx) | (unsigned)quant(py, a.b.y0, a.b.sy) << 16;
+        };
+        if (i0 + 7 < c1) {                                      // all loads first: one latency per sub-range
+            const uint2 k8 = __ldcg((const uint2*)(a.keep + i0)), t8 = __ldcg((const uint2*)(a.tier + i0));
+            float xs[8], ys[8];
+            if (vec) {
+                const float4 x0 = __ldcg((const float4*)(qx + i0)), x1 = __ldcg((const float4*)(qx + i0 + 4));
+                const float4 y0 = __ldcg((const float4*)(qy + i0)), y1 = __ldcg((const float4*)(qy + i0 + 4));
+                xs[0] = x0.x; xs[1] = x0.y; xs[2] = x0.z; xs[3] = x0.w;
+                xs[4] = x1.x; xs[5] = x1.y; xs[6] = x1.z; xs[7] = x1.w;
+                ys[0] = y0.x; ys[1] = y0.y; ys[2] = y0.z; ys[3] = y0.w;
+                ys[4] = y1.x; ys[5] = y1.y; ys[6] = y1.z; ys[7] = y1.w;
+            } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const long long i = i0 + j;
-            if (i < c1 && (__ldcg(a.keep + i) | ((all_mask >> __ldcg(a.tier + i)) & 1))) bits |= 1u << j;
+                for (int j = 0; j < 8; ++j) {
+                    xs[j] = __ldcg(qx + i0 + j);
+                    ys[j] = __ldcg(qy + i0 + j);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const unsigned kw = j < 4 ? k8.x : k8.y, tw = j < 4 ? t8.x : t8.y, sh = 8 * (j & 3);
+                put(j, (kw >> sh) & 0xffu, (tw >> sh) & 0xffu, xs[j], ys[j]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const long long i = i0 + j;
+                oq[j] = 0;
+                if (i < c1) put(j, __ldcg(a.keep + i), __ldcg(a.tier + i), __ldcg(qx + i), __ldcg(qy + i));
+            }
         }
         const int c = __popc(bits);
         int inc = c;
@@ -812,12 +1077,12 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         }
         long long q = off + wb + inc - c;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 8; ++j) {
             if (!((bits >> j) & 1)) continue;
             const long long i = i0 + j;
             a.sel[q] = (unsigned)i;
-            a.ox[q] = quant(__ldcg(qx + i), a.b.x0, a.b.sx);
-            a.oy[q] = quant(__ldcg(qy + i), a.b.y0, a.b.sy);
+            a.ox[q] = (unsigned short)(oq[j] & 0xffffu);
+            a.oy[q] = (unsigned short)(oq[j] >> 16);
             ++q;
         }
         off += all;
@@ -831,10 +1096,11 @@ struct Work {
     unsigned char *tier, *keep;
     int* counts;
     double *rate, *part;
+    unsigned* vdir;
     int* vkey;
     unsigned* vmul;
     double* vpre;
-    long long* blockcnt;
+    long long* blk;
     Ctl* ctl;
 };
 
@@ -846,13 +1112,14 @@ int make_work(sss_ctx* ctx, long long n, int grid, int n_ctl, Work* W) {
     const size_t o_qy = off; off += al((size_t)n * 4);
     const size_t o_tier = off; off += al((size_t)n);
     const size_t o_keep = off; off += al((size_t)n);
-    const size_t o_cnts = off; off += al((size_t)K2 * 4);
-    const size_t o_rate = off; off += al((size_t)K2 * 32);
+    const size_t o_cnts = off; off += al((size_t)2 * K2 * 4);
+    const size_t o_rate = off; off += al((size_t)K2 * 8);
     const size_t o_part = off; off += al((size_t)2 * CAND * GROUPS * 8);
-    const size_t o_vkey = off; off += al((size_t)VALUE_SLOTS * 4);
-    const size_t o_vmul = off; off += al((size_t)VALUE_SLOTS * 4);
+    const size_t o_vdir = off; off += al((size_t)2 * VDIR * 4);
+    const size_t o_vkey = off; off += al((size_t)2 * VALUE_SLOTS * 4);
+    const size_t o_vmul = off; off += al((size_t)2 * VALUE_SLOTS * 4);
     const size_t o_vpre = off; off += al((size_t)2 * (VALUE_MAX + 1) * 8);
-    const size_t o_blk = off; off += al((size_t)grid * 8);
+    const size_t o_blk = off; off += al((size_t)grid * BLK * 8);
     const size_t o_ctl = off; off += al(sizeof(Ctl) * (size_t)n_ctl);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off, &scr);
@@ -865,10 +1132,11 @@ int make_work(sss_ctx* ctx, long long n, int grid, int n_ctl, Work* W) {
     W->counts = (int*)(p + o_cnts);
     W->rate = (double*)(p + o_rate);
     W->part = (double*)(p + o_part);
+    W->vdir = (unsigned*)(p + o_vdir);
     W->vkey = (int*)(p + o_vkey);
     W->vmul = (unsigned*)(p + o_vmul);
     W->vpre = (double*)(p + o_vpre);
-    W->blockcnt = (long long*)(p + o_blk);
+    W->blk = (long long*)(p + o_blk);
     W->ctl = (Ctl*)(p + o_ctl);
     return SSS_OK;
 }
@@ -968,7 +1236,8 @@ int sample_batch(sss_ctx* ctx, int64_t n, int k, const float* const* x, const fl
     a.counts = W.counts;
     a.rate = W.rate;
     a.part = W.part;
-    a.blockcnt = W.blockcnt;
+    a.blk = W.blk;
+    a.vdir = W.vdir;
     a.vkey = W.vkey;
     a.vmul = W.vmul;
     a.vpre = W.vpre;

@@ -206,3 +206,43 @@ def test_many_distinct_cell_counts_take_the_exact_rounds():
     assert np.array_equal(sel.view(np.uint32), rs)
     assert np.array_equal(qx.view(np.uint16), rx) and np.array_equal(qy.view(np.uint16), ry)
     assert 100_000 < len(rs) < 140_000
+
+
+# cell counts that reach each path of the count histogram: counts on both
+# sides of the direct table's end (4096), up to 512 larger counts (ranked)
+# and more (bitonic network), and more than 1024 distinct counts (prefix
+# sums in global memory)
+HIST_CASES = {
+    "direct_1500": np.arange(1, 1501),
+    "across_4096": np.concatenate([np.arange(1, 1001), np.arange(4000, 4201)]),
+    "ranked_300": np.concatenate([np.arange(1, 200), 4096 + 7 * np.arange(300)]),
+    "bitonic_600": np.concatenate([np.arange(1, 100), 4096 + np.arange(600)]),
+}
+
+
+@pytest.mark.parametrize("name", list(HIST_CASES))
+def test_count_histogram_paths(name):
+    """Cell j of a shuffled set of LOD cells holds counts[j] asteroids:
+    bit-exact against the oracle, with the LOD budget thinning them."""
+    from oracle import frames as ofr
+    from solarsystemsimulator_b200.stream import StreamFrames
+    k = 512
+    counts = HIST_CASES[name]
+    rng = np.random.default_rng(len(name))
+    cells = rng.choice(k * k, len(counts), replace=False)
+    cid = np.repeat(cells, counts)
+    x = ((cid % k + 0.5 + rng.uniform(-0.3, 0.3, len(cid))) / k).astype(np.float32)
+    y = ((cid // k + 0.5 + rng.uniform(-0.3, 0.3, len(cid))) / k).astype(np.float32)
+    n = len(x)
+    a = np.ones(n, bool)
+    inj = np.zeros(n, bool)
+    view = (0.5, 0.5, 0.25, 0.25)                     # box (0, 0, 1, 1): one LOD cell per grid cell
+    box = ofr.make_box(x, y, view)
+    sf = StreamFrames(a, inj)
+    xd, yd = torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda()
+    assert sf.box(xd, yd, view, False) == box
+    sel, qx, qy = (t.cpu().numpy() for t in sf.sample(xd, yd, 0.5, 0.5, box, False, 120_000))
+    rs, rx, ry = ofr.sample_frame(x, y, np.ones(n, bool), a, inj, box, False, 120_000)
+    assert np.array_equal(sel.view(np.uint32), rs)
+    assert np.array_equal(qx.view(np.uint16), rx) and np.array_equal(qy.view(np.uint16), ry)
+    assert 80_000 < len(rs) <= 120_000
