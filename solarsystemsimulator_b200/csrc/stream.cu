@@ -809,9 +809,11 @@ __device__ bool filter(const SampleArgs& a, const float* qx, const float* qy, in
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
     if (blockIdx.x == 0) block_fast_bisection(a, tb, (double)budget, sm);
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return false;
-    double lo = __ldcg(&a.ctl->lohi[0]), hi = __ldcg(&a.ctl->lohi[1]);
+    // every thread reads the control words after a barrier: L1-cached loads,
+    // so that one request per SM reaches their L2 line
+    double lo = __ldca(&a.ctl->lohi[0]), hi = __ldca(&a.ctl->lohi[1]);
     // the halvings the histogram could not decide (normally none): exact rounds
-    int left = 40 - __ldcg(&a.ctl->fast_steps);
+    int left = 40 - __ldca(&a.ctl->fast_steps);
     for (int round = 0; left > 0; ++round) {
         double* part = a.part + (round & 1) * CAND * GROUPS;
         phase_group_sums(tb, lo, hi, part, sm);
@@ -959,8 +961,9 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     }
     if (!grid_barrier(a.ctl, epoch, &sm.bad)) return;
     // ---- plan (the reference's _lod_auswahl), identical in every block
-    const long long mm = (long long)__ldcg(a.ctl->tier_cnt + 1), ma = (long long)__ldcg(a.ctl->tier_cnt + 2),
-                    mi = (long long)__ldcg(a.ctl->tier_cnt + 3);
+    // (every thread reads the counts: L1-cached loads, one L2 request per SM)
+    const long long mm = (long long)__ldca(a.ctl->tier_cnt + 1), ma = (long long)__ldca(a.ctl->tier_cnt + 2),
+                    mi = (long long)__ldca(a.ctl->tier_cnt + 3);
     const long long m = mm + ma + mi;
     const int T_ALL = (1 << 1) | (1 << 2) | (1 << 3), T_MASS = 1 << 1, T_AST = (1 << 2) | (1 << 3);
     int all_mask = 0;
@@ -977,7 +980,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
                     all_mask |= T_MASS;
                 } else {
                     if (!filter(a, qx, qy, T_MASS, m_budget, 0, epoch, sm)) return;
-                    kept = (long long)__ldcg(a.ctl->kept + 0);
+                    kept = (long long)__ldca(a.ctl->kept + 0);
                 }
                 rest = a.budget - kept;
                 if (rest > 0 && ma + mi > 0) {
@@ -999,7 +1002,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
                     all_mask |= masks[q];
                 } else {
                     if (!filter(a, qx, qy, masks[q], rest, q, epoch, sm)) return;
-                    kept = (long long)__ldcg(a.ctl->kept + q);
+                    kept = (long long)__ldca(a.ctl->kept + q);
                 }
                 rest -= kept;
             }
@@ -1011,10 +1014,10 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     long long before = 0;
     for (int j = threadIdx.x; j < (int)blockIdx.x; j += SAMPLE_THREADS) {
         const long long* rec = a.blk + (size_t)j * BLK;
-        long long e = __ldcg(rec + 4) + __ldcg(rec + 5);
+        long long e = __ldca(rec + 4) + __ldca(rec + 5);            // (read by every later block: L1-cached)
 #pragma unroll
         for (int t = 1; t <= 3; ++t)
-            if ((all_mask >> t) & 1) e += __ldcg(rec + t);
+            if ((all_mask >> t) & 1) e += __ldca(rec + t);
         before += e;
     }
     long long off = block_sum_ll(before, sm.red);
