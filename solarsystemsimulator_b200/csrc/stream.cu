@@ -284,6 +284,7 @@ struct Smem {
     double leaf[GROUP_LEAVES][32];
     double tot[32];
     double dred[SAMPLE_WARPS];
+    double dred2[SAMPLE_WARPS];
     long long red[SAMPLE_WARPS];
     int wcnt[SAMPLE_WARPS];
     int bad;
@@ -318,8 +319,12 @@ __device__ void phase_hist(const SampleArgs& a, const Tables& tb, const float* q
             if (c < 0) continue;
             unsigned h = ((unsigned)c * 2654435761u) >> 20;       // Fibonacci hash to 12 bits
             for (int probe = 0; probe < HIST_SLOTS; ++probe) {
-                const int prev = atomicCAS(sm.u.h.key + h, -1, c);
-                if (prev == -1 || prev == c) {
+                int k = *(volatile int*)(sm.u.h.key + h);
+                if (k == -1) {
+                    k = atomicCAS(sm.u.h.key + h, -1, c);
+                    if (k == -1) k = c;                              // this lane took the slot
+                }
+                if (k == c) {
                     atomicAdd(sm.u.h.val + h, 1);
                     break;
                 }
@@ -439,25 +444,41 @@ __device__ __forceinline__ long long block_excl_scan_ll(long long v, Smem& sm, l
     return before + inc - v;
 }
 
-__device__ __forceinline__ double block_excl_scan_d(double v, Smem& sm, double* total) {
+// two exclusive block scans of doubles at once: shuffle scans in each warp,
+// then the warp totals added in warp order; a thread's exclusive value is
+// its inclusive one minus its own term
+__device__ __forceinline__ void block_excl_scan_d2(double va, double vb, Smem& sm, double& ea, double& eb,
+                                                   double& ta, double& tb) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double inc = v;
+    double ia = va, ib = vb;
     for (int o = 1; o < 32; o <<= 1) {
-        const double t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
+        const double xa = __shfl_up_sync(0xffffffffu, ia, o), xb = __shfl_up_sync(0xffffffffu, ib, o);
+        if (lane >= o) {
+            ia += xa;
+            ib += xb;
+        }
     }
     __syncthreads();
-    if (lane == 31) sm.dred[warp] = inc;
+    if (lane == 31) {
+        sm.dred[warp] = ia;
+        sm.dred2[warp] = ib;
+    }
     __syncthreads();
-    double before = 0.0, all = 0.0;
+    double ba = 0.0, aa = 0.0, bb = 0.0, ab = 0.0;
 #pragma unroll
     for (int w = 0; w < SAMPLE_WARPS; ++w) {
-        const double x = sm.dred[w];
-        if (w < warp) before += x;
-        all += x;
+        const double xa = sm.dred[w], xb = sm.dred2[w];
+        if (w < warp) {
+            ba += xa;
+            bb += xb;
+        }
+        aa += xa;
+        ab += xb;
     }
-    *total = all;
-    return before + (inc - v);
+    ta = aa;
+    tb = ab;
+    ea = ba + (ia - va);
+    eb = bb + (ib - vb);
 }
 
 __device__ __forceinline__ void value_insert(const Tables& tb, int v, unsigned m) {
@@ -573,6 +594,8 @@ __device__ void block_fast_bisection(const SampleArgs& a, const Tables& tb, doub
     // the tables were filled by every block before the last grid barrier,
     // whose acquire orders those writes before these (L1-cached) loads
     const int* lkey = tb.vkey + threadIdx.x * PER;
+    const int over = *tb.over;
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(tb.vmul + threadIdx.x * PER));  // read below for the occupied slots
     unsigned dn[8], lmask = 0;
     {
         const uint4 d0 = *(const uint4*)(tb.vdir + 8 * threadIdx.x);
@@ -596,7 +619,7 @@ __device__ void block_fast_bisection(const SampleArgs& a, const Tables& tb, doub
     const int D = Ds + Dl;
     int Dlp = Dl > 0 ? 1 : 0;
     while (Dlp < Dl) Dlp <<= 1;
-    if (__ldcg(tb.over) != 0 || D > VALUE_MAX || D < 1 || Ds + Dlp > HIST_SLOTS) {
+    if (over != 0 || D > VALUE_MAX || D < 1 || Ds + Dlp > HIST_SLOTS) {
         if (threadIdx.x == 0) {
             a.ctl->lohi[0] = 0.0;
             a.ctl->lohi[1] = budget;
@@ -661,9 +684,8 @@ __device__ void block_fast_bisection(const SampleArgs& a, const Tables& tb, doub
         la += (double)c * (double)sv[i];
         lw += (double)c * cell_weight(sv[i]);
     }
-    double tot_a = 0.0, tot_w = 0.0;
-    double ea = block_excl_scan_d(la, sm, &tot_a);                   // (the scans' barriers end the reads of sn)
-    double ew = block_excl_scan_d(lw, sm, &tot_w);
+    double tot_a, tot_w, ea, ew;
+    block_excl_scan_d2(la, lw, sm, ea, ew, tot_a, tot_w);           // (its barriers end the reads of sn)
     for (int i = i0; i < i1; ++i) {
         const int c = !in_smem ? sn[i] : (i == i0 ? n0 : n1);
         pre[2 * i] = ea;
@@ -705,21 +727,25 @@ __device__ void block_fast_bisection(const SampleArgs& a, const Tables& tb, doub
         }
         const double den = W - pre[2 * (bl + 1) + 1];
         const double s_est = den > 0.0 ? (budget - pre[2 * (bl + 1)]) / den : budget;
-        double lo = 0.0, hi = budget, s0 = 0.0, s1 = 0.0;
+        double lo = 0.0, hi = budget, s0 = 0.0, s1 = 0.0, lo0 = 0.0, hi0 = 0.0, lo1 = 0.0, hi1 = 0.0;
         bool p0 = false, p1 = false;
-        for (int j = 0; j < 40; ++j) {
+        for (int j = 0; j < 40; ++j) {                               // lane j (and j - 32) keeps step j and the interval after it
             const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
             const bool up = s > s_est;
+            if (up) hi = s;
+            else lo = s;
             if (j == lane) {
                 s0 = s;
                 p0 = up;
+                lo0 = lo;
+                hi0 = hi;
             }
             if (j == lane + 32) {
                 s1 = s;
                 p1 = up;
+                lo1 = lo;
+                hi1 = hi;
             }
-            if (up) hi = s;
-            else lo = s;
         }
         auto certain = [&](double s, bool up) {
             const double s2 = s * s;
@@ -737,12 +763,13 @@ __device__ void block_fast_bisection(const SampleArgs& a, const Tables& tb, doub
         const unsigned ok1 = __ballot_sync(0xffffffffu, lane >= 8 || certain(s1, p1));
         const unsigned long long bad = (unsigned long long)~ok0 | ((unsigned long long)(~ok1 & 0xffu) << 32);
         int steps = bad ? __ffsll((long long)bad) - 1 : 40;
-        lo = 0.0;
-        hi = budget;
-        for (int j = 0; j < steps; ++j) {
-            const double s = __dmul_rn(0.5, __dadd_rn(lo, hi));
-            if (s > s_est) hi = s;
-            else lo = s;
+        if (steps == 0) {
+            lo = 0.0;
+            hi = budget;
+        } else {                                                     // the interval after step steps - 1
+            const int j = steps - 1;
+            lo = __shfl_sync(0xffffffffu, j < 32 ? lo0 : lo1, j & 31);
+            hi = __shfl_sync(0xffffffffu, j < 32 ? hi0 : hi1, j & 31);
         }
         int klo = 0, khi = D;
         bool stop = false;
