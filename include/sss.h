@@ -376,6 +376,15 @@ int  sss_pm3_gather(sss_pm3* p, const sss_pm3_particles* s, int mode, double hdt
                     void* stream);
 /* opening half kick and drift of one KDK step: v += hdt a; x = wrap(x + dt v) */
 int  sss_pm3_kick_drift(sss_pm3* p, const sss_pm3_particles* s, double hdt, double dt, void* stream);
+/* short-range part of a P3M force (no reference counterpart: the exact
+ * complement of a mesh solved with r_split = 1 / (2 alpha)): adds
+ * G m (erfc(alpha r) + 2 alpha r e^{-alpha^2 r^2} / sqrt(pi) + (1 + eps^2 /
+ * r^2)^{-3/2} - 1) d / r^3 over the pairs closer than r_cut (nearest
+ * periodic image, r_cut <= box / 3) to the accelerations in s->a (a mesh
+ * force from an SSS_PM3_FORCE gather), then runs the epilogue `mode` as
+ * sss_pm3_gather does */
+int  sss_pm3_short(sss_pm3* p, const sss_pm3_particles* s, double G, double alpha, double r_cut, double eps,
+                   int mode, double hdt, double dt, float* snap, void* stream);
 
 /* ------------------------------------------------ Ewald direct sum, f64
  *

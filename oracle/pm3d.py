@@ -19,6 +19,10 @@ reciprocal part over k = 2 pi h / L with |h| <= h_max, plus the Plummer
 softening applied to the nearest image of every pair as
 (r^2 + eps^2)^(-3/2) - r^-3 (so the result does not depend on alpha).
 
+The P3M pair term (p3m_short) has no reference counterpart: it is the
+exact complement of the Gaussian-filtered mesh force (the Ewald real-space
+term with alpha = 1 / (2 r_s)) plus the softening, inside r_cut.
+
 The MLP restatement (67 -> 128 -> 128 -> 3, SiLU) rounds to bf16 at exactly
 the points where the tensor-core kernels do (inputs, weights, hidden
 activations, output and hidden deltas), so its gradients are comparable with
@@ -178,6 +182,35 @@ def ewald_pair(r2, alpha, eps2, rc2, near_image=True):
     soft = np.expm1(-1.5 * np.log1p(eps2 / r2)) * inv_r3
     far = soft + np.where(r2 < rc2, (erfc(x) + gauss) * inv_r3, 0.0)
     return np.where(small, close, far)
+
+
+def p3m_short(src, mass, tgt, alpha, r_cut, G=1.0, L=1.0, eps=0.0, self_index=None):
+    """The P3M pair term at tgt (T, 3), f64: over the sources closer than
+    r_cut (nearest image, r_cut <= L / 3), a += G m (erfc(x) + 2x/sqrt(pi)
+    e^{-x^2} + (1 + eps^2/r^2)^{-3/2} - 1) d / r^3 with x = alpha r and
+    d = x_j - x_i; coincident pairs and self_index[i] are skipped. No
+    reference counterpart: the exact complement of the mesh force filtered
+    by exp(-k^2 r_split^2), r_split = 1 / (2 alpha) (the Ewald real-space
+    term of ewald_pair with the softening kept inside r_cut)."""
+    src = np.asarray(src, np.float64)
+    tgt = np.asarray(tgt, np.float64)
+    m = np.asarray(mass, np.float64)
+    out = np.zeros((len(tgt), 3))
+    eps2 = float(eps) ** 2
+    sp = 2.0 / math.sqrt(math.pi)
+    for i in range(len(tgt)):
+        d = src - tgt[i]
+        d = d - L * np.rint(d / L)
+        r2 = (d * d).sum(1)
+        keep = (r2 > 0.0) & (r2 < r_cut * r_cut)
+        if self_index is not None and self_index[i] >= 0:
+            keep[self_index[i]] = False
+        r2k = r2[keep]
+        r = np.sqrt(r2k)
+        x = alpha * r
+        g = erfc(x) + sp * x * np.exp(-x * x) + np.expm1(-1.5 * np.log1p(eps2 / r2k))
+        out[i] = G * ((m[keep] * g / (r2k * r)) @ d[keep])
+    return out
 
 
 def ewald_accel(src, mass, tgt, G=1.0, L=1.0, alpha=10.0, r_cut=0.46, h_max=17, eps=0.0,

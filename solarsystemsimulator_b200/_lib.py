@@ -138,6 +138,9 @@ SIGNATURES = {
                                       ctypes.c_double, _dp, _vp]),
     "sss_pm3_kick_drift": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.c_double, ctypes.c_double,
                                           _vp]),
+    "sss_pm3_short": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, _dp, _vp]),
     "sss_ewald_structure": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.c_double, _dp, ctypes.c_int,
                                            ctypes.c_int, _dp, _vp]),
     "sss_ewald_accel": (ctypes.c_int, [_vp, ctypes.POINTER(Pm3Particles), ctypes.POINTER(_dp), _dp, _c_i64,

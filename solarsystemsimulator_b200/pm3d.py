@@ -45,9 +45,15 @@ class PMPeriodic3D:
     """Mesh solver of one mesh size (an sss_pm3 plan) and the KDK stepper."""
 
     def __init__(self, mesh_n: int = 256, box: float = 1.0, G: float = 1.0, device: int = 0, deconv: int = 2,
-                 r_split_cells: float = 0.6):
+                 r_split_cells: float = 0.6, short_range: bool = False, softening: float = 0.0,
+                 x_cut: float = 3.5):
         """Green's function -4 pi G / k^2 * W_CIC(k)^-deconv *
-        exp(-k^2 r_split^2), r_split = r_split_cells mesh cells."""
+        exp(-k^2 r_split^2), r_split = r_split_cells mesh cells.
+
+        short_range adds the P3M pair term every force pass: the exact
+        complement of that mesh force (erfc split with alpha = 1 / (2
+        r_split)) and the Plummer softening, for pairs closer than r_cut =
+        x_cut / alpha (sss_pm3_short)."""
         self.device = int(device)
         self.ctx = _lib.context(device)
         self.mesh_n = int(mesh_n)
@@ -55,6 +61,12 @@ class PMPeriodic3D:
         self.G = float(G)
         self.deconv = int(deconv)
         self.r_split = float(r_split_cells) * self.box / self.mesh_n
+        self.short_range = bool(short_range)
+        self.softening = float(softening)
+        self.alpha = 0.5 / self.r_split if self.r_split > 0.0 else 0.0
+        self.r_cut = float(x_cut) / self.alpha if self.alpha > 0.0 else 0.0
+        if self.short_range and not (self.r_split > 0.0 and 3.0 * self.r_cut <= self.box):
+            raise ValueError("short_range needs r_split > 0 and r_cut <= box / 3")
         ptr = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             self.ctx.check(self.ctx.lib.sss_pm3_create(self.ctx.ptr, self.mesh_n, self.box, ctypes.byref(ptr)))
@@ -143,10 +155,25 @@ class PMPeriodic3D:
     def kick_drift(self, st, hdt: float, dt: float) -> None:
         self._call("sss_pm3_kick_drift", ctypes.byref(st["parts"]), float(hdt), float(dt))
 
+    def short(self, st, mode=_lib.PM3_FORCE, hdt=0.0, dt=0.0, snap=None) -> None:
+        """Add the P3M pair term to the mesh force in the state, then the
+        epilogue `mode`."""
+        self._call("sss_pm3_short", ctypes.byref(st["parts"]), self.G, self.alpha, self.r_cut, self.softening,
+                   int(mode), float(hdt), float(dt), snap.data_ptr() if snap is not None else None)
+
+    def method_forces(self, st, mode=_lib.PM3_FORCE, hdt=0.0, dt=0.0, snap=None) -> None:
+        """The force without the network (mesh, and the pair term when
+        short_range) with the epilogue `mode`."""
+        self.mesh_forces(st)
+        if self.short_range:
+            self.gather(st)
+            self.short(st, mode, hdt, dt, snap)
+        else:
+            self.gather(st, mode, hdt, dt, snap)
+
     def forces(self, st, net: ShortRangeMLP | None = None) -> torch.Tensor:
         """Accelerations at the current positions into the state (3, N)."""
-        self.mesh_forces(st)
-        self.gather(st)
+        self.method_forces(st)
         if net is not None:
             net_correct(net, self, st, _lib.PM3_FORCE, 0.0, 0.0, None)
         st["acc_valid"] = True
@@ -167,11 +194,10 @@ class PMPeriodic3D:
         for s in range(steps):
             mode = _lib.PM3_KICK_DRIFT if s < steps - 1 else _lib.PM3_KICK
             row = snap[s] if snap is not None else None
-            self.mesh_forces(st)
             if net is None:
-                self.gather(st, mode, hdt, dt, row)
+                self.method_forces(st, mode, hdt, dt, row)
             else:
-                self.gather(st)
+                self.method_forces(st)
                 net_correct(net, self, st, mode, hdt, dt, row)
         return snap.cpu().numpy() if snap is not None else None
 
@@ -226,10 +252,11 @@ class NBodyPMLearned:
     def __init__(self, device: int = 0, mesh_n: int = 256, box: float = 1.0, G: float = 1.0,
                  softening: float = 1e-3, check_every: int = 50, samples: int = 16384, tol: float | None = None,
                  iters: int = 200, batch: int = 2048, lr: float = 1e-3, seed: int = 0, fallback: str = "mesh",
-                 learned: bool = True, deconv: int = 2, r_split_cells: float = 0.6):
+                 learned: bool = True, deconv: int = 2, r_split_cells: float = 0.6, short_range: bool = False,
+                 x_cut: float = 3.5):
         if fallback not in ("mesh", "direct"):
             raise ValueError("fallback must be 'mesh' or 'direct'")
-        self.pm = PMPeriodic3D(mesh_n, box, G, device, deconv, r_split_cells)
+        self.pm = PMPeriodic3D(mesh_n, box, G, device, deconv, r_split_cells, short_range, softening, x_cut)
         self.net = ShortRangeMLP(device, seed) if learned else None
         self.ewald = EwaldDirect(box, G, softening, device=device)
         self.judge = CorrectionJudge(tol)
@@ -265,9 +292,9 @@ class NBodyPMLearned:
         return self.ewald.accel(st["parts"], tgt, idx)
 
     def _mesh_at(self, st, idx):
-        """Mesh forces of all particles into the state; returns them at idx."""
-        self.pm.mesh_forces(st)
-        self.pm.gather(st)
+        """The force without the network (mesh, and the P3M pair term when
+        short_range) of all particles into the state; returns it at idx."""
+        self.pm.method_forces(st)
         return st["buf"][6:9, idx].clone()
 
     def _full_force(self, st):

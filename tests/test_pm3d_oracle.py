@@ -7,6 +7,8 @@ depend on the splitting parameter alpha, a symmetric lattice feels no
 force, the mesh force conserves momentum and agrees with the direct sum on
 a smooth density, and the MLP gradient matches finite differences.
 """
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -163,3 +165,35 @@ def test_adam_restatement():
     p1, m1, v1 = o.adam(p, g, m, v, 1, 0.1)
     # first step of Adam moves every parameter by lr against its gradient's sign
     assert np.allclose(p1, p - 0.1 * np.sign(g), rtol=0, atol=1e-6)
+
+
+def test_p3m_pair_term_two_bodies():
+    """Two bodies 0.01 apart, across the periodic boundary: the pair term is
+    G m (erfc(x) + 2x e^{-x^2}/sqrt(pi) + (1 + eps^2/r^2)^{-3/2} - 1) / r^2
+    towards the other body; nothing beyond r_cut."""
+    from oracle import pm3d as opm
+    alpha, eps = 32.0, 2e-3
+    pos = np.array([[0.995, 0.3, 0.7], [0.005, 0.3, 0.7]])
+    a = opm.p3m_short(pos, np.array([2.0, 3.0]), pos, alpha, 0.1, eps=eps, self_index=np.array([0, 1]))
+    r, x = 0.01, alpha * 0.01
+    g = math.erfc(x) + 2.0 / math.sqrt(math.pi) * x * math.exp(-x * x) + (1.0 + eps * eps / (r * r)) ** -1.5 - 1.0
+    assert a[0, 0] == pytest.approx(3.0 * g / r ** 2, rel=1e-12)
+    assert a[1, 0] == pytest.approx(-2.0 * g / r ** 2, rel=1e-12)
+    assert np.abs(a[:, 1:]).max() == 0.0
+    far = opm.p3m_short(pos, np.array([2.0, 3.0]), pos, alpha, 0.009, eps=eps, self_index=np.array([0, 1]))
+    assert np.abs(far).max() == 0.0
+
+
+def test_p3m_pair_term_is_the_ewald_real_space_part():
+    """With softening and r_cut inside the nearest image, the pair term is
+    the real-space part of the Ewald sum (no k vectors) wherever the
+    softening correction beyond r_cut is negligible."""
+    from oracle import pm3d as opm
+    rng = np.random.default_rng(4)
+    src = rng.uniform(0, 1, (300, 3))
+    m = rng.uniform(0.5, 1.5, 300)
+    tgt = src[:5]
+    alpha, r_cut, eps = 8.0, 0.33, 1e-6
+    real = opm.ewald_accel(src, m, tgt, alpha=alpha, r_cut=r_cut, h_max=0, eps=eps, self_index=np.arange(5))
+    pair = opm.p3m_short(src, m, tgt, alpha, r_cut, eps=eps, self_index=np.arange(5))
+    assert np.allclose(pair, real, rtol=1e-9, atol=1e-9 * np.abs(real).max())
