@@ -24,10 +24,11 @@
 //             higher index (13 or so of the 26, periodic). The sources are
 //             staged through the warp's shared memory in chunks of 32,
 //             relative to the item's cell corner, so that f32 differences
-//             keep the positions' resolution; lane l meets source (l + k)
-//             mod 32 at step k and the sources' sums rotate through the lanes
-//             with them, so that both sides accumulate in registers. Both go
-//             to an f32 accumulator per particle with atomics.
+//             keep the positions' resolution; lane l meets sources (l + k)
+//             and (l + k + 16) mod 32 at step k, in packed f32x2 arithmetic,
+//             and the sources' sums rotate through the lanes with them, so
+//             that both sides accumulate in registers. Both go to an f32
+//             accumulator per particle with atomics.
 //   finish  : acceleration = mesh force (already in a) + G x accumulator, in
 //             f64, through the KDK epilogue of the force passes.
 
@@ -108,6 +109,46 @@ struct PPArgs {
     long long n;
 };
 
+// ---- packed f32x2 pair arithmetic: two sources per lane and step
+typedef unsigned long long f2x;                     // two packed f32
+
+__device__ __forceinline__ f2x pk2(float lo, float hi) {
+    f2x r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(f2x v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b) {
+    f2x d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x mul2(f2x a, f2x b) {
+    f2x d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2x fma2(f2x a, f2x b, f2x c) {
+    f2x d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ f2x shfl2(f2x v, int from) {
+    return __shfl_sync(0xffffffffu, v, from);
+}
+
 // h(r) of a pair (a_i += m_j h d, a_j -= m_i h d, d = x_j - x_i), for
 // 0 < r < r_cut: (g(x) + (1 + u)^{-3/2} - 1) / r^3 with u = eps^2 / r^2,
 // evaluated as (g - 1) / r^3 + (r^2 + eps^2)^{-3/2} (its rounding is about
@@ -116,62 +157,79 @@ struct PPArgs {
 // Stegun 7.1.26, |error| <= 1.5e-7), so g shares its Gaussian with the
 // second term 2 x e^{-x^2} / sqrt(pi). No branches: out of range (and for
 // coincident particles, where the arithmetic is not finite) the caller
-// selects 0.
-__device__ __forceinline__ float pp_h(float r2, float alpha, float eps2) {
-    const float rinv = rsqrtf(r2);
-    const float inv_r3 = rinv * rinv * rinv;
-    const float x = alpha * (r2 * rinv);
-    const float ex = __expf(-x * x);
-    const float t = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
-    const float poly =
-        t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f))));
-    const float g = ex * fmaf(1.12837917f, x, poly);
-    const float si = rsqrtf(r2 + eps2);
-    return fmaf(g - 1.0f, inv_r3, si * si * si);
+// selects 0. Two pairs at a time in packed f32x2 arithmetic; the reciprocal
+// square roots, the exponential and the reciprocal are f32 MUFU operations.
+__device__ __forceinline__ f2x pp_h2(f2x R2, const f2x* K) {
+    // K: alpha, -log2(e), p, 1, a1..a5, 2/sqrt(pi), eps^2, -1 (each in both halves)
+    float r0, r1;
+    upk2(R2, r0, r1);
+    const f2x RI = pk2(sss_rsqrt_approx_f32(r0), sss_rsqrt_approx_f32(r1));
+    const f2x INV3 = mul2(mul2(RI, RI), RI);
+    const f2x X = mul2(K[0], mul2(R2, RI));
+    float v0, v1;
+    upk2(mul2(mul2(X, X), K[1]), v0, v1);
+    const f2x EX = pk2(ex2_approx(v0), ex2_approx(v1));
+    float d0, d1;
+    upk2(fma2(K[2], X, K[3]), d0, d1);
+    const f2x T = pk2(rcp_approx(d0), rcp_approx(d1));
+    const f2x POLY = mul2(T, fma2(T, fma2(T, fma2(T, fma2(T, K[8], K[7]), K[6]), K[5]), K[4]));
+    const f2x G = mul2(EX, fma2(K[9], X, POLY));
+    float s0, s1;
+    upk2(add2(R2, K[10]), s0, s1);
+    const f2x SI = pk2(sss_rsqrt_approx_f32(s0), sss_rsqrt_approx_f32(s1));
+    return fma2(add2(G, K[11]), INV3, mul2(mul2(SI, SI), SI));
 }
 
-// One chunk of sources (stage[0 .. 32), masses in w; invalid entries have
-// w = 0 and the lanes without a target tm = 0) against the lanes' targets,
-// steps k0 .. k1 - 1 (lane l meets source (l + k) mod 32); `half` limits
-// step 16 to lanes 0 .. 15 (the item's own chunk, whose pairs (l, l + 16)
-// and (l + 16, l) coincide). The sources' sums end on their own lanes and go
-// to the accumulator (positions src0 .. src0 + m - 1).
-__device__ __forceinline__ void pp_chunk(const float4* stage, int lane, int k0, int k1, bool half, float tx,
-                                         float ty, float tz, float tm, const PPArgs& q, float& ax, float& ay,
-                                         float& az, long long src0, int m) {
-    float bx = 0.0f, by = 0.0f, bz = 0.0f;                         // the sum of source (lane + k) mod 32
+// One chunk of sources against the lanes' targets, two sources per step:
+// offsets (a, a + da) for steps a = a0 .. a1 - 1 (source (lane + offset) mod
+// 32); `own` masks offset 16 on lanes 16 .. 31 (the item's own chunk, whose
+// pairs (l, l + 16) and (l + 16, l) coincide). Both sources' sums rotate
+// through the lanes and end on their own lanes, then go to the accumulator.
+__device__ __forceinline__ void pp_chunk2(const float4* stage, int lane, int a0, int a1, int da, bool own,
+                                          f2x NTX, f2x NTY, f2x NTZ, f2x NTM, const f2x* K,
+                                          const PPArgs& q, f2x& AX, f2x& AY, f2x& AZ, long long src0, int m) {
+    f2x BX = 0ull, BY = 0ull, BZ = 0ull;             // sums of sources (lane + a) and (lane + a + da)
 #pragma unroll 2
-    for (int k = k0; k < k1; ++k) {
-        const float4 sj = stage[(lane + k) & 31];
-        const float dx = sj.x - tx, dy = sj.y - ty, dz = sj.z - tz;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const bool in = r2 < q.rc2 && r2 > 0.0f && !(half && k == 16 && lane >= 16);
-        if (__any_sync(0xffffffffu, in)) {                          // (warp-uniform: no divergent pair arithmetic)
-            const float h0 = pp_h(r2, q.alpha, q.eps2);
-            const float h = in ? h0 : 0.0f;
-            const float hj = h * sj.w, hi = h * tm;
-            ax = fmaf(hj, dx, ax);
-            ay = fmaf(hj, dy, ay);
-            az = fmaf(hj, dz, az);
-            bx = fmaf(-hi, dx, bx);
-            by = fmaf(-hi, dy, by);
-            bz = fmaf(-hi, dz, bz);
+    for (int a = a0; a < a1; ++a) {
+        const float4 sa = stage[(lane + a) & 31], sb = stage[(lane + a + da) & 31];
+        const f2x DX = add2(pk2(sa.x, sb.x), NTX), DY = add2(pk2(sa.y, sb.y), NTY), DZ = add2(pk2(sa.z, sb.z), NTZ);
+        const f2x R2 = fma2(DX, DX, fma2(DY, DY, mul2(DZ, DZ)));
+        float r0, r1;
+        upk2(R2, r0, r1);
+        const bool in0 = r0 < q.rc2 && r0 > 0.0f;
+        const bool in1 = r1 < q.rc2 && r1 > 0.0f && !(own && a + da == 16 && lane >= 16);
+        if (__any_sync(0xffffffffu, in0 || in1)) {                  // (warp-uniform)
+            float h0, h1;
+            upk2(pp_h2(R2, K), h0, h1);
+            const f2x H = pk2(in0 ? h0 : 0.0f, in1 ? h1 : 0.0f);
+            const f2x HJ = mul2(H, pk2(sa.w, sb.w)), HI = mul2(H, NTM);
+            AX = fma2(HJ, DX, AX);
+            AY = fma2(HJ, DY, AY);
+            AZ = fma2(HJ, DZ, AZ);
+            BX = fma2(HI, DX, BX);
+            BY = fma2(HI, DY, BY);
+            BZ = fma2(HI, DZ, BZ);
         }
-        if (k + 1 < k1) {                                          // take source (lane + k + 1)'s sum from the next lane
+        if (a + 1 < a1) {                                          // take the next lane's sums (sources + 1)
             const int from = (lane + 1) & 31;
-            bx = __shfl_sync(0xffffffffu, bx, from);
-            by = __shfl_sync(0xffffffffu, by, from);
-            bz = __shfl_sync(0xffffffffu, bz, from);
+            BX = shfl2(BX, from);
+            BY = shfl2(BY, from);
+            BZ = shfl2(BZ, from);
         }
     }
-    const int from = (lane - (k1 - 1)) & 31;                       // lane l now holds source (l + k1 - 1)'s sum
-    bx = __shfl_sync(0xffffffffu, bx, from);
-    by = __shfl_sync(0xffffffffu, by, from);
-    bz = __shfl_sync(0xffffffffu, bz, from);
+    // lane l holds sources (l + a1 - 1) and (l + a1 - 1 + da): deliver both to their lanes
+    const int fa = (lane - (a1 - 1)) & 31, fb = (lane - (a1 - 1 + da)) & 31;
+    float xa, xb, ya, yb, za, zb, t0, t1;
+    upk2(shfl2(BX, fa), xa, t0);
+    upk2(shfl2(BX, fb), t1, xb);
+    upk2(shfl2(BY, fa), ya, t0);
+    upk2(shfl2(BY, fb), t1, yb);
+    upk2(shfl2(BZ, fa), za, t0);
+    upk2(shfl2(BZ, fb), t1, zb);
     if (lane < m) {
-        atomicAdd(q.acc + src0 + lane, bx);
-        atomicAdd(q.acc + q.n + src0 + lane, by);
-        atomicAdd(q.acc + 2 * q.n + src0 + lane, bz);
+        atomicAdd(q.acc + src0 + lane, xa + xb);
+        atomicAdd(q.acc + q.n + src0 + lane, ya + yb);
+        atomicAdd(q.acc + 2 * q.n + src0 + lane, za + zb);
     }
 }
 
@@ -181,6 +239,11 @@ __global__ void __launch_bounds__(PP_WARPS * 32) k_pp_pairs(const PPArgs q) {
     const int M = q.M;
     const unsigned total = *q.n_items;
     float4* stage = sh[w];
+    const f2x K[12] = {pk2(q.alpha, q.alpha), pk2(-1.44269504f, -1.44269504f), pk2(0.3275911f, 0.3275911f),
+                       pk2(1.0f, 1.0f), pk2(0.254829592f, 0.254829592f), pk2(-0.284496736f, -0.284496736f),
+                       pk2(1.421413741f, 1.421413741f), pk2(-1.453152027f, -1.453152027f),
+                       pk2(1.061405429f, 1.061405429f), pk2(1.12837917f, 1.12837917f), pk2(q.eps2, q.eps2),
+                       pk2(-1.0f, -1.0f)};
     for (;;) {
         unsigned it = 0;
         if (lane == 0) it = atomicAdd(q.next, 1u);
@@ -200,12 +263,13 @@ __global__ void __launch_bounds__(PP_WARPS * 32) k_pp_pairs(const PPArgs q) {
             tz = (float)(p.z - oz);
             tm = (float)p.w;
         }
-        float ax = 0.0f, ay = 0.0f, az = 0.0f;
-        // the item's own particles with each other (steps 1 .. 16)
+        const f2x NTX = pk2(-tx, -tx), NTY = pk2(-ty, -ty), NTZ = pk2(-tz, -tz), NTM = pk2(-tm, -tm);
+        f2x AX = 0ull, AY = 0ull, AZ = 0ull;
+        // the item's own particles with each other (offsets 1 .. 16 as (j, j + 8), j = 1 .. 8)
         __syncwarp();
         stage[lane] = make_float4(tx, ty, tz, tm);
         __syncwarp();
-        pp_chunk(stage, lane, 1, 17, true, tx, ty, tz, tm, q, ax, ay, az, t0, min(32, cl - t0));
+        pp_chunk2(stage, lane, 1, 9, 8, true, NTX, NTY, NTZ, NTM, K, q, AX, AY, AZ, t0, min(32, cl - t0));
         // the later particles of the cell, then the neighbouring cells of higher index
         for (int nb = -1; nb < 27; ++nb) {
             int s0, s1;
@@ -234,13 +298,17 @@ __global__ void __launch_bounds__(PP_WARPS * 32) k_pp_pairs(const PPArgs q) {
                 }
                 stage[lane] = v;
                 __syncwarp();
-                pp_chunk(stage, lane, 0, 32, false, tx, ty, tz, tm, q, ax, ay, az, j0, min(32, s1 - j0));
+                pp_chunk2(stage, lane, 0, 16, 16, false, NTX, NTY, NTZ, NTM, K, q, AX, AY, AZ, j0, min(32, s1 - j0));
             }
         }
         if (act) {
-            atomicAdd(q.acc + t, ax);
-            atomicAdd(q.acc + q.n + t, ay);
-            atomicAdd(q.acc + 2 * q.n + t, az);
+            float x0, x1, y0, y1, z0, z1;
+            upk2(AX, x0, x1);
+            upk2(AY, y0, y1);
+            upk2(AZ, z0, z1);
+            atomicAdd(q.acc + t, x0 + x1);
+            atomicAdd(q.acc + q.n + t, y0 + y1);
+            atomicAdd(q.acc + 2 * q.n + t, z0 + z1);
         }
     }
 }
