@@ -208,6 +208,11 @@ int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, const float* vx
                    const float* rr, const unsigned char* is_ast, const unsigned char* vis, int64_t n,
                    double dt_y, double h, double halo, float lo, float hi, int* out_hits,
                    int64_t capacity, int64_t* n_hits, int64_t* n_cand, void* stream);
+/* sort k hits of sss_broadphase in place into the reference's output order,
+ * (offset, a, b) ascending: it concatenates one part per neighbour offset,
+ * each ascending in (a, b) (film_producer.py:255-290); n = the bodies of the
+ * call (a, b < n < 2^30) */
+int sss_broadphase_order(sss_ctx* ctx, int* hits, int64_t k, int64_t n, void* stream);
 
 /* ------------------------------------------------------ particle mesh, 2-D
  *

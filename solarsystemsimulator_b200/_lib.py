@@ -96,6 +96,7 @@ SIGNATURES = {
     "sss_broadphase": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_float, ctypes.c_float, _dp,
                                       _c_i64, ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64), _vp]),
+    "sss_broadphase_order": (ctypes.c_int, [_vp, _dp, _c_i64, _c_i64, _vp]),
     "sss_pm2d_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     "sss_pm2d_destroy": (None, [_vp]),
     "sss_pm2d_bbox": (ctypes.c_int, [_vp, _dp, _dp, _c_i64, _dp, _vp]),

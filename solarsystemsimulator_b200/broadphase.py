@@ -78,10 +78,12 @@ def bounce_hits(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, rr, is_
                                     device=device)
     if k == 0:
         return None, nc
-    h_ = buf.cpu().numpy().astype(np.int64)
-    order = np.lexsort((h_[:, 2], h_[:, 1], h_[:, 0]))      # (offset, a, b): the reference's order
-    h_ = h_[order]
-    return (h_[:, 1].copy(), h_[:, 2].copy()), nc
+    ctx = _lib.context(device)
+    with torch.cuda.device(device):                               # (offset, a, b): the reference's order
+        ctx.check(ctx.lib.sss_broadphase_order(ctx.ptr, buf.data_ptr(), k, len(gx),
+                                               ctypes.c_void_p(_lib.stream_handle(device))))
+    h_ = buf.cpu().numpy()
+    return (h_[:, 1].astype(np.int64), h_[:, 2].astype(np.int64)), nc
 
 
 class Erkennungskarte:

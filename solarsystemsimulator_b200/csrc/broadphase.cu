@@ -23,8 +23,8 @@
 // 32 run bodies x up to 992 partners. A warp skips each aligned chunk of 32
 // partners whose bounding box is provably out of reach of the run bodies' box
 // and streams the others as broadcast loads from records stored in sorted
-// order. Hits are appended; the host sorts them by (offset, a, b), which is
-// the reference's output order.
+// order. Hits are appended; sss_broadphase_order sorts them by (offset, a, b)
+// on the device, which is the reference's output order.
 
 #include "devscan.cuh"
 
@@ -591,6 +591,23 @@ __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
     }
 }
 
+// Hit order of the reference's output, (offset, a, b) ascending, as one
+// 64-bit key: offset (3 bits) above a and b (B bits each, a, b < 2^B).
+__global__ void k_hit_keys(const Hit* __restrict__ h, long long k, int B, unsigned long long* __restrict__ keys,
+                           unsigned* __restrict__ vals) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const Hit v = h[i];
+    keys[i] = ((unsigned long long)(unsigned)v.o << (2 * B)) | ((unsigned long long)v.a << B) | v.b;
+    vals[i] = (unsigned)i;
+}
+
+__global__ void k_hit_gather(const Hit* __restrict__ in, const unsigned* __restrict__ order, long long k,
+                             Hit* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) out[i] = in[order[i]];
+}
+
 }  // namespace
 
 extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, const float* vx, const float* vy,
@@ -737,5 +754,38 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     *n_hits = (int64_t)nh;
     if ((long long)nh > capacity)
         return sss_set_err(ctx, SSS_ERR_CAPACITY, "hit buffer holds %lld, %llu hits found", (long long)capacity, nh);
+    return SSS_OK;
+}
+
+extern "C" int sss_broadphase_order(sss_ctx* ctx, int* hits, int64_t k, int64_t n, void* stream) {
+    if (!ctx) return SSS_ERR_ARG;
+    if (k < 0 || n < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
+    if (k > 0 && !hits) return sss_set_err(ctx, SSS_ERR_ARG, "NULL hits");
+    if (n >= ((int64_t)1 << 30)) return sss_set_err(ctx, SSS_ERR_ARG, "too many bodies for the packed hit key");
+    if (k < 2) return SSS_OK;
+    SSS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    int B = 1;
+    while (((int64_t)1 << B) < n) ++B;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~(size_t)255; return o; };
+    const size_t o_k0 = take(8 * k), o_k1 = take(8 * k), o_v0 = take(4 * k), o_v1 = take(4 * k);
+    const size_t o_tmp = take(12 * k), o_rs = take(8 * sss_dev::radix_scratch(k));
+    void* scr = nullptr;
+    int rc = sss_scratch(ctx, off, &scr);
+    if (rc) return rc;
+    char* S = (char*)scr;
+    unsigned long long* k0 = (unsigned long long*)(S + o_k0);
+    unsigned long long* k1 = (unsigned long long*)(S + o_k1);
+    unsigned* v0 = (unsigned*)(S + o_v0);
+    unsigned* v1 = (unsigned*)(S + o_v1);
+    Hit* tmp = (Hit*)(S + o_tmp);
+    const unsigned nb = (unsigned)((k + 255) / 256);
+    k_hit_keys<<<nb, 256, 0, s>>>((const Hit*)hits, k, B, k0, v0);
+    SSS_LAUNCH_CHECK(ctx, "k_hit_keys");
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, k, (long long*)(S + o_rs), s, 3 + 2 * B));
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tmp, hits, 12 * (size_t)k, cudaMemcpyDeviceToDevice, s));
+    k_hit_gather<<<nb, 256, 0, s>>>(tmp, v0, k, (Hit*)hits);
+    SSS_LAUNCH_CHECK(ctx, "k_hit_gather");
     return SSS_OK;
 }
