@@ -173,3 +173,30 @@ def test_non_finite_and_far_bodies():
     ref, cref = obp.hits(x, y, vx, vy, rr, dt, h, halo)
     res, cand = bp.bounce_hits(x, y, vx, vy, dt, h, halo, rr=rr)
     assert cand == cref and _same(res, ref)
+
+
+@pytest.mark.parametrize("k,n", [(1, 10), (5_000, 200_000), (70_000, 3_000), (20_000, (1 << 30) - 1)])
+def test_hit_order_on_the_device(k, n):
+    """sss_broadphase_order sorts (offset, a, b) triples exactly as
+    np.lexsort does, duplicates and the largest body index included."""
+    import ctypes
+    import torch
+    from solarsystemsimulator_b200 import _lib
+    rng = np.random.default_rng(k)
+    h = np.stack([rng.integers(0, 5, k), rng.integers(0, n, k), rng.integers(0, n, k)], 1).astype(np.int32)
+    h[: k // 10] = h[0]                                   # repeated triples
+    h[-1, 1:] = n - 1
+    d = torch.as_tensor(h).cuda()
+    ctx = _lib.context(0)
+    ctx.check(ctx.lib.sss_broadphase_order(ctx.ptr, d.data_ptr(), k, n, ctypes.c_void_p(_lib.stream_handle(0))))
+    want = h[np.lexsort((h[:, 2], h[:, 1], h[:, 0]))]
+    assert np.array_equal(d.cpu().numpy(), want)
+
+
+def test_hit_order_rejects_bad_sizes():
+    import ctypes
+    from solarsystemsimulator_b200 import _lib
+    ctx = _lib.context(0)
+    assert ctx.lib.sss_broadphase_order(ctx.ptr, None, -1, 10, None) == _lib.SSS_ERR_ARG
+    assert ctx.lib.sss_broadphase_order(ctx.ptr, None, 5, 10, None) == _lib.SSS_ERR_ARG
+    assert ctx.lib.sss_broadphase_order(ctx.ptr, None, 0, 1 << 30, None) == _lib.SSS_ERR_ARG
