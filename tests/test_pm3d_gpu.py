@@ -256,3 +256,31 @@ def test_learned_run_gains_and_judge_reverts(mods):
     # network would move the particles by 5e-7 .. 1e-5 over these 5 steps
     d = (x_after - st["buf"][0:3]).abs()
     assert float(torch.minimum(d, 1.0 - d).max()) <= 1e-9
+
+
+def test_learned_run_on_the_p3m_force(mods):
+    """The learned model over the mesh + P3M pair term (32^3 particles on
+    64^3, r_split 1 cell, r_cut 3 / alpha): the judge accepts exactly the
+    checks where the corrected force is no worse than the method's, and on
+    the evolved state the method's force is far better than the mesh's."""
+    _lib, pm3d, _, _ = mods
+    from solarsystemsimulator_b200.workloads import periodic_structure
+    w = periodic_structure(n_side=32, mesh_n=64, seed=21, fcc=False)
+    sim = pm3d.NBodyPMLearned(0, mesh_n=64, softening=w["softening"], check_every=10, samples=4096, iters=200,
+                              batch=1024, lr=2e-3, seed=1, short_range=True, r_split_cells=1.0, x_cut=3.0)
+    st = sim.load_state(w["pos"], w["vel"], w["mass"])
+    recs = sim.run(st, 2e-3, 30)
+    assert len(recs) == 4
+    judged = [r for r in recs if r.err_corr is not None]
+    assert judged and all((r.err_corr <= r.err_mesh) == bool(r.accepted) for r in judged)
+    assert all(r.reverted == (not r.accepted) for r in judged)
+    plain = pm3d.PMPeriodic3D(64, 1.0, 1.0, 0, 2, 0.6)
+    pos, vel = sim.pm.export_f64(st)
+    stp = plain.load_state(pos, vel, w["mass"])
+    idx = torch.arange(0, st["n"], 7, device=st["buf"].device)
+    ref = sim.ewald.accel(stp["parts"], stp["buf"][0:3, idx].contiguous(), idx)
+    plain.forces(stp)
+    e_mesh = pm3d.median_rel_err(stp["buf"][6:9, idx], ref)
+    sim.pm.method_forces(st)
+    e_p3m = pm3d.median_rel_err(st["buf"][6:9, idx], ref)
+    assert e_p3m < 0.2 * e_mesh, (e_p3m, e_mesh)
