@@ -160,10 +160,10 @@ __device__ __forceinline__ bool ccd_f64(const Body& A, const Body& B, double dt)
 __global__ void k_sorted_records(const float* __restrict__ x, const float* __restrict__ y,
                                  const float* __restrict__ vx, const float* __restrict__ vy,
                                  const float* __restrict__ rr, const unsigned* __restrict__ ai,
-                                 const unsigned* __restrict__ order, long long na, float4* __restrict__ rec,
-                                 uint2* __restrict__ rec2) {
+                                 const unsigned* __restrict__ order, const long long* __restrict__ d_na,
+                                 float4* __restrict__ rec, uint2* __restrict__ rec2) {
     const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= na) return;
+    if (pos >= *d_na) return;
     const unsigned b = ai[order[pos]];
     rec[pos] = make_float4(x[b], y[b], vx[b], vy[b]);
     rec2[pos] = make_uint2(__float_as_uint(rr[b]), b);
@@ -209,10 +209,16 @@ __device__ __forceinline__ unsigned spread2(unsigned v) {
 }
 
 __global__ void k_sub_keys(const float* __restrict__ x, const float* __restrict__ y, const unsigned* __restrict__ ai,
-                           const long long* __restrict__ cx, const long long* __restrict__ cy, long long na,
-                           double h, unsigned long long* __restrict__ sk, unsigned* __restrict__ sv) {
+                           const long long* __restrict__ cx, const long long* __restrict__ cy,
+                           const long long* __restrict__ d_na, long long n, double h,
+                           unsigned long long* __restrict__ sk, unsigned* __restrict__ sv) {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= na) return;
+    if (r >= n) return;
+    if (r >= *d_na) {                                              // padding up to n: sorts after every row
+        sk[r] = 0xFFFull;
+        sv[r] = (unsigned)r;
+        return;
+    }
     const unsigned b = ai[r];
     const double fx = __ddiv_rn((double)x[b], h) - (double)cx[r];
     const double fy = __ddiv_rn((double)y[b], h) - (double)cy[r];
@@ -223,9 +229,9 @@ __global__ void k_sub_keys(const float* __restrict__ x, const float* __restrict_
 }
 
 __global__ void k_gather_keys(const unsigned long long* __restrict__ rowkey, const unsigned* __restrict__ order,
-                              long long na, unsigned long long* __restrict__ keys) {
+                              const long long* __restrict__ d_na, long long n, unsigned long long* __restrict__ keys) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < na) keys[p] = rowkey[order[p]];
+    if (p < n) keys[p] = p < *d_na ? rowkey[order[p]] : ~0ull;   // padding sorts after every row (stable)
 }
 
 // Bounding box of every aligned chunk of 32 sorted records: x, y, vx, vy
@@ -238,10 +244,11 @@ struct ChunkBox {
 
 __device__ __forceinline__ float nan_max(float a, float b) { return (b > a || b != b) ? b : a; }
 
-__global__ void k_chunk_boxes(const float4* __restrict__ rec, const uint2* __restrict__ rec2, long long na,
-                              ChunkBox* __restrict__ boxes) {
+__global__ void k_chunk_boxes(const float4* __restrict__ rec, const uint2* __restrict__ rec2,
+                              const long long* __restrict__ d_na, ChunkBox* __restrict__ boxes) {
     const int lane = threadIdx.x & 31;
     const long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long na = *d_na;
     const long long nc = (na + 31) / 32;
     if (c >= nc) return;
     const long long j = c * 32 + lane;
@@ -281,9 +288,14 @@ __global__ void k_chunk_boxes(const float4* __restrict__ rec, const uint2* __res
 // set, is the reference's; the order of the hits is restored by sorting them
 // by (offset, a, b).
 __global__ void k_run_flags(const long long* __restrict__ cx, const long long* __restrict__ cy,
-                            const unsigned* __restrict__ order, long long na, long long* __restrict__ flags) {
+                            const unsigned* __restrict__ order, const long long* __restrict__ d_na, long long n,
+                            long long* __restrict__ flags) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= na) return;
+    if (p >= n) return;
+    if (p >= *d_na) {                                              // padding: no runs
+        flags[p] = 0;
+        return;
+    }
     bool start = p == 0;
     if (!start) {
         const unsigned r = order[p], q = order[p - 1];
@@ -292,26 +304,31 @@ __global__ void k_run_flags(const long long* __restrict__ cx, const long long* _
     flags[p] = start ? 1 : 0;
 }
 
-__global__ void k_run_starts(const long long* __restrict__ flags, const long long* __restrict__ pos, long long na,
-                             long long* __restrict__ run_start) {
+__global__ void k_run_starts(const long long* __restrict__ flags, const long long* __restrict__ pos,
+                             const long long* __restrict__ d_na, long long* __restrict__ run_start) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < na && flags[p]) run_start[pos[p]] = p;
+    if (p < *d_na && flags[p]) run_start[pos[p]] = p;
 }
 
 constexpr int TILE_B = 992;       // partners per tile (at most 32 aligned chunks of 32); 32 run bodies per tile
 
 // Item t = o * n_run + q: run q against the partner range of offset o (its
 // first position and length), its tile count, and the candidates summed per
-// block into n_cand.
+// block into n_cand. Launched over an upper bound of items; those past
+// 5 n_run get no tiles.
 __global__ void __launch_bounds__(256) k_items(const long long* __restrict__ cx, const long long* __restrict__ cy,
                                                const unsigned* __restrict__ order,
-                                               const unsigned long long* __restrict__ ks, long long na,
-                                               const long long* __restrict__ run_start, long long n_run,
+                                               const unsigned long long* __restrict__ ks,
+                                               const long long* __restrict__ d_na,
+                                               const long long* __restrict__ run_start,
+                                               const long long* __restrict__ d_nrun, long long max_items,
                                                long long* __restrict__ item_b0, long long* __restrict__ item_nb,
                                                long long* __restrict__ tiles, unsigned long long* __restrict__ n_cand) {
     __shared__ unsigned long long bs[8];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long na = *d_na, n_run = *d_nrun;
     unsigned long long cand = 0;
+    if (t < max_items && t >= 5 * n_run) tiles[t] = 0;
     if (t < 5 * n_run) {
         const int o = (int)(t / n_run);
         const long long q = t - (long long)o * n_run;
@@ -345,7 +362,9 @@ struct TileArgs {
     const long long* tile_start; // [5 n_run + 1] exclusive prefix of the tile counts
     const unsigned long long* ks; // sorted keys
     const ChunkBox* boxes;       // [ceil(na / 32)] boxes of the aligned chunks of 32 records
-    long long na, n_run, n_tiles;
+    const long long* na;         // alive bodies, runs and tiles (device counts)
+    const long long* n_run;
+    const long long* n_tiles;
     TestParams tp;
 };
 
@@ -505,10 +524,11 @@ __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
     PairQueue q{q_j[wib], q_l[wib], 0};
     const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long per = (a.n_tiles + warps - 1) / warps;
-    const long long tb = warp0 * per, te = min(tb + per, a.n_tiles);
+    const long long na = *a.na, n_run = *a.n_run, n_tiles = *a.n_tiles;
+    const long long per = (n_tiles + warps - 1) / warps;
+    const long long tb = warp0 * per, te = min(tb + per, n_tiles);
     if (tb >= te) return;
-    const long long n_items = 5 * a.n_run;
+    const long long n_items = 5 * n_run;
     long long t0 = 0;
     if (lane == 0) t0 = find_segment(a.tile_start, n_items, tb);
     long long t = __shfl_sync(0xffffffffu, t0, 0);
@@ -520,9 +540,9 @@ __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
             t_start = t_end;
             t_end = a.tile_start[t + 1];
         }
-        const int o = (int)(t / a.n_run);
-        const long long qr = t - (long long)o * a.n_run;
-        const long long p0 = a.run_start[qr], p1 = qr + 1 < a.n_run ? a.run_start[qr + 1] : a.na;
+        const int o = (int)(t / n_run);
+        const long long qr = t - (long long)o * n_run;
+        const long long p0 = a.run_start[qr], p1 = qr + 1 < n_run ? a.run_start[qr + 1] : na;
         const long long b0 = a.item_b0[t], nb = a.item_nb[t];
         const long long n_bt = (nb + TILE_B - 1) / TILE_B;
         const long long local = tid - t_start;
@@ -641,7 +661,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_v = take(nn);                  // v0 + v1 (unsigned, 2 per long long)
     const size_t o_ai = take((nn + 1) / 2 + 1);
     const size_t o_flag = take(nn), o_pos = take(nn), o_run = take(nn);
-    const size_t o_ib0 = take(5 * nn), o_inb = take(5 * nn), o_tst = take(5 * nn + 1);
+    const size_t o_ib0 = take(5 * nn), o_inb = take(5 * nn), o_tst = take(5 * nn + 3);  // + run and tile counts
     const size_t o_rec = take(2 * nn), o_rec2 = take(nn);      // float4 and uint2 per alive body
     const size_t o_rowkey = take(nn);                          // cell key per alive row
     const size_t o_box = take((nn + 31) / 32 * (sizeof(ChunkBox) / 8));
@@ -672,59 +692,54 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     ChunkBox* boxes = (ChunkBox*)(S + o_box);
     unsigned long long* d_ncand = d_nh + 1;
 
+    // Every size after the alive count stays on the device: the launches are
+    // sized for n bodies (5 n items, a persistent tile grid) and read the
+    // counts there, so the call has one host readback, at the end.
     // 1) alive compaction (ascending body order) + cells + keys
     k_alive_count<<<(unsigned)tiles, BP_NT, 0, s>>>(is_ast, vis, x, nn, lo, hi_halo, counts);
     sss_dev::k_scan_sums<<<1, sss_dev::SCAN_NT, 0, s>>>(counts, tiles);
-    long long na = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&na, counts + tiles, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-    if (na < 2) return SSS_OK;
+    const long long* d_na = counts + tiles;
     k_alive_scatter<<<(unsigned)tiles, BP_NT, 0, s>>>(is_ast, vis, x, y, nn, lo, hi_halo, h, counts, ai, cx, cy,
                                                        rowkey, v0);
     SSS_LAUNCH_CHECK(ctx, "k_alive_scatter");
     // 2) sort by the position inside the cell, then stably by the cell key
-    //    (ascending signed order): key, then sub-cell, then body order
-    const unsigned nb_r = (unsigned)((na + 255) / 256);
-    k_sub_keys<<<nb_r, 256, 0, s>>>(x, y, ai, cx, cy, na, h, k0, v0);
+    //    (ascending signed order): key, then sub-cell, then body order; the
+    //    n - na padding entries sort last in both
+    const unsigned nb_n = (unsigned)((nn + 255) / 256);
+    k_sub_keys<<<nb_n, 256, 0, s>>>(x, y, ai, cx, cy, d_na, nn, h, k0, v0);
     SSS_LAUNCH_CHECK(ctx, "k_sub_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, na, scan_tmp, s, 12));
-    k_gather_keys<<<nb_r, 256, 0, s>>>(rowkey, v0, na, k0);
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s, 12));
+    k_gather_keys<<<nb_n, 256, 0, s>>>(rowkey, v0, d_na, nn, k0);
     SSS_LAUNCH_CHECK(ctx, "k_gather_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, na, scan_tmp, s));
-    k_sorted_records<<<nb_r, 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, na, rec, rec2);
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s));
+    k_sorted_records<<<nb_n, 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, d_na, rec, rec2);
     SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
-    const long long n_chunks = (na + 31) / 32;
-    k_chunk_boxes<<<(unsigned)((n_chunks * 32 + 255) / 256), 256, 0, s>>>(rec, rec2, na, boxes);
+    const long long n_chunks = (nn + 31) / 32;
+    k_chunk_boxes<<<(unsigned)((n_chunks * 32 + 255) / 256), 256, 0, s>>>(rec, rec2, d_na, boxes);
     SSS_LAUNCH_CHECK(ctx, "k_chunk_boxes");
     // 3) cell runs of the sorted order
-    const unsigned nb_a = (unsigned)((na + 255) / 256);
-    k_run_flags<<<nb_a, 256, 0, s>>>(cx, cy, v0, na, flags);
+    k_run_flags<<<nb_n, 256, 0, s>>>(cx, cy, v0, d_na, nn, flags);
     SSS_LAUNCH_CHECK(ctx, "k_run_flags");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, na, scan_tmp, s));
-    k_run_starts<<<nb_a, 256, 0, s>>>(flags, pos, na, run_start);
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, nn, scan_tmp, s));
+    // the run count: the scan's total, kept after the items' tile starts
+    const long long ntiles_n = (nn + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    long long* d_nrun = tile_st + 5 * nn + 1;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(d_nrun, scan_tmp + ntiles_n, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+    k_run_starts<<<nb_n, 256, 0, s>>>(flags, pos, d_na, run_start);
     SSS_LAUNCH_CHECK(ctx, "k_run_starts");
-    const long long atiles = (na + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
-    long long n_run = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&n_run, scan_tmp + atiles, sizeof(long long), cudaMemcpyDeviceToHost, s));
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(d_nh, 0, 2 * sizeof(unsigned long long), s));
-    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     // 4) (run, offset) items: partner ranges, tiles, candidates
-    const long long n_items = 5 * n_run;
-    k_items<<<(unsigned)((n_items + 255) / 256), 256, 0, s>>>(cx, cy, v0, k0, na, run_start, n_run, item_b0,
-                                                               item_nb, tile_st, d_ncand);
+    const long long max_items = 5 * nn;
+    k_items<<<(unsigned)((max_items + 255) / 256), 256, 0, s>>>(cx, cy, v0, k0, d_na, run_start, d_nrun, max_items,
+                                                                item_b0, item_nb, tile_st, d_ncand);
     SSS_LAUNCH_CHECK(ctx, "k_items");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(tile_st, tile_st, n_items, scan_tmp, s));
-    const long long itiles = (n_items + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
-    long long n_tiles = 0;
-    unsigned long long total = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&n_tiles, scan_tmp + itiles, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tile_st + n_items, scan_tmp + itiles, sizeof(long long),
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(tile_st, tile_st, max_items, scan_tmp, s));
+    const long long itiles = (max_items + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    long long* d_ntiles = tile_st + 5 * nn + 2;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tile_st + max_items, scan_tmp + itiles, sizeof(long long),
                                       cudaMemcpyDeviceToDevice, s));
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&total, d_ncand, sizeof(total), cudaMemcpyDeviceToHost, s));
-    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-    *n_cand = (int64_t)total;
-    if (n_tiles == 0) return SSS_OK;
-    // 5) tiles: keep rule + tests
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ntiles, scan_tmp + itiles, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+    // 5) tiles: keep rule + tests (a persistent grid; warps split the tiles)
     TileArgs ta;
     ta.rec = rec;
     ta.rec2 = rec2;
@@ -734,26 +749,28 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     ta.tile_start = tile_st;
     ta.ks = k0;
     ta.boxes = boxes;
-    ta.na = na;
-    ta.n_run = n_run;
-    ta.n_tiles = n_tiles;
+    ta.na = d_na;
+    ta.n_run = d_nrun;
+    ta.n_tiles = d_ntiles;
     ta.tp.dtf = (float)dt_y;
     ta.tp.dt = dt_y;
     ta.tp.hi = hi;
     ta.tp.hits = (Hit*)out_hits;
     ta.tp.cap = capacity;
     ta.tp.n_hits = d_nh;
-    long long blocks = (n_tiles + BP_NT / 32 - 1) / (BP_NT / 32);
-    const long long max_blocks = (long long)ctx->num_sms * 32;
-    if (blocks > max_blocks) blocks = max_blocks;
-    k_tiles<<<(unsigned)blocks, BP_NT, 0, s>>>(ta);
+    k_tiles<<<(unsigned)(ctx->num_sms * 32), BP_NT, 0, s>>>(ta);
     SSS_LAUNCH_CHECK(ctx, "k_tiles");
-    unsigned long long nh = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&nh, d_nh, sizeof(nh), cudaMemcpyDeviceToHost, s));
+    unsigned long long res[2] = {0, 0};
+    long long na = 0;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(res, d_nh, sizeof(res), cudaMemcpyDeviceToHost, s));
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&na, d_na, sizeof(na), cudaMemcpyDeviceToHost, s));
     SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
-    *n_hits = (int64_t)nh;
-    if ((long long)nh > capacity)
-        return sss_set_err(ctx, SSS_ERR_CAPACITY, "hit buffer holds %lld, %llu hits found", (long long)capacity, nh);
+    if (na < 2) return SSS_OK;                   // fewer than two alive asteroids: no candidates, no hits
+    *n_cand = (int64_t)res[1];
+    *n_hits = (int64_t)res[0];
+    if ((long long)res[0] > capacity)
+        return sss_set_err(ctx, SSS_ERR_CAPACITY, "hit buffer holds %lld, %llu hits found", (long long)capacity,
+                           res[0]);
     return SSS_OK;
 }
 
