@@ -321,6 +321,12 @@ int sss_stream_sample(sss_ctx* ctx, int64_t n, const float* x, const float* y, c
                       int64_t budget, unsigned* sel, uint16_t* qx, uint16_t* qy, int64_t* n_sel, void* stream);
 int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const float* y, int log_zoom, float* out4,
                       void* stream);
+/* Log-zoom display coordinates of n bodies (replaces _anzeige_koords with
+ * log_zoom, server.py:99-111): q = p * log1p(r) / (log 33 * r), r = |p|, in
+ * f32 with the C library's rounding of hypot and log1p; 0 where r <= 1e-9.
+ * x, y, qx, qy are device arrays of n floats. Asynchronous. */
+int sss_stream_display(sss_ctx* ctx, int64_t n, const float* x, const float* y, float* qx, float* qy,
+                       void* stream);
 /* sss_stream_sample_batch: k samples of the same bodies at once, as build_frame
  * packs the samples of one frame (server.py:378-537): x[i], y[i] (host arrays of
  * k device pointers) and t_cut[i] (host) per sample, the other inputs shared;
@@ -496,14 +502,18 @@ int sss_batched_launch(sss_ctx* ctx, int dim, double* const* x, double* const* v
  * The first call on a device does a one-time set-up with that device
  * current (it resolves the array's device address with
  * cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call shares the array and finds the previous call's contents in it;
- * the call clears what must start at zero. Calls whose work overlaps on the
- * GPU (different streams, or devices sharing no order) race on the array:
- * order them on one stream.
+ * Every call on a device shares that device's copy of the array and finds
+ * the previous call's contents in it; the call clears what must start at
+ * zero. Calls whose work overlaps on the same GPU (different streams with no
+ * order between them) race on the array: order them on one stream. Calls on
+ * different devices use separate copies of the array and do not race.
  *
  * device: CUDA device of all pointers (made current). d_status: optional
- * device int that a timed-out bounded wait sets to SSS_ERR_TIMEOUT (NULL =
- * an internal word). errbuf/errbuf_len: optional host buffer for a message.
+ * device int that a timed-out bounded wait sets to SSS_ERR_TIMEOUT. With
+ * d_status NULL the timeout goes to an internal word that no caller can
+ * read: the call still returns SSS_OK and a timed-out call's accelerations
+ * may be incomplete without notice, so a caller that must detect timeouts
+ * passes a d_status. errbuf/errbuf_len: optional host buffer for a message.
  * No reference counterpart. */
 #define SSS_NOALLOC_SCRATCH_BYTES     (32u << 20)
 #define SSS_NOALLOC_MAX_MIXED_SOURCES 1044480

@@ -23,11 +23,105 @@ LOD_MASSEN_WOLKE_AB = 200
 LOD_MASSEN_ANTEIL = 0.5
 
 
+def _f32_bits(x):
+    return np.asarray(x, np.float32).view(np.int32)
+
+
+def _f32_of(bits):
+    return np.asarray(bits, np.int32).view(np.float32)
+
+
+_LN2_HI = _f32_of(0x3F317180)
+_LN2_LO = _f32_of(0x3717F7D1)
+_LOG1P_R = [_f32_of(b) for b in (0x3F2AAAAB, 0x3ECCCCCD, 0x3E924925, 0x3E638E29, 0x3E3A3325, 0x3E1CD04F,
+                                  0x3E178897)]
+
+
+def log1p_f32(x):
+    """log(1 + x) for f32 x >= 0, every operation rounded to f32, by the
+    published reduction method of fdlibm's log1pf (Sun Microsystems, 1993),
+    which is the f32 log1p of the C library (glibc up to 2.40) that NumPy
+    calls for float32 log1p where it dispatches no SIMD kernel:
+    1 + x = 2^k (1 + f) with sqrt(2)/2 <= 1 + f < sqrt(2) and a correction
+    c for the rounding of 1 + x; s = f / (2 + f);
+    log(1 + f) = f - (hfsq - s (hfsq + R(s^2))), hfsq = f^2 / 2, R a
+    degree-7 minimax polynomial; k ln 2 in two parts. Checked bit for bit
+    against the C library's log1pf on every f32 in [2^-31, 2^22)."""
+    F = np.float32
+    x = np.asarray(x, np.float32)
+    hx = _f32_bits(x)
+    out = np.full(x.shape, np.nan, np.float32)
+    tiny = (hx >= 0) & (hx < 0x31000000)                               # x < 2^-29
+    xt = x[tiny]
+    out[tiny] = np.where(hx[tiny] < 0x24800000, xt, xt - xt * xt * F(0.5))
+    near = (hx >= 0x31000000) & (hx < 0x3ED413D7)                      # 2^-29 <= x < 0.41422: k = 0
+    far = (hx >= 0x3ED413D7) & (hx < 0x7F800000)
+    big = hx >= 0x7F800000                                             # inf, nan
+    out[big] = x[big] + x[big]
+    xf, hf = x[far], hx[far]
+    small_u = hf < 0x5A000000
+    u = np.where(small_u, xf + F(1.0), xf).astype(np.float32)
+    hu = _f32_bits(u)
+    k = (hu >> 23) - 127
+    c = np.where(k > 0, F(1.0) - (u - xf), xf - (u - F(1.0))).astype(np.float32)
+    c = np.where(small_u, c / u, F(0.0)).astype(np.float32)
+    hu = hu & 0x007FFFFF
+    low = hu < 0x3504F7
+    u = np.where(low, _f32_of(hu | 0x3F800000), _f32_of(hu | 0x3F000000))
+    k = np.where(low, k, k + 1)
+    hu = np.where(low, hu, (0x00800000 - hu) >> 2)
+
+    def finish(f, k, c, hu):
+        # the k = 0 forms drop the correction c, also where k comes out 0 after the reduction
+        kf = k.astype(np.float32)
+        k0 = k == 0
+        hfsq = F(0.5) * f * f
+        res = np.empty(f.shape, np.float32)
+        e = (hu == 0) & (f == 0)
+        res[e] = np.where(k0[e], F(0.0), kf[e] * _LN2_HI + (c[e] + kf[e] * _LN2_LO))
+        t = (hu == 0) & (f != 0)                                       # |f| < 2^-20
+        ft = f[t]
+        R = hfsq[t] * (F(1.0) - F(0.66666666666666666) * ft)
+        res[t] = np.where(k0[t], ft - R, kf[t] * _LN2_HI - ((R - (kf[t] * _LN2_LO + c[t])) - ft))
+        g = hu != 0
+        fg, hq = f[g], hfsq[g]
+        s = fg / (F(2.0) + fg)
+        z = s * s
+        R = z * (_LOG1P_R[0] + z * (_LOG1P_R[1] + z * (_LOG1P_R[2] + z * (_LOG1P_R[3] + z * (
+            _LOG1P_R[4] + z * (_LOG1P_R[5] + z * _LOG1P_R[6]))))))
+        res[g] = np.where(k0[g], fg - (hq - s * (hq + R)),
+                          kf[g] * _LN2_HI - ((hq - (s * (hq + R) + (kf[g] * _LN2_LO + c[g]))) - fg))
+        return res
+
+    xn = x[near]
+    out[near] = finish(xn, np.zeros(xn.shape, np.int32), np.zeros(xn.shape, np.float32),
+                       np.ones(xn.shape, np.int32))
+    out[far] = finish((u - F(1.0)).astype(np.float32), k, c, hu)
+    return out
+
+
+def hypot_f32(x, y):
+    """f32 hypot correctly rounded: the squares of f32 values are exact in
+    f64, their sum is rounded once, the f64 square root once more, then the
+    result to f32 (what the C library's hypotf returns for finite input)."""
+    xd = np.asarray(x, np.float32).astype(np.float64)
+    yd = np.asarray(y, np.float32).astype(np.float64)
+    r = np.sqrt(xd * xd + yd * yd).astype(np.float32)
+    inf = np.isinf(xd) | np.isinf(yd)
+    return np.where(inf, np.float32(np.inf), r)
+
+
 def display_coords(x, y, log_zoom):
+    """_anzeige_koords (server.py:99-111) with NumPy's float32 hypot and
+    log1p taken as the C library computes them (log1p_f32, hypot_f32).
+    NumPy on a CPU with AVX512_SKX dispatches float32 log1p to a SIMD
+    kernel that differs from the C library in the last bit or two for
+    about 10 % of the inputs; the golden log-zoom frame is written with
+    that dispatch switched off (tests/golden/make_golden_frames.py)."""
     if not log_zoom:
         return x, y
-    r = np.hypot(x, y)
-    sk = np.where(r > 1e-9, np.log1p(r) / (FILM_LOG33 * np.maximum(r, 1e-30)), 0.0)
+    r = hypot_f32(x, y)
+    sk = np.where(r > 1e-9, log1p_f32(r) / (FILM_LOG33 * np.maximum(r, 1e-30)), 0.0)
     return x * sk, y * sk
 
 

@@ -130,6 +130,7 @@ SIGNATURES = {
                                                ctypes.POINTER(ctypes.c_double), ctypes.c_int, _c_i64, _dp, _dp, _dp,
                                                ctypes.POINTER(_c_i64), _vp]),
     "sss_stream_minmax": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), _vp]),
+    "sss_stream_display": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, _dp, _vp]),
     "sss_pm3_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),
     "sss_pm3_destroy": (None, [_vp]),
     "sss_pm3_meshes": (ctypes.c_int, [_vp, ctypes.POINTER(_dp), ctypes.POINTER(_dp)]),

@@ -1,8 +1,8 @@
 """Asteroid x asteroid collision broadphase on one B200.
 
 Drop-in for the detection layer of the reference's backend/film_producer.py
-(`Erkennungskarte`, `_zellschluessel`, `bounce_suche`, `_streifengrenzen`,
-`NACHBARN`, `CHUNK`). The pair search runs in libsss (`sss_broadphase`); the
+(`Erkennungskarte`, `_zellschluessel`, `bounce_suche`, `NACHBARN`, `CHUNK`).
+The pair search runs in libsss (`sss_broadphase`); the
 hit list is bit-exact against the reference's `_hits` on the same f32
 snapshot (same pairs, same (i, j) orientation, same order).
 
@@ -23,7 +23,6 @@ from . import _lib
 
 NACHBARN = ((0, 0), (1, 0), (0, 1), (1, 1), (1, -1))   # film_producer.py:155
 CHUNK = 4_000_000                                     # film_producer.py:163 (no chunking needed here)
-LAST_ALPHA = 0.35                                     # film_producer.py:410
 
 
 def _dev_f32(a, device) -> torch.Tensor:
@@ -127,75 +126,68 @@ def _zellschluessel(cx, cy):
         return cx * np.int64(73856093) ^ cy * np.int64(19349663)
 
 
-def _streifengrenzen(gx_lebt, anteile):
-    """x stripes holding the given shares of the living asteroids
-    (film_producer.py:382-405); the outer bounds are infinite."""
-    if len(anteile) < 2:
-        return [(-np.inf, np.inf)]
-    q, lauf = [], 0.0
-    for a in anteile[:-1]:
-        lauf += a
-        q.append(100.0 * lauf)
-    g = gx_lebt.cpu().numpy() if isinstance(gx_lebt, torch.Tensor) else np.asarray(gx_lebt)
-    schnitte = [float(v) for v in np.percentile(g, q)]
-    kanten = [-np.inf, *schnitte, np.inf]
-    return list(zip(kanten[:-1], kanten[1:]))
+def percentile_linear(sorted_vals, q: float) -> float:
+    """NumPy's default ("linear") percentile of the ascending f32 values
+    `sorted_vals` (NumPy array or device tensor; NaN sorts last and makes the
+    result NaN), with NumPy 2's arithmetic for f32 input, all of it in f32:
+    q / 100, the virtual index (n - 1) * q, its fractional part t, and the
+    interpolation a + (b - a) t, or b - (b - a)(1 - t) for t >= 1/2. Only the
+    two neighbours and the last value are read."""
+    f32 = np.float32
+    n = int(sorted_vals.shape[0])
+    if n == 0:
+        raise ValueError("percentile of an empty sample")
+
+    def at(i):
+        v = sorted_vals[i]
+        return f32(v.item() if isinstance(v, torch.Tensor) else v)
+
+    if np.isnan(at(n - 1)):
+        return float("nan")
+    vi = f32(n - 1) * (f32(q) / f32(100))
+    if vi >= n - 1:
+        return float(at(n - 1))
+    lo = np.floor(vi)
+    a, b = at(int(lo)), at(int(lo) + 1)
+    t = vi - lo
+    d = b - a
+    if t >= 0.5:
+        return float(b - d * (f32(1) - t))
+    return float(a + d * t)
 
 
-LAST_MIN_ANTEIL = 0.05                                # film_producer.py:415
-
-
-def _lastanteile(anteile, last):
-    """Stripe shares for the next sample from the measured candidate counts
-    (film_producer.py:418-479): each share is multiplied by
-    (fair share / measured share) ** LAST_ALPHA, renormalised, and shares
-    below LAST_MIN_ANTEIL are pinned there while the rest share the
-    remaining room (uniform shares if that room is gone)."""
-    n = len(anteile)
-    if n < 2:
-        return list(anteile)
-    ges = float(sum(last))
-    if ges <= 0 or min(last) < 0:
-        return list(anteile)
-    neu = [max(anteile[i] * ((1.0 / n) / max(last[i] / ges, 1e-9)) ** LAST_ALPHA, 1e-6) for i in range(n)]
-    summe = sum(neu)
-    neu = [a / summe for a in neu]
-    klein = [a < LAST_MIN_ANTEIL for a in neu]
-    if any(klein):
-        platz = 1.0 - LAST_MIN_ANTEIL * sum(klein)
-        rest = sum(a for a, k in zip(neu, klein) if not k)
-        if platz <= 0 or rest <= 0:
-            return [1.0 / n] * n
-        neu = [LAST_MIN_ANTEIL if k else a / rest * platz for a, k in zip(neu, klein)]
-    return neu
+def search_cell(gvx, gvy, alive, dt_y: float) -> float:
+    """The broadphase cell size h = max(1e-4, 2 v95 dt) of bounce_suche
+    (film_producer.py:357-359): v95 the 95th percentile of the f32 speeds
+    hypot(vx, vy) of the living asteroids (device mask `alive`), the speeds
+    rounded as the C library's hypotf rounds them (exact squares in f64, one
+    square root), sorted on the device."""
+    dev = alive.device
+    vx = _dev_f32(gvx, dev)[alive].double()
+    vy = _dev_f32(gvy, dev)[alive].double()
+    speed = torch.sqrt(vx * vx + vy * vy).float()
+    v95 = percentile_linear(torch.sort(speed).values, 95)
+    return max(1e-4, 2.0 * v95 * dt_y)
 
 
 def bounce_suche(det, det_pool, rows, dt_y: float, rr_max: float, anteile=None):
-    """Asteroid x asteroid collisions over the detection cards
-    (film_producer.py:324-379): h from the 95th speed percentile, halo
-    2h + 2 r_max, one stripe per card. Returns (hits | None, candidates,
-    h, new shares)."""
+    """Asteroid x asteroid collisions of one sample (film_producer.py:324-379).
+
+    One B200 is one detection card and owns the whole x range: the card
+    searches (-inf, inf), so there is no stripe split and no load to balance;
+    the shares come back as given (uniform when absent or of the wrong
+    length), as the reference returns them for a single card. rows[0] holds
+    the sample's f32 fields (x, y, vx, vy); further rows and det_pool are
+    not used. The reach is the reference's: h from search_cell and a halo
+    of 2h + 2 r_max. Returns (hits | None, candidate count, h, shares)."""
+    n_rows = len(rows)
+    shares = list(anteile) if anteile is not None and len(anteile) == n_rows else [1.0 / n_rows] * n_rows
+    card = det[0]
     gx, gy, gvx, gvy = rows[0]
-    if anteile is None or len(anteile) != len(rows):
-        anteile = [1.0 / len(rows)] * len(rows)
-    k0 = det[0]
-    dev = torch.device("cuda", k0.dev)
-    lebt = torch.nonzero((k0.g_ast != 0) & (k0.g_vis != 0)).flatten()
-    if lebt.numel() < 2:
-        return None, 0, 0.0, anteile
-    vx_t, vy_t = _dev_f32(gvx, dev), _dev_f32(gvy, dev)
-    speed = torch.hypot(vx_t[lebt], vy_t[lebt]).double()
-    v95 = float(torch.quantile(speed, 0.95))
-    grenzen = _streifengrenzen(_dev_f32(gx, dev)[lebt], anteile)
-    h = max(1e-4, 2.0 * v95 * dt_y)
-    halo = 2.0 * h + 2.0 * rr_max
-    for karte, (lo, hi) in zip(det, grenzen):
-        karte.streifen(lo, hi)
-    teile = [karte.bounce_hits(*row, dt_y, h, halo) for karte, row in zip(det[:len(rows)], rows)]
-    hits = [t for t, _ in teile if t is not None]
-    je_karte = [kand for _, kand in teile]
-    neu = _lastanteile(anteile, je_karte)
-    if not hits:
-        return None, sum(je_karte), h, neu
-    return ((np.concatenate([t[0] for t in hits]), np.concatenate([t[1] for t in hits])),
-            sum(je_karte), h, neu)
+    alive = (card.g_ast != 0) & (card.g_vis != 0)
+    if int(alive.sum()) < 2:
+        return None, 0, 0.0, shares
+    h = search_cell(gvx, gvy, alive, dt_y)
+    card.streifen(-np.inf, np.inf)
+    hits, cand = card.bounce_hits(gx, gy, gvx, gvy, dt_y, h, 2.0 * h + 2.0 * rr_max)
+    return hits, cand, h, shares

@@ -779,6 +779,7 @@ extern "C" int sss_broadphase_order(sss_ctx* ctx, int* hits, int64_t k, int64_t 
     if (k < 0 || n < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
     if (k > 0 && !hits) return sss_set_err(ctx, SSS_ERR_ARG, "NULL hits");
     if (n >= ((int64_t)1 << 30)) return sss_set_err(ctx, SSS_ERR_ARG, "too many bodies for the packed hit key");
+    if (k > (int64_t)INT32_MAX) return sss_set_err(ctx, SSS_ERR_ARG, "too many hits for the 32-bit sort index");
     if (k < 2) return SSS_OK;
     SSS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = (cudaStream_t)stream;

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(SW_NT) k_sweep_write(const SweepIn in, const S
 __device__ __forceinline__ bool runaway(const SweepIn& in, const SweepHead& h, long long j) {
     if (!h.has_mass || in.vis[j] == 0 || in.is_ast[j] == 0) return false;
     const float dx = __fsub_rn(in.gx[j], h.bx), dy = __fsub_rn(in.gy[j], h.by);
-    const float r = fmaxf(hypotf(dx, dy), 1e-6f);
+    const float r = fmaxf(sss_hypot_f32(dx, dy), 1e-6f);
     const float v2 = __fadd_rn(__fmul_rn(in.gvx[j], in.gvx[j]), __fmul_rn(in.gvy[j], in.gvy[j]));
     const float vesc2 = __fdiv_rn(h.vesc_coef, r);
     return v2 > __fmul_rn(9.0f, vesc2);

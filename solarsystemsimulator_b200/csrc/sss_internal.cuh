@@ -168,3 +168,12 @@ __device__ __forceinline__ double sss_gm_rinv3_cuda(double gm, double r2) {
     const double inv = rsqrt(r2);
     return ((gm * inv) * inv) * inv;
 }
+
+// f32 hypot, correctly rounded as the C library's hypotf (which NumPy calls for float32
+// hypot): the squares of f32 values are exact in f64, their sum is rounded once, the square
+// root once, then the result to f32.
+__device__ __forceinline__ float sss_hypot_f32(float x, float y) {
+    if (isinf(x) || isinf(y)) return __int_as_float(0x7F800000);
+    const double xd = x, yd = y;
+    return __double2float_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(xd, xd), __dmul_rn(yd, yd))));
+}

@@ -42,12 +42,81 @@ struct Box {
     float x1, y1;                      // f32 of x0 + spanx, y0 + spany (summed in f64)
 };
 
+// log(1 + x) for f32 x >= 0 with every operation rounded to f32, by the published reduction
+// method of fdlibm's log1pf (Sun Microsystems, 1993): the f32 log1p of the C library that NumPy
+// calls for float32 log1p where it dispatches no SIMD kernel. 1 + x = 2^k (1 + f) with
+// sqrt(2)/2 <= 1 + f < sqrt(2) and a correction c for the rounding of 1 + x, s = f / (2 + f),
+// log(1 + f) = f - (hfsq - s (hfsq + R(s^2))) with hfsq = f^2 / 2 and R a degree-7 minimax
+// polynomial, k ln 2 in two parts; where k comes out 0 the correction is not applied.
+__device__ __forceinline__ float log1p_f32(float x) {
+    const int hx = __float_as_int(x);
+    if (hx >= 0x7F800000 || hx < 0) return __fadd_rn(x, x);            // inf, nan (x < 0 never occurs)
+    if (hx < 0x31000000)                                                // x < 2^-29
+        return hx < 0x24800000 ? x : __fsub_rn(x, __fmul_rn(__fmul_rn(x, x), 0.5f));
+    int k = 0, hu = 1;
+    float f = x, c = 0.0f;
+    if (hx >= 0x3ED413D7) {                                             // x >= 0.41422: reduce
+        float u;
+        if (hx < 0x5A000000) {
+            u = __fadd_rn(1.0f, x);
+            hu = __float_as_int(u);
+            k = (hu >> 23) - 127;
+            c = k > 0 ? __fsub_rn(1.0f, __fsub_rn(u, x)) : __fsub_rn(x, __fsub_rn(u, 1.0f));
+            c = __fdiv_rn(c, u);
+        } else {
+            u = x;
+            hu = __float_as_int(u);
+            k = (hu >> 23) - 127;
+        }
+        hu &= 0x007FFFFF;
+        if (hu < 0x3504F7) {
+            u = __int_as_float(hu | 0x3F800000);
+        } else {
+            k += 1;
+            u = __int_as_float(hu | 0x3F000000);
+            hu = (0x00800000 - hu) >> 2;
+        }
+        f = __fsub_rn(u, 1.0f);
+    }
+    const float kf = (float)k;
+    const float hfsq = __fmul_rn(__fmul_rn(0.5f, f), f);
+    if (hu == 0) {                                                      // |f| < 2^-20
+        if (f == 0.0f) return k == 0 ? 0.0f : __fadd_rn(__fmul_rn(kf, __int_as_float(0x3F317180)),
+                                                        __fadd_rn(c, __fmul_rn(kf, __int_as_float(0x3717F7D1))));
+        const float R = __fmul_rn(hfsq, __fsub_rn(1.0f, __fmul_rn(0.6666666666666666f, f)));
+        if (k == 0) return __fsub_rn(f, R);
+        return __fsub_rn(__fmul_rn(kf, __int_as_float(0x3F317180)),
+                         __fsub_rn(__fsub_rn(R, __fadd_rn(__fmul_rn(kf, __int_as_float(0x3717F7D1)), c)), f));
+    }
+    const float s = __fdiv_rn(f, __fadd_rn(2.0f, f));
+    const float z = __fmul_rn(s, s);
+    float R = __int_as_float(0x3E178897);
+    R = __fadd_rn(__int_as_float(0x3E1CD04F), __fmul_rn(z, R));
+    R = __fadd_rn(__int_as_float(0x3E3A3325), __fmul_rn(z, R));
+    R = __fadd_rn(__int_as_float(0x3E638E29), __fmul_rn(z, R));
+    R = __fadd_rn(__int_as_float(0x3E924925), __fmul_rn(z, R));
+    R = __fadd_rn(__int_as_float(0x3ECCCCCD), __fmul_rn(z, R));
+    R = __fadd_rn(__int_as_float(0x3F2AAAAB), __fmul_rn(z, R));
+    R = __fmul_rn(z, R);
+    const float t = __fmul_rn(s, __fadd_rn(hfsq, R));
+    if (k == 0) return __fsub_rn(f, __fsub_rn(hfsq, t));
+    return __fsub_rn(__fmul_rn(kf, __int_as_float(0x3F317180)),
+                     __fsub_rn(__fsub_rn(hfsq, __fadd_rn(t, __fadd_rn(__fmul_rn(kf, __int_as_float(0x3717F7D1)), c))),
+                               f));
+}
+
+// Display scale of _anzeige_koords (server.py:99-111) for log zoom: log1p(r) / (log 33 * r) in
+// f32, 0 at the origin.
+__device__ __forceinline__ float log_zoom_scale(float px, float py) {
+    const float r = sss_hypot_f32(px, py);
+    return r > 1e-9f ? __fdiv_rn(log1p_f32(r), __fmul_rn(LOG33F, fmaxf(r, 1e-30f))) : 0.0f;
+}
+
 __global__ void k_disp(const float* __restrict__ x, const float* __restrict__ y, long long n, float* __restrict__ qx,
                        float* __restrict__ qy) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float r = hypotf(x[i], y[i]);
-    const float sk = r > 1e-9f ? __fdiv_rn(log1pf(r), __fmul_rn(LOG33F, fmaxf(r, 1e-30f))) : 0.0f;
+    const float sk = log_zoom_scale(x[i], y[i]);
     qx[i] = __fmul_rn(x[i], sk);
     qy[i] = __fmul_rn(y[i], sk);
 }
@@ -955,8 +1024,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
             if (i >= c1) break;
             float px = bx[u], py = by[u];
             if (a.log_zoom) {
-                const float r = hypotf(px, py);
-                const float sk = r > 1e-9f ? __fdiv_rn(log1pf(r), __fmul_rn(LOG33F, fmaxf(r, 1e-30f))) : 0.0f;
+                const float sk = log_zoom_scale(px, py);
                 px = __fmul_rn(px, sk);
                 py = __fmul_rn(py, sk);
                 a.qx[i] = px;
@@ -1186,6 +1254,17 @@ int sample_grid(sss_ctx* ctx, int* grid) {
 }
 
 }  // namespace
+
+extern "C" int sss_stream_display(sss_ctx* ctx, int64_t n, const float* x, const float* y, float* qx, float* qy,
+                                  void* stream) {
+    if (!ctx) return SSS_ERR_ARG;
+    if (n < 0 || (n > 0 && (!x || !y || !qx || !qy)))
+        return sss_set_err(ctx, SSS_ERR_ARG, "display: negative size or NULL buffer");
+    if (n == 0) return SSS_OK;
+    k_disp<<<nb(n), 256, 0, (cudaStream_t)stream>>>(x, y, n, qx, qy);
+    SSS_LAUNCH_CHECK(ctx, "k_disp");
+    return SSS_OK;
+}
 
 extern "C" int sss_stream_minmax(sss_ctx* ctx, int64_t n, const float* x, const float* y, int log_zoom, float* out4,
                                  void* stream) {

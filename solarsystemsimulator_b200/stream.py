@@ -56,6 +56,19 @@ class StreamFrames:
         i = torch.as_tensor(np.asarray(idx, np.int64)).to(self.dev)
         self.kill_t[i] = torch.minimum(self.kill_t[i], torch.full_like(self.kill_t[i], float(t)))
 
+    def display(self, x, y):
+        """Log-zoom display coordinates of f32 device tensors x, y
+        (_anzeige_koords with log_zoom, server.py:99-111): new tensors."""
+        x = x.to(device=self.dev, dtype=torch.float32).contiguous()
+        y = y.to(device=self.dev, dtype=torch.float32).contiguous()
+        if x.numel() != y.numel():
+            raise ValueError("display: x and y must have the same length")
+        qx, qy = torch.empty_like(x), torch.empty_like(y)
+        with torch.cuda.device(self.device):
+            self.ctx.check(self.ctx.lib.sss_stream_display(self.ctx.ptr, x.numel(), x.data_ptr(), y.data_ptr(),
+                                                           qx.data_ptr(), qy.data_ptr(), self._s()))
+        return qx, qy
+
     def box(self, x, y, view, log_zoom: bool):
         """The reference box: 2x the viewport about the camera, or before
         the client reported one, the whole distribution plus 5 %."""

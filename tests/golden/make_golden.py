@@ -2,7 +2,7 @@
 
 Run in the build container (where the reference checkout exists):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference [which ...]
 
 The reference's array-level Python (NumPy oracles in backend/test_*.py,
 backend/pm_kernel.py, the broadphase of backend/film_producer.py) is
@@ -173,11 +173,60 @@ def broadphase(ref):
         np.zeros(2), np.full(2, 1e-4))
 
 
+def clouds_scene(n_per_cloud=40_000):
+    """The asteroid-cloud configuration's broadphase input: 5 Gaussian clouds
+    of n_per_cloud asteroids from the seeded generator, the f32 snapshot of
+    x, y, vx, vy and radii, dt = 0.5 day, h from the 95th speed percentile
+    (film_producer.py:357-359)."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from solarsystemsimulator_b200 import workloads
+    w = workloads.asteroid_clouds(n_per_cloud=n_per_cloud)
+    a = np.flatnonzero(w["is_ast"] != 0)
+    f = [np.ascontiguousarray(v, dtype=np.float32) for v in
+         (w["pos"][0, a], w["pos"][1, a], w["vel"][0, a], w["vel"][1, a], w["radius"][a])]
+    dt = 0.5
+    v95 = float(np.percentile(np.hypot(f[2], f[3]), 95))
+    h = max(1e-4, 2.0 * v95 * dt)
+    halo = 2.0 * h + 2.0 * float(f[4].max())
+    return f, dt, h, halo
+
+
+def scene_digest(f):
+    import hashlib
+    d = hashlib.sha256()
+    for v in f:
+        d.update(np.ascontiguousarray(v, dtype=np.float32).tobytes())
+    return d.hexdigest()
+
+
+def broadphase_clouds(ref):
+    """The 200,000-asteroid cloud scene through the reference's own `_hits`
+    (film_producer.py:223-317). Only the hit list, the candidate count, the
+    scalars and a digest of the input are stored; the test rebuilds the
+    scene from the seeded generator and checks the digest first."""
+    import time
+    import film_producer as fp
+    f, dt, h, halo = clouds_scene()
+    n = len(f[0])
+    karte = fp.Erkennungskarte(0, np.ones(n, bool), -np.inf, np.inf)
+    karte.stammdaten(np.ones(n, np.uint8), f[4])
+    t0 = time.time()
+    hits, kand = karte.bounce_hits(f[0], f[1], f[2], f[3], dt, h, halo)
+    print(f"_hits on {n} asteroids: {kand} candidates, {time.time() - t0:.0f} s")
+    hi = np.empty(0, np.int64) if hits is None else np.asarray(hits[0], np.int64)
+    hj = np.empty(0, np.int64) if hits is None else np.asarray(hits[1], np.int64)
+    _save("broadphase_asteroid_clouds_200k.npz", n_per_cloud=40_000, dt=dt, h=h, halo=halo,
+          digest=np.array(scene_digest(f)), hit_i=hi.astype(np.int32), hit_j=hj.astype(np.int32),
+          n_cand=np.int64(kand))
+
+
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2 or not os.path.isdir(os.path.join(sys.argv[1], "backend")):
+        sys.exit("usage: make_golden.py REFERENCE_CHECKOUT [selfgrav|frame|pm|broadphase|broadphase_clouds ...]")
+    ref = sys.argv[1]
     sys.path.insert(0, os.path.join(ref, "backend"))
     cupy_shim.install()
-    which = sys.argv[2:] or ["selfgrav", "frame", "pm", "broadphase"]
+    which = sys.argv[2:] or ["selfgrav", "frame", "pm", "broadphase", "broadphase_clouds"]
     for w in which:
         globals()[w](ref)
 

@@ -10,6 +10,13 @@ the inputs and, per sample, the culled/thinned index list, the u16
 coordinates and the box.
 
     python tests/golden/make_golden_frames.py /path/to/reference/backend
+
+NumPy runs with its SIMD dispatch switched off (NPY_DISABLE_CPU_FEATURES,
+read when NumPy is imported), so float32 log1p and hypot are the C
+library's: on CPUs with AVX512_SKX NumPy would otherwise take float32 log1p
+from a SIMD kernel that differs from the C library in the last bit or two
+for about 10 % of the inputs, and the log-zoom frame would depend on the
+CPU that wrote it.
 """
 from __future__ import annotations
 
@@ -17,7 +24,10 @@ import os
 import struct
 import sys
 
-import numpy as np
+os.environ["NPY_DISABLE_CPU_FEATURES"] = ("AVX512F AVX512CD AVX512_SKX AVX512_CLX AVX512_CNL AVX512_ICL "
+                                          "AVX512_SPR AVX2 FMA3 F16C AVX")
+
+import numpy as np  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -147,4 +157,6 @@ def main(backend: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/backend")
+    if len(sys.argv) < 2 or not os.path.isfile(os.path.join(sys.argv[1], "server.py")):
+        sys.exit("usage: make_golden_frames.py REFERENCE_CHECKOUT/backend")
+    main(sys.argv[1])

@@ -49,7 +49,7 @@ def test_stripe_union_equals_single_card(load_golden, scene):
     full = set(zip(g["hit_i"].tolist(), g["hit_j"].tolist()))
     for k in (2, 3, 5):
         got, count = set(), 0
-        for lo, hi in bp._streifengrenzen(g["x"], [1.0 / k] * k):
+        for lo, hi in g[f"stripes{k}_bounds"]:
             karte.streifen(lo, hi)
             res, _ = karte.bounce_hits(g["x"], g["y"], g["vx"], g["vy"], float(g["dt_y"]), float(g["h"]),
                                        float(g["halo"]))
@@ -200,3 +200,86 @@ def test_hit_order_rejects_bad_sizes():
     assert ctx.lib.sss_broadphase_order(ctx.ptr, None, -1, 10, None) == _lib.SSS_ERR_ARG
     assert ctx.lib.sss_broadphase_order(ctx.ptr, None, 5, 10, None) == _lib.SSS_ERR_ARG
     assert ctx.lib.sss_broadphase_order(ctx.ptr, None, 0, 1 << 30, None) == _lib.SSS_ERR_ARG
+    # more hits than the 32-bit sort index holds (checked before any access)
+    assert ctx.lib.sss_broadphase_order(ctx.ptr, ctypes.c_void_p(16), (1 << 31), 10, None) == _lib.SSS_ERR_ARG
+
+
+def _clouds_scene(n_per_cloud=40_000):
+    """The asteroid-cloud configuration's broadphase input, built as
+    tests/golden/make_golden.py builds it for the reference's `_hits`."""
+    import hashlib
+    from solarsystemsimulator_b200 import workloads
+    w = workloads.asteroid_clouds(n_per_cloud=n_per_cloud)
+    a = np.flatnonzero(w["is_ast"] != 0)
+    f = [np.ascontiguousarray(v, dtype=np.float32) for v in
+         (w["pos"][0, a], w["pos"][1, a], w["vel"][0, a], w["vel"][1, a], w["radius"][a])]
+    d = hashlib.sha256()
+    for v in f:
+        d.update(v.tobytes())
+    return f, d.hexdigest()
+
+
+def test_asteroid_clouds_200k_bit_exact_against_reference(load_golden):
+    """The configured scene (200,000 asteroids in 5 Gaussian clouds, 3.1e9
+    candidate pairs): pairs, order and candidate count equal to the
+    reference's own `_hits` on it; h and the halo come from bounce_suche and
+    equal the reference's (film_producer.py:357-362)."""
+    bp = _bp()
+    g = load_golden("broadphase_asteroid_clouds_200k.npz")
+    f, digest = _clouds_scene(int(g["n_per_cloud"]))
+    assert digest == str(g["digest"])                  # the same f32 input as the reference saw
+    x, y, vx, vy, rr = f
+    n = len(x)
+    karte = bp.Erkennungskarte(0, np.ones(n, bool), -np.inf, np.inf)
+    karte.stammdaten(np.ones(n, np.uint8), rr)
+    res, cand, h, shares = bp.bounce_suche([karte], None, [(x, y, vx, vy)], float(g["dt"]), float(rr.max()))
+    assert h == float(g["h"]) and shares == [1.0]
+    assert cand == int(g["n_cand"])
+    assert _same(res, (g["hit_i"].astype(np.int64), g["hit_j"].astype(np.int64)))
+    assert len(res[0]) == 5192
+
+
+def test_bounce_suche_matches_reference_arithmetic():
+    """bounce_suche's cell size from the living asteroids' speeds (hidden
+    bodies and non-asteroids excluded) equals max(1e-4, 2 v95 dt) with v95 =
+    np.percentile(np.hypot(f32, f32), 95), and its hits equal the oracle's."""
+    bp = _bp()
+    for seed, n in ((3, 50_000), (4, 7), (5, 2)):
+        x, y, vx, vy, rr = _scene(seed, n, "clumps")
+        rng = np.random.default_rng(seed)
+        is_ast = rng.random(n) > 0.1
+        vis = (rng.random(n) > 0.1).astype(np.uint8)
+        if n == 2:
+            is_ast[:] = True
+            vis[:] = 1
+        lebt = np.flatnonzero(is_ast & (vis != 0))
+        dt = 0.5 / 365.25
+        v95 = float(np.percentile(np.hypot(vx[lebt], vy[lebt]), 95))
+        h_ref = max(1e-4, 2.0 * v95 * dt)
+        karte = bp.Erkennungskarte(0, is_ast, -np.inf, np.inf)
+        karte.stammdaten(vis, rr)
+        res, cand, h, shares = bp.bounce_suche([karte], None, [(x, y, vx, vy)], dt, float(rr.max()))
+        assert h == h_ref and shares == [1.0]
+        ref, cref = obp.hits(x, y, vx, vy, rr, dt, h_ref, 2.0 * h_ref + 2.0 * float(rr.max()), is_ast=is_ast, vis=vis)
+        assert cand == cref and _same(res, ref)
+
+
+def test_one_alive_body_among_many():
+    """Exactly one living asteroid among many bodies (hidden ones and
+    non-asteroids around it, in the same cell): no pair, no candidate."""
+    bp = _bp()
+    n = 5000
+    x = np.full(n, 1.0, np.float32)
+    rr = np.full(n, 1e-3, np.float32)
+    for is_ast, vis in ((np.zeros(n, bool), np.ones(n, np.uint8)), (np.ones(n, bool), np.zeros(n, np.uint8))):
+        is_ast = is_ast.copy()
+        vis = vis.copy()
+        is_ast[1234] = True
+        vis[1234] = 1
+        ref = obp.hits(x, x, x, x, rr, 0.01, 0.1, 0.2, is_ast=is_ast, vis=vis)
+        assert ref == (None, 0)
+        assert bp.bounce_hits(x, x, x, x, 0.01, 0.1, 0.2, rr=rr, is_ast=is_ast, vis=vis) == (None, 0)
+    # one alive body inside the stripe window, many outside it
+    x2 = np.concatenate([np.full(n - 1, 50.0, np.float32), np.array([1.0], np.float32)])
+    assert bp.bounce_hits(x2, x2, x2, x2, 0.01, 0.1, 0.2, rr=rr, lo=0.0, hi=2.0) == \
+        obp.hits(x2, x2, x2, x2, rr, 0.01, 0.1, 0.2, lo=0.0, hi=2.0) == (None, 0)

@@ -1,6 +1,7 @@
-"""Host-side logic of the broadphase (no GPU): cell hash, stripe bounds and
-the stripe load regulator, against the reference's behaviour."""
+"""Host-side logic of the broadphase (no GPU): the cell hash and the
+percentile arithmetic of the search cell, against NumPy and the reference."""
 import numpy as np
+import pytest
 
 from solarsystemsimulator_b200 import broadphase as bp
 
@@ -15,23 +16,20 @@ def test_cell_hash_wraps_like_int64():
     assert k.tolist() == want
 
 
-def test_stripes_cover_the_line():
-    g = np.random.default_rng(1).normal(size=1000)
-    assert bp._streifengrenzen(g, [1.0]) == [(-np.inf, np.inf)]
-    s = bp._streifengrenzen(g, [0.25, 0.25, 0.5])
-    assert s[0][0] == -np.inf and s[-1][1] == np.inf
-    assert all(s[i][1] == s[i + 1][0] for i in range(len(s) - 1))
-
-
-def test_load_regulator_converges_and_respects_floor():
-    # a skewed load narrows the loaded stripe; shares stay normalised and >= 5 %
-    a = [0.5, 0.5]
-    for _ in range(30):
-        dichte = [4.0, 1.0]                     # stripe 0 is four times denser
-        last = [d * x for d, x in zip(dichte, a)]
-        a = bp._lastanteile(a, last)
-    assert abs(sum(a) - 1.0) < 1e-12
-    assert a[0] < 0.3 and a[1] > 0.7
-    b = bp._lastanteile([0.9, 0.1], [1, 10**9])
-    assert min(b) >= bp.LAST_MIN_ANTEIL - 1e-12 and abs(sum(b) - 1) < 1e-12
-    assert bp._lastanteile([0.5, 0.5], [0, 0]) == [0.5, 0.5]
+@pytest.mark.parametrize("seed", range(6))
+def test_percentile_matches_numpy_on_f32(seed):
+    """percentile_linear reproduces np.percentile(f32 speeds, 95), the
+    reference's v95 (film_producer.py:357), bit for bit: every size from 1
+    to 60 and a few large ones, ties, NaN."""
+    rng = np.random.default_rng(seed)
+    sizes = list(range(1, 61)) + [1000, 4097, 200_000]
+    for n in sizes:
+        v = np.hypot(rng.normal(0, 3, n), rng.normal(0, 3, n)).astype(np.float32)
+        if seed == 1:
+            v = np.round(v, 1).astype(np.float32)            # ties
+        if seed == 2 and n > 3:
+            v[n // 2] = np.nan
+        for q in (95, 50, 0, 100, 99.9):
+            want = np.percentile(v, q)
+            got = bp.percentile_linear(np.sort(v), q)
+            assert (np.isnan(want) and np.isnan(got)) or got == float(want), (n, q, got, want)
