@@ -97,3 +97,25 @@ def test_rejects_oversized_systems():
     big = {"pos": np.zeros((3, 65)), "vel": np.zeros((3, 65)), "mass": np.ones(65), "G": 1.0, "dt": 1e-3}
     with pytest.raises(ValueError):
         batched.BatchedSystems([big], device=0)
+
+
+def test_matches_reference_advance_golden(load_golden):
+    """The batched kernel against the reference's own reference_advance
+    (test_kernel.py:16-81) on all-massive systems whose substep stays at
+    MAX_SUB_DT_YEARS (fixture by tests/golden/make_golden.py): 400 Yoshida-4
+    steps, 2-D, each system also repeated so every size group holds many."""
+    from solarsystemsimulator_b200 import batched
+    g = load_golden("batched_reference_advance.npz")
+    base = []
+    for s in range(3):
+        base.append({"pos": np.stack([g[f"x{s}"], g[f"y{s}"]]), "vel": np.stack([g[f"vx{s}"], g[f"vy{s}"]]),
+                     "mass": g[f"m{s}"], "G": float(g["G"]), "dt": float(g["dt"])})
+    systems = [base[k % 3] for k in range(300)]
+    ens = batched.BatchedSystems(systems, device=0, eps2=float(g["eps2"]), dim=2)
+    ens.run(int(g["steps"]))
+    for k, (p, v) in enumerate(ens.export()):
+        s = k % 3
+        rp = np.stack([g[f"rx{s}"], g[f"ry{s}"]])
+        rv = np.stack([g[f"rvx{s}"], g[f"rvy{s}"]])
+        assert np.abs(p - rp).max() <= 1e-12 * np.abs(rp).max()
+        assert np.abs(v - rv).max() <= 1e-12 * np.abs(rv).max()

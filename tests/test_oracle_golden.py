@@ -64,3 +64,23 @@ def test_momentum_conservation_of_oracle():
     a = osg.accel(rec, rec, 1e-3, dim=3)
     p = (m[:, None] * a[:, :3]).sum(0)
     assert np.abs(p).max() < 1e-12 * (m[:, None] * np.abs(a[:, :3])).sum()
+
+
+def test_batched_oracle_matches_reference_advance(load_golden):
+    """oracle/batched.py's fixed-step Yoshida-4 against the reference's own
+    test_kernel.reference_advance (test_kernel.py:16-81) on all-massive
+    planetary systems of 3, 7 and 12 bodies whose substep stays at
+    MAX_SUB_DT_YEARS: 400 steps, within 1e-13 of the scale (rounding order
+    only: the reference's position-Verlet form against kick-drift-kick)."""
+    from oracle import batched as ob
+    g = load_golden("batched_reference_advance.npz")
+    for s in range(3):
+        pos = np.stack([g[f"x{s}"], g[f"y{s}"]])
+        vel = np.stack([g[f"vx{s}"], g[f"vy{s}"]])
+        p, v = ob.yoshida(pos, vel, g[f"m{s}"], float(g["G"]), float(g["dt"]), int(g["steps"]),
+                          eps2=float(g["eps2"]))
+        rp = np.stack([g[f"rx{s}"], g[f"ry{s}"]])
+        rv = np.stack([g[f"rvx{s}"], g[f"rvy{s}"]])
+        assert np.abs(p - rp).max() <= 1e-13 * np.abs(rp).max()
+        assert np.abs(v - rv).max() <= 1e-13 * np.abs(rv).max()
+        assert np.abs(rp - pos).max() > 0.5                     # the systems really moved

@@ -47,6 +47,23 @@ def test_deposit_matches_oracle(mods, clump):
     assert abs(rho.sum() - ref.sum()) <= 1e-5 * ref.sum()
 
 
+def test_deposit_in_a_plane_is_the_reference_2d_deposit(mods, load_golden):
+    """k_deposit3 with every body on the plane z = 0 against the reference's
+    own 2-D deposit (pm_kernel._cic_deposit, fixture pm2d_n2000_g128.npz):
+    the plane times h^3 is its mass grid to f32 rounding, the other planes
+    stay empty."""
+    _lib, pm3d, _, _ = mods
+    g = load_golden("pm2d_n2000_g128.npz")
+    n, h = int(g["grid_n"]), float(g["h"])
+    pos = np.stack([g["x"] - float(g["x0"]), g["y"] - float(g["y0"]), np.zeros(len(g["x"]))], 1)
+    pm = pm3d.PMPeriodic3D(n, n * h, 1.0)
+    st = pm.load_state(pos, np.zeros_like(pos), g["m"])
+    pm.mesh_forces(st)
+    rho = pm.rho.double().cpu().numpy().reshape(n, n, n)
+    assert np.abs(rho[:, :, 1:]).max() == 0.0
+    assert np.abs(rho[:, :, 0] * h ** 3 - g["rho"]).max() <= 2e-6 * np.abs(g["rho"]).max()
+
+
 @pytest.mark.parametrize("mesh,deconv,rs", [(32, 2, 0.6), (64, 2, 0.6), (32, 0, 0.0), (48, 1, 1.0)])
 def test_forces_match_oracle(mods, mesh, deconv, rs):
     _lib, pm3d, _, _ = mods

@@ -197,3 +197,19 @@ def test_p3m_pair_term_is_the_ewald_real_space_part():
     real = opm.ewald_accel(src, m, tgt, alpha=alpha, r_cut=r_cut, h_max=0, eps=eps, self_index=np.arange(5))
     pair = opm.p3m_short(src, m, tgt, alpha, r_cut, eps=eps, self_index=np.arange(5))
     assert np.allclose(pair, real, rtol=1e-9, atol=1e-9 * np.abs(real).max())
+
+
+def test_deposit_in_a_plane_is_the_reference_2d_deposit(load_golden):
+    """With z on a mesh plane the 3-D CIC stencil reduces to the 2-D one: the
+    oracle's deposit of the reference's own 2-D case (pm_kernel._cic_deposit,
+    pm_kernel.py:63-90, fixture pm2d_n2000_g128.npz) in plane z = 0 of a
+    periodic box of the same cells, times h^3, is the reference's mass grid.
+    The bodies sit inside the grid's margin, so its clipping never acts and
+    the periodic wrap never reaches them."""
+    g = load_golden("pm2d_n2000_g128.npz")
+    n, h = int(g["grid_n"]), float(g["h"])
+    pos = np.stack([g["x"] - float(g["x0"]), g["y"] - float(g["y0"]), np.zeros(len(g["x"]))], 1)
+    rho3 = o.cic_deposit(pos, g["m"], n, L=n * h)
+    plane = rho3[:, :, 0] * h ** 3
+    assert np.abs(rho3[:, :, 1:]).max() == 0.0
+    assert np.abs(plane - g["rho"]).max() <= 1e-12 * np.abs(g["rho"]).max()

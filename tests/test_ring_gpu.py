@@ -82,3 +82,39 @@ def test_reorder_matches_oracle():
     outs = rng.normal(0, 1, (K, 4 * nm + 2 * (n - nm))).astype(np.float32)
     got = ring.reorder_selfgrav(torch.as_tensor(outs).cuda(), sg_m, sg_t, n).cpu().numpy()
     assert np.array_equal(got, orng.reorder_selfgrav(outs, sg_m, sg_t, n))
+
+
+@pytest.mark.parametrize("case", ["few", "overflow"])
+def test_slot_matches_reference_golden(load_golden, case):
+    """sss_ring_slot against the bytes the reference's own schreibe_slot
+    wrote (tests/golden/make_golden.py): the golden hot bodies become gap-free
+    sub-sample chains in the frame kernel's layout [m_sub][2][n_ast]."""
+    import ctypes
+    from solarsystemsimulator_b200 import _lib
+    g = load_golden("ring_slots.npz")
+    n, m_sub, sub_max = int(g["n"]), int(g["m_sub"]), int(g[f"{case}_sub_max"])
+    idx, pos = g[f"{case}_idx"], g[f"{case}_pos"]
+    sub_pos = np.zeros((m_sub, 2, n), np.float32)
+    sub_pos[:, :, idx] = pos
+    sub_n = np.zeros(n, np.uint8)
+    sub_n[idx] = m_sub
+    sub_n[np.setdiff1d(np.arange(0, n, 7), idx)] = m_sub - 1      # chains with a gap are not hot
+    d = {k: torch.as_tensor(v).cuda() for k, v in
+         (("row", g["out_i"]), ("pos", sub_pos), ("sn", sub_n), ("ai", np.arange(n, dtype=np.int64)))}
+    slot = torch.zeros(orng.slot_bytes(n, m_sub, sub_max), dtype=torch.uint8, device="cuda")
+    hot = ctypes.c_int64()
+    ctx = _lib.context(0)
+    ctx.check(ctx.lib.sss_ring_slot(ctx.ptr, d["row"].data_ptr(), n, d["pos"].data_ptr(), d["sn"].data_ptr(),
+                                    d["ai"].data_ptr(), n, m_sub, 2, sub_max, slot.data_ptr(), ctypes.byref(hot),
+                                    ctypes.c_void_p(_lib.stream_handle(0))))
+    got, nh = _defined(slot.cpu().numpy(), n, m_sub, sub_max)
+    want, nh_ref = _defined(g[f"{case}_slot"], n, m_sub, sub_max)
+    assert nh == nh_ref and got == want
+    assert (hot.value > sub_max) == bool(g[f"{case}_overflow"])
+
+
+def test_reorder_matches_reference_golden(load_golden):
+    from solarsystemsimulator_b200 import ring
+    g = load_golden("ring_slots.npz")
+    got = ring.reorder_selfgrav(torch.as_tensor(g["sg_outs"]).cuda(), g["sg_m"], g["sg_t"], int(g["sg_n"]))
+    assert np.array_equal(got.cpu().numpy(), g["sg_full"])
