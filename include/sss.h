@@ -169,9 +169,16 @@ typedef struct sss_frame_state {
     int      max_sub_steps;       /* MAX_SUB_STEPS_PER_FRAME */
     double   w1, w0;              /* Yoshida weights */
     int      massless_asteroids;  /* 1: every asteroid mass is 0 (no back-reaction) */
+    int      fine_guard;          /* iteration limit of a hot asteroid's fine loop
+                                     (0 = SSS_FINE_GUARD, the reference's 8000) */
 } sss_frame_state;
+#define SSS_FINE_GUARD 8000
 
-/* One launch of k raster samples of length dt_raster (frame_kernel). snap is
+/* One launch of k raster samples of length dt_raster (frame_kernel). When
+ * the substep guard (max_sub_steps) or a fine-loop guard (fine_guard) runs
+ * out before its interval is covered, the launch stops that interval there
+ * as the reference does (nbody_kernel.py:248-250, :424) and records
+ * SSS_ERR_GUARD in the device status word (sss_device_status). snap is
  * [k][2*dim][n_ast + M] floats in original body order ([x|y|(z)|vx|vy|(vz)],
  * the layout NBodyCuda.step_batch returns); sub_pos [k][m_sub][dim][n_ast]
  * and sub_n [k][n_ast] hold the hot asteroids' sub-samples (sub_n == m_sub:
@@ -234,6 +241,11 @@ int  sss_pm2d_field(sss_pm2d* p, const double* gx, const double* gy, const doubl
 /* field read back at n points with the deposit's stencil (:93-107, :150-154) */
 int  sss_pm2d_gather(sss_pm2d* p, const double* px, const double* py, int64_t n, double x0, double y0,
                      double h, double* ax, double* ay, void* stream);
+/* one caller-held N x N f64 field (row stride ld >= N, device) read at n
+ * points with the deposit's stencil; replaces _cic_gather (:93-107) */
+int  sss_pm2d_gather_field(sss_ctx* ctx, const double* field, int grid_n, int64_t ld, const double* px,
+                           const double* py, int64_t n, double x0, double y0, double h, double* out,
+                           void* stream);
 /* the N x N crops of the last field into ax, ay (the arrays pm_force_field returns) */
 int  sss_pm2d_fields(sss_pm2d* p, double* ax, double* ay, void* stream);
 /* the N x N density of the last field call into rho (:63-90) */
@@ -529,6 +541,16 @@ int sss_allpairs_accel_noalloc(int device, int dim, int precision,
  * kind 0 = f64 DFMA, 1 = f32 FFMA, 2 = packed f32x2 FMA. Synchronous; the
  * roofline denominator of the all-pairs kernels. No reference counterpart. */
 int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops);
+
+/* Self-test of the bounded waits: runs one wait that nothing completes, with
+ * a limit of limit_s seconds (0 < limit_s <= 10), so that it gives up and
+ * records SSS_ERR_TIMEOUT in the device status word, which
+ * sss_device_status then returns; the context stays usable. which: 0 = the
+ * mbarrier wait of the bulk-copy and tensor-core kernels (an mbarrier that
+ * expects two arrivals gets one), 1 = the frame kernel's grid barrier and
+ * 2 = the stream-frame kernel's grid barrier (one of two blocks leaves
+ * without arriving). Asynchronous. No reference counterpart. */
+int sss_selftest_wait(sss_ctx* ctx, int which, double limit_s, void* stream);
 
 #ifdef __cplusplus
 }

@@ -56,6 +56,7 @@ class FrameState(ctypes.Structure):
         ("G", ctypes.c_double), ("softening", ctypes.c_double), ("max_sub_dt", ctypes.c_double),
         ("max_sub_steps", ctypes.c_int), ("w1", ctypes.c_double), ("w0", ctypes.c_double),
         ("massless_asteroids", ctypes.c_int),
+        ("fine_guard", ctypes.c_int),
     ]
 
 
@@ -103,6 +104,8 @@ SIGNATURES = {
     "sss_pm2d_build_kernels": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp]),
     "sss_pm2d_field": (ctypes.c_int, [_vp, _dp, _dp, _dp, _c_i64, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, _vp]),
+    "sss_pm2d_gather_field": (ctypes.c_int, [_vp, _dp, ctypes.c_int, _c_i64, _dp, _dp, _c_i64, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, _dp, _vp]),
     "sss_pm2d_gather": (ctypes.c_int, [_vp, _dp, _dp, _c_i64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                        _dp, _dp, _vp]),
     "sss_pm2d_density": (ctypes.c_int, [_vp, _dp, _vp]),
@@ -158,6 +161,7 @@ SIGNATURES = {
                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp]),
     "sss_mlp_correct": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(Pm3Particles), _dp, _dp, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _vp]),
+    "sss_selftest_wait": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp]),
     "sss_probe_fma": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,
@@ -231,6 +235,10 @@ class Context:
 
     def status(self, stream: int) -> None:
         self.check(self.lib.sss_device_status(self.ptr, _vp(stream)))
+
+    def status_code(self, stream: int) -> int:
+        """Synchronise the stream, read and clear the device status word."""
+        return int(self.lib.sss_device_status(self.ptr, _vp(stream)))
 
     @property
     def num_sms(self) -> int:

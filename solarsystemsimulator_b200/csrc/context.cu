@@ -110,7 +110,8 @@ extern "C" int sss_device_status(sss_ctx* ctx, void* stream) {
     if (e != cudaSuccess) return sss_cuda_err(ctx, e, "cudaMemcpy (status)");
     if (h != 0) {
         cudaMemset(ctx->d_status, 0, sizeof(int));
-        return sss_set_err(ctx, h, "device reported status %d (a bounded wait timed out)", h);
+        return sss_set_err(ctx, h, h == SSS_ERR_GUARD ? "device reported status %d (a step guard ran out)"
+                                                      : "device reported status %d (a bounded wait timed out)", h);
     }
     return SSS_OK;
 }

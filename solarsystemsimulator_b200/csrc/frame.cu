@@ -61,6 +61,8 @@ struct FrameArgs {
     unsigned* gbar;           // [2] arrival count, generation
     int* status;
     int* guard_out;           // substeps used (written by CTA 0)
+    int fine_guard;           // iteration limit of a hot asteroid's fine loop
+    uint64_t wait_ns;         // limit of a grid-barrier wait
 };
 
 struct FrameShared {
@@ -88,7 +90,7 @@ __device__ bool grid_sync(const FrameArgs& a, FrameShared& s) {
         } else {
             const uint64_t t0 = sss_globaltimer();
             while (*vgen == gen) {
-                if (sss_globaltimer() - t0 > SSS_WAIT_LIMIT_NS) {
+                if (sss_globaltimer() - t0 > a.wait_ns) {
                     atomicExch(a.status, SSS_ERR_TIMEOUT);
                     s.abort_ = 1;
                     break;
@@ -254,7 +256,7 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
     const double rad = a.arad[i];
     double tau = 0.0;
     int guardF = 0;
-    while (tau < span - 1e-15 && guardF++ < 8000) {
+    while (tau < span - 1e-15 && guardF++ < a.fine_guard) {
         const double al = tau / span;
         double dtF = a.max_sub_dt;
         for (int k = 0; k < a.M; ++k) {
@@ -309,6 +311,9 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
             }
         }
     }
+    // the guard ran out before the interval was covered: the reference stops there silently
+    // (nbody_kernel.py:424); the state keeps it, the status word records it
+    if (tau < span - 1e-15) atomicCAS(a.status, SSS_OK, SSS_ERR_GUARD);
     for (int c = 0; c < D; ++c) { a.ax[c][i] = p[c]; a.av[c][i] = v[c]; }
     double acc[3];
     massive_field<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
@@ -373,6 +378,8 @@ __global__ void __launch_bounds__(FR_NT) k_frame(const FrameArgs a) {
             const double dmin = pair_dt<D>(a, s);
             if (tid == 0) {
                 if (s.rem <= 1e-12 || s.guard++ >= a.max_sub_steps) {
+                    // a raster left unfinished by the substep guard (nbody_kernel.py:248-250)
+                    if (s.rem > 1e-12) atomicCAS(a.status, SSS_OK, SSS_ERR_GUARD);
                     s.done = 1;
                 } else {
                     double dtH = dmin;
@@ -480,6 +487,16 @@ __global__ void __launch_bounds__(FR_NT) k_frame(const FrameArgs a) {
     }
 }
 
+// Self-test of the bounded grid barrier: CTA 1 leaves without arriving, so
+// CTA 0's wait runs out after a.wait_ns and records SSS_ERR_TIMEOUT.
+__global__ void k_frame_barrier_selftest(const FrameArgs a) {
+    __shared__ FrameShared s;
+    if (threadIdx.x == 0) s.abort_ = 0;
+    __syncthreads();
+    if (blockIdx.x != 0) return;
+    grid_sync(a, s);
+}
+
 // Scatter updates at original indices into the resident state:
 // mode 0 = set x,v; 1 = add to x,v; 2 = set x,v and mass; vals [m][2D(+1)].
 struct ScatterPtrs {
@@ -571,6 +588,8 @@ extern "C" int sss_frame_launch(sss_ctx* ctx, const sss_frame_state* st, double 
     a.hit_m = hit_m;
     a.status = ctx->d_status;
     a.guard_out = guard_used;
+    a.fine_guard = st->fine_guard > 0 ? st->fine_guard : SSS_FINE_GUARD;
+    a.wait_ns = SSS_WAIT_LIMIT_NS;
 
     void* fn = (D == 3) ? (void*)k_frame<3> : (void*)k_frame<2>;
     int per_sm = 0;
@@ -616,5 +635,22 @@ extern "C" int sss_frame_scatter(sss_ctx* ctx, const sss_frame_state* st, const 
     p.mm = st->mas_m;
     k_frame_scatter<<<(m + 127) / 128, 128, 0, (cudaStream_t)stream>>>(p, slot, vals, m, st->dim, mode);
     SSS_LAUNCH_CHECK(ctx, "k_frame_scatter launch");
+    return SSS_OK;
+}
+
+// Runs the frame kernel's grid barrier with one CTA that never arrives (see
+// k_frame_barrier_selftest); the wait gives up after limit_s seconds.
+int sss_frame_barrier_selftest(sss_ctx* ctx, double limit_s, cudaStream_t s) {
+    void* scr = nullptr;
+    int rc = sss_scratch(ctx, 256, &scr);
+    if (rc) return rc;
+    FrameArgs a;
+    memset(&a, 0, sizeof(a));
+    a.gbar = (unsigned*)scr;
+    a.status = ctx->d_status;
+    a.wait_ns = (uint64_t)(limit_s * 1e9);
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(a.gbar, 0, 2 * sizeof(unsigned), s));
+    k_frame_barrier_selftest<<<2, FR_NT, 0, s>>>(a);
+    SSS_LAUNCH_CHECK(ctx, "k_frame_barrier_selftest");
     return SSS_OK;
 }

@@ -109,6 +109,24 @@ __global__ void k_cic_gather_2d(const double* __restrict__ px, const double* __r
     ay[p] = out[1];
 }
 
+// bilinear read of one caller-held N x N field with row stride ld (_cic_gather, pm_kernel.py:93-107)
+__global__ void k_cic_gather_field_2d(const double* __restrict__ px, const double* __restrict__ py, long long np_,
+                                      int n, long long ld, double x0, double y0, double h,
+                                      const double* __restrict__ f, double* __restrict__ out) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np_) return;
+    int i, j;
+    double tx, ty;
+    cic2(px[p], py[p], x0, y0, h, n, i, j, tx, ty);
+    const double ux = __dsub_rn(1.0, tx), uy = __dsub_rn(1.0, ty);
+    const long long c00 = (long long)i * ld + j, c10 = c00 + ld, c01 = c00 + 1, c11 = c10 + 1;
+    const double t00 = __dmul_rn(__dmul_rn(f[c00], ux), uy);
+    const double t10 = __dmul_rn(__dmul_rn(f[c10], tx), uy);
+    const double t01 = __dmul_rn(__dmul_rn(f[c01], ux), ty);
+    const double t11 = __dmul_rn(__dmul_rn(f[c11], tx), ty);
+    out[p] = __dadd_rn(__dadd_rn(__dadd_rn(t00, t10), t01), t11);
+}
+
 // min/max of x and y: out[0..3] = xmin, xmax, ymin, ymax (two-pass: blocks -> final)
 __global__ void k_bbox_2d(const double* __restrict__ x, const double* __restrict__ y, long long n,
                           double* __restrict__ part) {
@@ -321,6 +339,20 @@ extern "C" int sss_pm2d_gather(sss_pm2d* p, const double* px, const double* py, 
     k_cic_gather_2d<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(px, py, n, p->n, x0, y0, h, p->fieldx,
                                                                          p->fieldy, ax, ay);
     SSS_LAUNCH_CHECK(p->ctx, "k_cic_gather_2d");
+    return SSS_OK;
+}
+
+// One field read at (px, py) with the deposit's stencil (_cic_gather, pm_kernel.py:93-107).
+extern "C" int sss_pm2d_gather_field(sss_ctx* ctx, const double* field, int grid_n, int64_t ld, const double* px,
+                                     const double* py, int64_t n, double x0, double y0, double h, double* out,
+                                     void* stream) {
+    if (!ctx) return SSS_ERR_ARG;
+    if (grid_n < 2 || ld < grid_n || n < 0) return sss_set_err(ctx, SSS_ERR_ARG, "gather_field: bad sizes");
+    if (n == 0) return SSS_OK;
+    if (!field || !px || !py || !out) return sss_set_err(ctx, SSS_ERR_ARG, "gather_field: NULL");
+    k_cic_gather_field_2d<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(px, py, n, grid_n, ld, x0, y0, h,
+                                                                               field, out);
+    SSS_LAUNCH_CHECK(ctx, "k_cic_gather_field_2d");
     return SSS_OK;
 }
 

@@ -82,3 +82,33 @@ extern "C" int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops) 
     *tflops = flops / (best_ms * 1e-3) / 1e12;
     return SSS_OK;
 }
+
+namespace {
+
+// Self-test of the mbarrier wait the bulk-copy and tensor-core kernels use:
+// an mbarrier that expects two arrivals gets one, so the wait for its phase
+// runs out after limit_ns and records SSS_ERR_TIMEOUT.
+__global__ void k_mbar_selftest(uint64_t limit_ns, int* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        sss_mbar_init(&bar, 2);
+        sss_fence_mbar_init();
+        sss_mbar_arrive(&bar);
+        sss_mbar_wait_bounded(&bar, 0, status, limit_ns);
+    }
+}
+
+}  // namespace
+
+extern "C" int sss_selftest_wait(sss_ctx* ctx, int which, double limit_s, void* stream) {
+    if (!ctx) return SSS_ERR_ARG;
+    if (which < 0 || which > 2) return sss_set_err(ctx, SSS_ERR_ARG, "which must be 0, 1 or 2");
+    if (!(limit_s > 0.0 && limit_s <= 10.0)) return sss_set_err(ctx, SSS_ERR_ARG, "limit_s must be in (0, 10]");
+    SSS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (which == 1) return sss_frame_barrier_selftest(ctx, limit_s, s);
+    if (which == 2) return sss_stream_barrier_selftest(ctx, limit_s, s);
+    k_mbar_selftest<<<1, 32, 0, s>>>((uint64_t)(limit_s * 1e9), ctx->d_status);
+    SSS_LAUNCH_CHECK(ctx, "k_mbar_selftest");
+    return SSS_OK;
+}

@@ -33,6 +33,9 @@ int sss_cuda_err(sss_ctx* ctx, cudaError_t e, const char* what);
 // Ensure ctx->scratch holds at least `bytes` (256-byte aligned).
 int sss_scratch(sss_ctx* ctx, size_t bytes, void** out);
 int sss_counters(sss_ctx* ctx, size_t n, unsigned** out);
+// Bounded-wait self-tests (a wait that nothing completes; sss_selftest_wait).
+int sss_frame_barrier_selftest(sss_ctx* ctx, double limit_s, cudaStream_t s);
+int sss_stream_barrier_selftest(sss_ctx* ctx, double limit_s, cudaStream_t s);
 
 #define SSS_CUDA_TRY(ctx, call)                                   \
     do {                                                          \
@@ -61,6 +64,10 @@ __device__ __forceinline__ uint64_t sss_globaltimer() {
 
 __device__ __forceinline__ unsigned sss_smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void sss_mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(sss_smem_addr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void sss_mbar_init(uint64_t* bar, unsigned count) {
@@ -100,13 +107,13 @@ __device__ __forceinline__ bool sss_mbar_try_wait(uint64_t* bar, unsigned parity
 }
 
 // Bounded wait for phase `parity` of `bar`. Returns false (and records
-// SSS_ERR_TIMEOUT in *status) if the phase did not complete within the limit.
+// SSS_ERR_TIMEOUT in *status) if the phase did not complete within limit_ns.
 __device__ __forceinline__ bool sss_mbar_wait_bounded(uint64_t* bar, unsigned parity,
-                                                      int* status) {
+                                                      int* status, uint64_t limit_ns = SSS_WAIT_LIMIT_NS) {
     if (sss_mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = sss_globaltimer();
     while (!sss_mbar_try_wait(bar, parity)) {
-        if (sss_globaltimer() - t0 > SSS_WAIT_LIMIT_NS) {
+        if (sss_globaltimer() - t0 > limit_ns) {
             atomicExch(status, SSS_ERR_TIMEOUT);
             return false;
         }

@@ -285,7 +285,8 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 }
 
 // false: a wait ran out here or in another block (the caller returns)
-__device__ __forceinline__ bool grid_barrier(Ctl* ctl, unsigned& epoch, int* s_bad) {
+__device__ __forceinline__ bool grid_barrier(Ctl* ctl, unsigned& epoch, int* s_bad,
+                                             unsigned max_polls = BARRIER_POLLS) {
     ++epoch;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -296,7 +297,7 @@ __device__ __forceinline__ bool grid_barrier(Ctl* ctl, unsigned& epoch, int* s_b
         const unsigned target = epoch * gridDim.x;
         int bad = 0;
         for (unsigned polls = 0; ld_acquire_u32(&ctl->bar) < target; ++polls) {
-            if (polls >= BARRIER_POLLS || *(volatile int*)&ctl->err) {
+            if (polls >= max_polls || *(volatile int*)&ctl->err) {
                 atomicExch(&ctl->err, SSS_ERR_TIMEOUT);
                 bad = 1;
                 break;
@@ -1399,4 +1400,31 @@ extern "C" int sss_stream_sample_batch(sss_ctx* ctx, int64_t n, int k, const flo
                                        int64_t* n_sel, void* stream) {
     return sample_batch(ctx, n, k, x, y, kill_t, t_cut, is_ast, injected, box, log_zoom, budget, sel, qx_out, qy_out,
                         n_sel, stream);
+}
+
+namespace {
+
+// Self-test of the sample kernel's grid barrier: block 1 leaves without
+// arriving, so block 0's wait runs out after max_polls polls and records
+// SSS_ERR_TIMEOUT.
+__global__ void k_sample_barrier_selftest(Ctl* ctl, unsigned max_polls, int* status) {
+    __shared__ int bad;
+    unsigned epoch = 0;
+    if (blockIdx.x != 0) return;
+    if (!grid_barrier(ctl, epoch, &bad, max_polls) && threadIdx.x == 0)
+        atomicCAS(status, SSS_OK, *(volatile int*)&ctl->err);
+}
+
+}  // namespace
+
+int sss_stream_barrier_selftest(sss_ctx* ctx, double limit_s, cudaStream_t st) {
+    void* scr = nullptr;
+    int rc = sss_scratch(ctx, sizeof(Ctl) + 256, &scr);
+    if (rc) return rc;
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(scr, 0, sizeof(Ctl), st));
+    const double polls = limit_s / 32e-9;              // at least 32 ns a poll
+    const unsigned max_polls = polls < 1.0 ? 1u : (polls > 4e9 ? 4000000000u : (unsigned)polls);
+    k_sample_barrier_selftest<<<2, SAMPLE_THREADS, 0, st>>>((Ctl*)scr, max_polls, ctx->d_status);
+    SSS_LAUNCH_CHECK(ctx, "k_sample_barrier_selftest");
+    return SSS_OK;
 }

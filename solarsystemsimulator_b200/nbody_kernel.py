@@ -33,6 +33,7 @@ G_AU = 4 * np.pi * np.pi
 SOFTENING = 1e-6
 MAX_SUB_DT_YEARS = 0.5 / 365.25
 MAX_SUB_STEPS_PER_FRAME = 100_000
+FINE_STEPS_MAX = 8000          # iteration guard of the hot asteroids' fine loop (nbody_kernel.py:424)
 YOSHIDA_W1 = 1.0 / (2.0 - 2.0 ** (1.0 / 3.0))
 YOSHIDA_W0 = -(2.0 ** (1.0 / 3.0)) / (2.0 - 2.0 ** (1.0 / 3.0))
 SUB_SAMPLES = 8
@@ -72,7 +73,12 @@ class NBodyCuda:
     """Few massive + many asteroid bodies, resident on one GPU."""
 
     def __init__(self, devices, m_sub=SUB_SAMPLES, *, G: float = G_AU, softening: float = SOFTENING,
-                 max_sub_dt: float = MAX_SUB_DT_YEARS, max_sub_steps: int = MAX_SUB_STEPS_PER_FRAME):
+                 max_sub_dt: float = MAX_SUB_DT_YEARS, max_sub_steps: int = MAX_SUB_STEPS_PER_FRAME,
+                 max_fine_steps: int = FINE_STEPS_MAX, strict_guard: bool = False):
+        """Additive keywords beyond the reference's: max_fine_steps is the
+        iteration guard of a hot asteroid's fine loop (the reference's fixed
+        8000); strict_guard=True turns a guard that ran out into an SSSError
+        (SSS_ERR_GUARD) instead of a RuntimeWarning."""
         if isinstance(devices, int):
             devices = [devices]
         if not devices or len(devices) > G_MAX:
@@ -88,6 +94,10 @@ class NBodyCuda:
         self.softening = float(softening)
         self.max_sub_dt = float(max_sub_dt)
         self.max_sub_steps = int(max_sub_steps)
+        if max_fine_steps < 1:
+            raise ValueError("max_fine_steps must be >= 1")
+        self.max_fine_steps = int(max_fine_steps)
+        self.strict_guard = bool(strict_guard)
         self._ctx = _lib.context(self.device)
 
     def name(self) -> str:
@@ -182,6 +192,7 @@ class NBodyCuda:
         c.softening = self.softening
         c.max_sub_dt = self.max_sub_dt
         c.max_sub_steps = self.max_sub_steps
+        c.fine_guard = self.max_fine_steps
         c.w1 = YOSHIDA_W1
         c.w0 = YOSHIDA_W0
         return c
@@ -213,9 +224,18 @@ class NBodyCuda:
         (nbody_kernel.py:783-934)."""
         snap = self.step_batch_device(st, dt_raster_years, k)
         out = snap.reshape(k, -1).cpu().numpy()
-        self._ctx.status(_lib.stream_handle(self.device))
-        if int(st["guard"].item()) >= self.max_sub_steps:
-            warnings.warn("MAX_SUB_STEPS_PER_FRAME reached: the batch stopped advancing", RuntimeWarning)
+        rc = self._ctx.status_code(_lib.stream_handle(self.device))
+        if rc == _lib.SSS_ERR_GUARD:
+            # the reference stops the interval where its guard runs out and goes on
+            # (nbody_kernel.py:248-250, :424); this build reports it
+            st["guard_exhausted"] = st.get("guard_exhausted", 0) + 1
+            msg = ("a step guard ran out (MAX_SUB_STEPS_PER_FRAME or the fine-loop limit): "
+                   "the batch did not cover its interval")
+            if self.strict_guard:
+                raise _lib.SSSError(rc, msg)
+            warnings.warn(msg, RuntimeWarning)
+        else:
+            self._ctx.check(rc)
         st["sub"] = self._collect_sub(st, k)
         st["hits"] = self._collect_hits(st)
         return out

@@ -136,6 +136,26 @@ def gather_accel(ax_grid, ay_grid, px, py, grid_n, x0, y0, h, device: int = 0):
     return ax, ay
 
 
+def _cic_gather(feld, gx, gy, grid_n, x0, y0, h, device: int = 0):
+    """The value of the (grid_n, grid_n) field `feld` at (gx, gy) with the
+    deposit's bilinear stencil (pm_kernel.py:93-107). Returns an f64 device
+    tensor."""
+    dev = torch.device("cuda", device)
+    f = _f64(feld, dev)
+    if f.dim() != 2 or f.shape[0] != grid_n or f.shape[1] != grid_n:
+        raise ValueError(f"feld must be ({grid_n}, {grid_n})")
+    x, y = _f64(gx, dev), _f64(gy, dev)
+    if x.numel() != y.numel():
+        raise ValueError("gx and gy must have the same length")
+    out = torch.empty_like(x)
+    ctx = _lib.context(device)
+    with torch.cuda.device(device):
+        ctx.check(ctx.lib.sss_pm2d_gather_field(ctx.ptr, f.data_ptr(), int(grid_n), f.stride(0), x.data_ptr(),
+                                                y.data_ptr(), x.numel(), float(x0), float(y0), float(h),
+                                                out.data_ptr(), ctypes.c_void_p(_lib.stream_handle(device))))
+    return out
+
+
 def pm_accelerations(gx, gy, gm, grid_n, x0, y0, h, eps2, G: float = G_AU, kernels=None, device: int = 0):
     """Acceleration of each mass via PM (pm_kernel.py:157-163)."""
     dev = torch.device("cuda", device)

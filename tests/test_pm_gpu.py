@@ -33,6 +33,34 @@ def test_grid_density_and_forces_match_reference(load_golden):
     assert fx.shape == (n, n) and fy.shape == (n, n)
 
 
+def test_cic_gather_drop_in(load_golden):
+    """_cic_gather(feld, gx, gy, grid_n, x0, y0, h) (pm_kernel.py:93-107) on a
+    field the caller holds: bit-identical to the oracle's restatement on a
+    random field (points inside the grid, on its clip edges and outside it),
+    and on the force field the same values gather_accel returns."""
+    from oracle import pm as opm
+    pk = _pk()
+    rng = np.random.default_rng(17)
+    n, x0, y0, h = 96, -3.0, 2.0, 0.05
+    feld = rng.normal(0, 1, (n, n))
+    px = x0 + rng.uniform(-0.5, n + 0.5, 5000) * h
+    py = y0 + rng.uniform(-0.5, n + 0.5, 5000) * h
+    px[:4] = [x0, x0 + (n - 1) * h, x0 + (n - 2) * h, x0 + 10.25 * h]
+    got = pk._cic_gather(feld, px, py, n, x0, y0, h).cpu().numpy()
+    assert np.array_equal(got, opm.cic_gather(feld, px, py, n, x0, y0, h))
+    # a non-contiguous field (a crop) is accepted too
+    big = rng.normal(0, 1, (n + 8, n + 8))
+    got = pk._cic_gather(torch.as_tensor(big).cuda()[:n, :n], px, py, n, x0, y0, h).cpu().numpy()
+    assert np.array_equal(got, opm.cic_gather(big[:n, :n], px, py, n, x0, y0, h))
+    g = load_golden("pm2d_n2000_g128.npz")
+    m = int(g["grid_n"])
+    x0, y0, h = float(g["x0"]), float(g["y0"]), float(g["h"])
+    fx, fy = pk.pm_force_field(g["x"], g["y"], g["m"], m, x0, y0, h, float(g["eps2"]))
+    ax, ay = pk.gather_accel(fx, fy, g["x"], g["y"], m, x0, y0, h)
+    assert torch.equal(pk._cic_gather(fx, g["x"], g["y"], m, x0, y0, h), ax)
+    assert torch.equal(pk._cic_gather(fy, g["x"], g["y"], m, x0, y0, h), ay)
+
+
 def test_kdk_matches_reference(load_golden):
     pk = _pk()
     g = load_golden("pm2d_kdk_n1500.npz")
