@@ -171,6 +171,10 @@ typedef struct sss_frame_state {
     int      massless_asteroids;  /* 1: every asteroid mass is 0 (no back-reaction) */
     int      fine_guard;          /* iteration limit of a hot asteroid's fine loop
                                      (0 = SSS_FINE_GUARD, the reference's 8000) */
+    int      pair_f32;            /* 1: asteroid x massive pair forces of calm asteroids
+                                     and the back-reaction in f32 (offsets formed in f64,
+                                     f32 rsqrt, sums in f64); hot asteroids' fine loops and
+                                     massive x massive pairs stay f64. 0: all f64 */
 } sss_frame_state;
 #define SSS_FINE_GUARD 8000
 
@@ -290,6 +294,24 @@ int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const float* y, 
                        const double* real_r, const double* mass, const int* hits, int64_t n_hits, double dt_y,
                        double e, int* pairs_out, int64_t* touched_out, double* deltas_out, int64_t* n_act,
                        int64_t* n_touched, void* stream);
+/* Fragmentation of fast asteroid x asteroid impacts (no counterpart in the
+ * reference's producer, which only detects a body x body shatter at 1.5
+ * v_esc, film_producer.py:801-822, and leaves the fragments to its client's
+ * shatter(), index.html:7705-7745). For each of the n_pairs active bounce
+ * pairs (int32 (a, b), e.g. sss_collide_bounce's pairs_out) in order whose
+ * impact speed |v_b - v_a| >= factor * sqrt(2 G (m_a + m_b) / (r_a + r_b))
+ * (and m_a + m_b > 0): parents_out receives (a, b) and frags_out n_frag
+ * records (x, y, vx, vy, m, r) f64: equal masses, radii keeping the volume,
+ * positions on a ring of radius r_a + r_b about the centre of mass,
+ * velocities the centre's plus a scatter of speed v_imp (0.25 + 0.35 U) at
+ * angle 2 pi k / n_frag + 0.6 (U - 1/2) with its mean removed (mass and
+ * momentum conserved); U from SplitMix64 of (seed, a, b, k). factor 0 turns
+ * it off. *n_events (host) receives the count; SSS_ERR_CAPACITY beyond cap.
+ * Synchronous. */
+int sss_collide_fragment(sss_ctx* ctx, int64_t n, const float* x, const float* y, const float* vx,
+                         const float* vy, const double* real_r, const double* mass, const int* pairs,
+                         int64_t n_pairs, double G, double factor, int n_frag, uint64_t seed, int* parents_out,
+                         double* frags_out, int64_t cap, int64_t* n_events, void* stream);
 
 /* ------------------------------------------------------- film ring slots
  *

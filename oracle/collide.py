@@ -257,3 +257,59 @@ def apply_merges(sample, n, pairs, runaways, mass, vis, real_r, is_ast, is_star_
             deact.append(j)
             events.append((0xFFFFFFFF, j, 0.0, 2, 0.0, float(sx[j]), float(sy[j])))
     return events, states, deact, None
+
+
+def _frag_uniform(seed, a, b, k, j):
+    """SplitMix64 of (seed, a, b, fragment k, draw j) -> [0, 1) f64, the
+    device generator of sss_collide_fragment."""
+    M = (1 << 64) - 1
+    h = (seed ^ ((a * 0x9E3779B97F4A7C15) & M) ^ ((b * 0xC2B2AE3D27D4EB4F) & M)) & M
+    h = (h + (2 * k + j + 1) * 0xD6E8FEB86659FD93) & M
+    h ^= h >> 30
+    h = (h * 0xBF58476D1CE4E5B9) & M
+    h ^= h >> 27
+    h = (h * 0x94D049BB133111EB) & M
+    h ^= h >> 31
+    return float(h >> 11) * 2.0 ** -53
+
+
+def fragment_events(x, y, vx, vy, real_r, mass, pairs, G, factor, seed, n_frag=5):
+    """Fragmentation of fast impacts among the active bounce pairs, in f64
+    (the construction of the reference client's shatter(), index.html:
+    7705-7745, with a seeded generator): [(a, b, fragments (n_frag, 6) of
+    x, y, vx, vy, m, r)] in pair order."""
+    out = []
+    if factor <= 0:
+        return out
+    x, y, vx, vy = (np.asarray(v, np.float32) for v in (x, y, vx, vy))
+    rr = np.asarray(real_r, np.float64)
+    mass = np.asarray(mass, np.float64)
+    for a, b in pairs:
+        a, b = int(a), int(b)
+        ma, mb = mass[a], mass[b]
+        mt = ma + mb
+        if not mt > 0.0:
+            continue
+        dvx = float(vx[b]) - float(vx[a])
+        dvy = float(vy[b]) - float(vy[a])
+        v_imp = np.sqrt(dvx * dvx + dvy * dvy)
+        touch = max(rr[a] + rr[b], 1e-12)
+        if not v_imp >= factor * np.sqrt(2.0 * G * mt / touch):
+            continue
+        cx = (ma * float(x[a]) + mb * float(x[b])) / mt
+        cy = (ma * float(y[a]) + mb * float(y[b])) / mt
+        cvx = (ma * float(vx[a]) + mb * float(vx[b])) / mt
+        cvy = (ma * float(vy[a]) + mb * float(vy[b])) / mt
+        ring = rr[a] + rr[b]
+        rf = np.cbrt((rr[a] ** 3 + rr[b] ** 3) / n_frag)
+        ang = [2.0 * np.pi * k / n_frag + (_frag_uniform(seed, a, b, k, 0) - 0.5) * 0.6 for k in range(n_frag)]
+        spd = [v_imp * (0.25 + 0.35 * _frag_uniform(seed, a, b, k, 1)) for k in range(n_frag)]
+        mx = sum(np.cos(t) * s for t, s in zip(ang, spd)) / n_frag
+        my = sum(np.sin(t) * s for t, s in zip(ang, spd)) / n_frag
+        f = np.empty((n_frag, 6))
+        for k in range(n_frag):
+            th = 2.0 * np.pi * k / n_frag
+            f[k] = (cx + np.cos(th) * ring, cy + np.sin(th) * ring, cvx + (np.cos(ang[k]) * spd[k] - mx),
+                    cvy + (np.sin(ang[k]) * spd[k] - my), mt / n_frag, rf)
+        out.append((a, b, f))
+    return out

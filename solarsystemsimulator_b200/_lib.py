@@ -56,7 +56,7 @@ class FrameState(ctypes.Structure):
         ("G", ctypes.c_double), ("softening", ctypes.c_double), ("max_sub_dt", ctypes.c_double),
         ("max_sub_steps", ctypes.c_int), ("w1", ctypes.c_double), ("w0", ctypes.c_double),
         ("massless_asteroids", ctypes.c_int),
-        ("fine_guard", ctypes.c_int),
+        ("fine_guard", ctypes.c_int), ("pair_f32", ctypes.c_int),
     ]
 
 
@@ -119,6 +119,9 @@ SIGNATURES = {
     "sss_collide_sweep": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                          ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _c_i64, _dp, _c_i64,
                                          ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64), _vp]),
+    "sss_collide_fragment": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_uint64, _dp, _dp, _c_i64,
+                                            ctypes.POINTER(_c_i64), _vp]),
     "sss_collide_bounce": (ctypes.c_int, [_vp, _c_i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _c_i64, ctypes.c_double,
                                           ctypes.c_double, _dp, _dp, _dp, ctypes.POINTER(_c_i64),
                                           ctypes.POINTER(_c_i64), _vp]),

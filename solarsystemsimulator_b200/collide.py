@@ -6,6 +6,8 @@ analysis of the reference's film producer with its array parts on the device.
     res = cr.bounce_deltas(g, hits_dev, n_hits, dt_y)    # bounce_deltas, :916-1019
     events, shatter = cr.apply_merges(sim, st, sample, pairs, runaways, k_ev)   # apply_merges, :781-861
     cr.apply_bounce(sim, st, res)                        # apply_bounce, :1021-1040 (deltas on the device)
+    parents, frags = cr.fragment(g, res, FRAG_V_ESC, seed)  # fast impacts break up (no reference counterpart)
+    cr.apply_fragments(sim, st, parents, frags)
 
 `g` is the sample on the device as f32 rows (4, n) [x|y|vx|vy] (the row the
 detection card holds); `sample` the same row on the host (f32, 4n). The
@@ -26,6 +28,8 @@ from . import _lib
 G_AU = 4 * np.pi * np.pi
 BOUNCE_E = 0.6            # restitution (film_producer.py:47)
 SHATTER_V_ESC = 1.5       # body x body impacts at >= 1.5 v_esc stop the film for the client's shatter
+N_FRAG = 5                # fragments of a fragmenting impact (the client's shatter(), index.html:7705-7745)
+FRAG_V_ESC = 5.0          # asteroid x asteroid impacts at >= 5 v_esc fragment (the asteroid-cloud configuration)
 
 
 class CollisionResponse:
@@ -171,6 +175,67 @@ class CollisionResponse:
                 vis[j] = 0
                 events.append((0xFFFFFFFF, j, 0.0, 2, 0.0, float(sx[j]), float(sy[j])))
         return events, None
+
+    def fragment(self, g: torch.Tensor, res, factor: float, seed: int, n_frag: int = N_FRAG):
+        """Fragmenting impacts among the active bounce pairs `res` (the
+        result of bounce_deltas): impact speed >= factor x the pair's escape
+        speed (sss_collide_fragment). Returns (parents int64 (E, 2), fragments
+        f64 (E, n_frag, 6) of x, y, vx, vy, m, r) as host arrays."""
+        empty = (np.zeros((0, 2), np.int64), np.zeros((0, n_frag, 6)))
+        if res is None or factor <= 0:
+            return empty
+        hi, hj = res[0], res[1]
+        k = int(hi.numel())
+        if k == 0:
+            return empty
+        g = g.contiguous()
+        pairs = torch.stack([hi, hj], 1).to(torch.int32).contiguous()
+        parents = torch.empty((k, 2), dtype=torch.int32, device=self.dev)
+        frags = torch.empty((k, n_frag, 6), dtype=torch.float64, device=self.dev)
+        ne = ctypes.c_int64()
+        with torch.cuda.device(self.device):
+            rc = self.ctx.lib.sss_collide_fragment(
+                self.ctx.ptr, self.n, g[0].data_ptr(), g[1].data_ptr(), g[2].data_ptr(), g[3].data_ptr(),
+                self.d_rr.data_ptr(), self.d_mass.data_ptr(), pairs.data_ptr(), k, self.G, float(factor),
+                int(n_frag), int(seed) & ((1 << 64) - 1), parents.data_ptr(), frags.data_ptr(), k,
+                ctypes.byref(ne), self._s())
+        self.ctx.check(rc)
+        e = ne.value
+        return parents[:e].cpu().numpy().astype(np.int64), frags[:e].cpu().numpy()
+
+    def apply_fragments(self, sim, st, parents, frags):
+        """Replace each fragmenting pair by its fragments (after the bounce
+        deltas of the sample were applied: the parents' states are set anew).
+        Fragments 0 and 1 take the parents' slots, the others free asteroid
+        slots (hidden asteroids, lowest index first); an event without
+        enough free slots is left out (its bounce stands). Returns
+        (events (a, b, fragment mass, 3, 0.0, x, y), slots used per event,
+        events left out)."""
+        events, used, skipped = [], [], 0
+        if len(parents) == 0:
+            return events, used, skipped
+        n_frag = frags.shape[1]
+        free = list(np.flatnonzero((self.vis == 0) & self.is_ast)[::-1])       # pop() gives the lowest
+        idx, vals, radii = [], [], []
+        for (a, b), f in zip(parents, frags):
+            if len(free) < n_frag - 2:
+                skipped += 1
+                continue
+            slots = [int(a), int(b)] + [int(free.pop()) for _ in range(n_frag - 2)]
+            for s_, row in zip(slots, f):
+                idx.append(s_)
+                vals.append([row[0], row[1], row[2], row[3], row[4]] if st["dim"] == 2 else
+                            [row[0], row[1], 0.0, row[2], row[3], 0.0, row[4]])
+                radii.append(row[5])
+                self.mass[s_] = row[4]
+                self.real_r[s_] = row[5]
+                self.vis[s_] = 1
+            used.append(slots)
+            events.append((int(a), int(b), float(f[0, 4]), 3, 0.0, float(f[:, 0].mean()), float(f[:, 1].mean())))
+        if idx:
+            sim.set_asteroids(st, idx, vals, radii)
+            self.refresh()
+        return events, used, skipped
 
     def apply_bounce(self, sim, st, res) -> int:
         """Add the bounce deltas to the simulation on the device (apply_bounce,

@@ -551,3 +551,153 @@ extern "C" int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const
     *n_touched = tot[1];
     return SSS_OK;
 }
+
+// ------------------------------------------------------------ fragmentation
+//
+// Asteroid x asteroid impacts far above the pair's escape speed break both
+// bodies into n_frag fragments (the asteroid-cloud configuration: above 5 x
+// v_esc). The reference's producer only detects a shatter (body x body at
+// 1.5 v_esc, film_producer.py:801-822) and leaves the fragments to its
+// client's shatter() (index.html:7705-7745): equal fragments on a ring of
+// radius r_a + r_b about the centre of mass, scattered velocities with their
+// mean removed so that mass and momentum are conserved. Here the same
+// construction runs on the device for every active bounce pair whose impact
+// speed |v_b - v_a| >= factor * sqrt(2 G (m_a + m_b) / (r_a + r_b)), with the
+// client's random numbers replaced by a counter-based generator (SplitMix64
+// of the seed, the two body indices and the fragment number), so a film is
+// reproducible. Radii keep the volume: r_f = cbrt((r_a^3 + r_b^3) / n_frag).
+
+namespace {
+
+constexpr int FRAG_NT = 128;
+
+__device__ __forceinline__ double frag_uniform(unsigned long long seed, long long a, long long b, int k, int j) {
+    unsigned long long h = seed ^ ((unsigned long long)a * 0x9E3779B97F4A7C15ull) ^
+                           ((unsigned long long)b * 0xC2B2AE3D27D4EB4Full);
+    h += (unsigned long long)(2 * k + j + 1) * 0xD6E8FEB86659FD93ull;
+    h ^= h >> 30;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 27;
+    h *= 0x94D049BB133111EBull;
+    h ^= h >> 31;
+    return (double)(h >> 11) * 0x1.0p-53;
+}
+
+struct FragIn {
+    const float *x, *y, *vx, *vy;
+    const double *rr, *mass;
+    double G, factor;
+    unsigned long long seed;
+    int n_frag;
+};
+
+__device__ __forceinline__ bool frag_test(const FragIn& in, long long a, long long b) {
+    const double ma = in.mass[a], mb = in.mass[b];
+    const double mt = ma + mb;
+    if (!(mt > 0.0) || !(in.factor > 0.0)) return false;
+    const double dvx = (double)in.vx[b] - (double)in.vx[a];
+    const double dvy = (double)in.vy[b] - (double)in.vy[a];
+    const double v_imp = sqrt(dvx * dvx + dvy * dvy);
+    double touch = in.rr[a] + in.rr[b];
+    if (touch < 1e-12) touch = 1e-12;
+    const double v_esc = sqrt(2.0 * in.G * mt / touch);
+    return v_imp >= in.factor * v_esc;
+}
+
+__global__ void __launch_bounds__(FRAG_NT) k_frag_flags(const FragIn in, const int* __restrict__ pairs, long long np_,
+                                                        long long* __restrict__ flags) {
+    const long long t = (long long)blockIdx.x * FRAG_NT + threadIdx.x;
+    if (t >= np_) return;
+    flags[t] = frag_test(in, pairs[2 * t], pairs[2 * t + 1]) ? 1 : 0;
+}
+
+// One thread per fragmenting pair: its n_frag fragments (x, y, vx, vy, m, r).
+__global__ void __launch_bounds__(FRAG_NT) k_frag_write(const FragIn in, const int* __restrict__ pairs, long long np_,
+                                                        const long long* __restrict__ flags,
+                                                        const long long* __restrict__ pos, long long cap,
+                                                        int* __restrict__ parents, double* __restrict__ frags) {
+    const long long t = (long long)blockIdx.x * FRAG_NT + threadIdx.x;
+    if (t >= np_ || !flags[t]) return;
+    const long long q = pos[t];
+    if (q >= cap) return;
+    const long long a = pairs[2 * t], b = pairs[2 * t + 1];
+    parents[2 * q] = (int)a;
+    parents[2 * q + 1] = (int)b;
+    const double ma = in.mass[a], mb = in.mass[b], mt = ma + mb;
+    const double xa = in.x[a], ya = in.y[a], xb = in.x[b], yb = in.y[b];
+    const double vxa = in.vx[a], vya = in.vy[a], vxb = in.vx[b], vyb = in.vy[b];
+    const double cx = (ma * xa + mb * xb) / mt, cy = (ma * ya + mb * yb) / mt;
+    const double cvx = (ma * vxa + mb * vxb) / mt, cvy = (ma * vya + mb * vyb) / mt;
+    const double dvx = vxb - vxa, dvy = vyb - vya;
+    const double v_imp = sqrt(dvx * dvx + dvy * dvy);
+    const int N = in.n_frag;
+    const double ring = in.rr[a] + in.rr[b];
+    const double rf = cbrt((in.rr[a] * in.rr[a] * in.rr[a] + in.rr[b] * in.rr[b] * in.rr[b]) / N);
+    const double mf = mt / N;
+    double mx = 0.0, my = 0.0;
+    for (int k = 0; k < N; ++k) {
+        const double ang = 2.0 * M_PI * k / N + (frag_uniform(in.seed, a, b, k, 0) - 0.5) * 0.6;
+        const double spd = v_imp * (0.25 + 0.35 * frag_uniform(in.seed, a, b, k, 1));
+        mx += cos(ang) * spd;
+        my += sin(ang) * spd;
+    }
+    mx /= N;
+    my /= N;
+    double* f = frags + q * (long long)N * 6;
+    for (int k = 0; k < N; ++k) {
+        const double ang = 2.0 * M_PI * k / N + (frag_uniform(in.seed, a, b, k, 0) - 0.5) * 0.6;
+        const double spd = v_imp * (0.25 + 0.35 * frag_uniform(in.seed, a, b, k, 1));
+        const double th = 2.0 * M_PI * k / N;
+        f[6 * k + 0] = cx + cos(th) * ring;
+        f[6 * k + 1] = cy + sin(th) * ring;
+        f[6 * k + 2] = cvx + (cos(ang) * spd - mx);
+        f[6 * k + 3] = cvy + (sin(ang) * spd - my);
+        f[6 * k + 4] = mf;
+        f[6 * k + 5] = rf;
+    }
+}
+
+}  // namespace
+
+extern "C" int sss_collide_fragment(sss_ctx* ctx, int64_t n, const float* x, const float* y, const float* vx,
+                                    const float* vy, const double* real_r, const double* mass, const int* pairs,
+                                    int64_t n_pairs, double G, double factor, int n_frag, uint64_t seed,
+                                    int* parents_out, double* frags_out, int64_t cap, int64_t* n_events,
+                                    void* stream) {
+    if (!ctx) return SSS_ERR_ARG;
+    if (!n_events) return sss_set_err(ctx, SSS_ERR_ARG, "NULL count pointer");
+    *n_events = 0;
+    if (n < 0 || n_pairs < 0 || cap < 0) return sss_set_err(ctx, SSS_ERR_ARG, "negative size");
+    if (n_frag < 2 || n_frag > 16) return sss_set_err(ctx, SSS_ERR_ARG, "n_frag must be in [2, 16]");
+    if (!(factor >= 0.0)) return sss_set_err(ctx, SSS_ERR_ARG, "factor must be >= 0");
+    if (n_pairs == 0 || factor == 0.0) return SSS_OK;
+    if (!x || !y || !vx || !vy || !real_r || !mass || !pairs || (cap > 0 && (!parents_out || !frags_out)))
+        return sss_set_err(ctx, SSS_ERR_ARG, "NULL array");
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t off = 0;
+    const size_t o_flags = off; off += al((size_t)n_pairs * 8);
+    const size_t o_pos = off; off += al((size_t)n_pairs * 8);
+    const size_t o_scan = off; off += al(scan_scratch(n_pairs) * 8);
+    void* scr = nullptr;
+    int rc = sss_scratch(ctx, off, &scr);
+    if (rc) return rc;
+    char* b = (char*)scr;
+    long long* flags = (long long*)(b + o_flags);
+    long long* pos = (long long*)(b + o_pos);
+    long long* scan = (long long*)(b + o_scan);
+    FragIn in{x, y, vx, vy, real_r, mass, G, factor, (unsigned long long)seed, n_frag};
+    k_frag_flags<<<nblk(n_pairs, FRAG_NT), FRAG_NT, 0, st>>>(in, pairs, n_pairs, flags);
+    SSS_LAUNCH_CHECK(ctx, "k_frag_flags");
+    SSS_CUDA_TRY(ctx, exclusive_scan(flags, pos, n_pairs, scan, st));
+    k_frag_write<<<nblk(n_pairs, FRAG_NT), FRAG_NT, 0, st>>>(in, pairs, n_pairs, flags, pos, cap, parents_out,
+                                                             frags_out);
+    SSS_LAUNCH_CHECK(ctx, "k_frag_write");
+    long long tot = 0;
+    const long long tiles = (n_pairs + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&tot, scan + tiles, 8, cudaMemcpyDeviceToHost, st));
+    SSS_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    *n_events = tot;
+    if (tot > cap) return sss_set_err(ctx, SSS_ERR_CAPACITY, "fragment: %lld events, capacity %lld", tot,
+                                      (long long)cap);
+    return SSS_OK;
+}

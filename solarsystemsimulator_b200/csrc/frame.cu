@@ -62,6 +62,7 @@ struct FrameArgs {
     int* status;
     int* guard_out;           // substeps used (written by CTA 0)
     int fine_guard;           // iteration limit of a hot asteroid's fine loop
+    int pair_f32;             // 1: asteroid x massive pair forces in f32 (calm asteroids, back-reaction)
     uint64_t wait_ns;         // limit of a grid-barrier wait
 };
 
@@ -131,6 +132,24 @@ __device__ __forceinline__ void massive_field(const FrameShared& s, const double
     }
 }
 
+// The f32-pair form (the asteroid-cloud configuration: FP32 pair forces with
+// FP64 state): the offset formed in f64 and rounded to f32, r^2, the f32
+// reciprocal square root and the pair factor in f32, the sum in f64.
+template <int D>
+__device__ __forceinline__ void massive_field_f32(const FrameShared& s, const double (*mpos)[M_MAX], int M,
+                                                  double G, double soft, const double* p, double* acc) {
+    for (int c = 0; c < D; ++c) acc[c] = 0.0;
+    const float Gf = (float)G, sf = (float)soft;
+    for (int k = 0; k < M; ++k) {
+        if (!s.mvis[k]) continue;
+        float dx[3], r2 = sf;
+        for (int c = 0; c < D; ++c) { dx[c] = (float)(mpos[c][k] - p[c]); r2 = fmaf(dx[c], dx[c], r2); }
+        const float inv = rsqrtf(r2);
+        const float f = Gf * (float)s.mm[k] * inv * inv * inv;
+        for (int c = 0; c < D; ++c) acc[c] += (double)(f * dx[c]);
+    }
+}
+
 // Same, massive positions interpolated between mx0 and mx at fraction al.
 template <int D>
 __device__ __forceinline__ void interp_field(const FrameShared& s, int M, double G, double soft, double al,
@@ -162,6 +181,17 @@ __device__ void back_partial(const FrameArgs& a, const FrameShared& s, int lo, i
         if (s.mvis[k]) {
             for (int i = lo + lane; i < hi; i += 32) {
                 if (!a.avis[i]) continue;
+                if (a.pair_f32) {
+                    float dx[3], r2 = (float)a.soft;
+                    for (int c = 0; c < D; ++c) {
+                        dx[c] = (float)(s.mx[c][k] - a.ax[c][i]);
+                        r2 = fmaf(dx[c], dx[c], r2);
+                    }
+                    const float inv = rsqrtf(r2);
+                    const float f = (float)a.G * (float)a.am[i] * inv * inv * inv;
+                    for (int c = 0; c < D; ++c) b[c] -= (double)(f * dx[c]);
+                    continue;
+                }
                 double dx[3], r2 = 0.0;
                 for (int c = 0; c < D; ++c) { dx[c] = s.mx[c][k] - a.ax[c][i]; r2 += dx[c] * dx[c]; }
                 r2 += a.soft;
@@ -357,7 +387,10 @@ __global__ void __launch_bounds__(FR_NT) k_frame(const FrameArgs a) {
     for (int i = lo + tid; i < hi; i += blockDim.x) {
         double p[3], acc[3] = {0.0, 0.0, 0.0};
         for (int c = 0; c < D; ++c) p[c] = a.ax[c][i];
-        if (a.avis[i]) massive_field<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
+        if (a.avis[i]) {
+            if (a.pair_f32) massive_field_f32<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
+            else massive_field<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
+        }
         for (int c = 0; c < D; ++c) a.aacc[c][i] = acc[c];
     }
     if (!back_reaction<D>(a, s, lo, hi, slot)) return;
@@ -433,7 +466,8 @@ __global__ void __launch_bounds__(FR_NT) k_frame(const FrameArgs a) {
                     if (!a.avis[i]) continue;
                     double p[3], acc[3];
                     for (int c = 0; c < D; ++c) p[c] = a.ax[c][i];
-                    massive_field<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
+                    if (a.pair_f32 && !a.hot[i]) massive_field_f32<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
+                    else massive_field<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
                     if (!a.hot[i]) {
                         for (int c = 0; c < D; ++c) {
                             a.av[c][i] += 0.5 * (a.aacc[c][i] + acc[c]) * dt;
@@ -589,6 +623,7 @@ extern "C" int sss_frame_launch(sss_ctx* ctx, const sss_frame_state* st, double 
     a.status = ctx->d_status;
     a.guard_out = guard_used;
     a.fine_guard = st->fine_guard > 0 ? st->fine_guard : SSS_FINE_GUARD;
+    a.pair_f32 = st->pair_f32 ? 1 : 0;
     a.wait_ns = SSS_WAIT_LIMIT_NS;
 
     void* fn = (D == 3) ? (void*)k_frame<3> : (void*)k_frame<2>;

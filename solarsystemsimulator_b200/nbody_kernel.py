@@ -74,11 +74,14 @@ class NBodyCuda:
 
     def __init__(self, devices, m_sub=SUB_SAMPLES, *, G: float = G_AU, softening: float = SOFTENING,
                  max_sub_dt: float = MAX_SUB_DT_YEARS, max_sub_steps: int = MAX_SUB_STEPS_PER_FRAME,
-                 max_fine_steps: int = FINE_STEPS_MAX, strict_guard: bool = False):
+                 max_fine_steps: int = FINE_STEPS_MAX, strict_guard: bool = False, pair_f32: bool = False):
         """Additive keywords beyond the reference's: max_fine_steps is the
         iteration guard of a hot asteroid's fine loop (the reference's fixed
         8000); strict_guard=True turns a guard that ran out into an SSSError
-        (SSS_ERR_GUARD) instead of a RuntimeWarning."""
+        (SSS_ERR_GUARD) instead of a RuntimeWarning; pair_f32=True evaluates
+        the asteroid x massive pair forces of calm asteroids and the
+        back-reaction in f32 (f64 state, f64 sums; hot asteroids and the
+        massive bodies' mutual forces stay f64)."""
         if isinstance(devices, int):
             devices = [devices]
         if not devices or len(devices) > G_MAX:
@@ -98,6 +101,7 @@ class NBodyCuda:
             raise ValueError("max_fine_steps must be >= 1")
         self.max_fine_steps = int(max_fine_steps)
         self.strict_guard = bool(strict_guard)
+        self.pair_f32 = bool(pair_f32)
         self._ctx = _lib.context(self.device)
 
     def name(self) -> str:
@@ -193,6 +197,7 @@ class NBodyCuda:
         c.max_sub_dt = self.max_sub_dt
         c.max_sub_steps = self.max_sub_steps
         c.fine_guard = self.max_fine_steps
+        c.pair_f32 = int(self.pair_f32)
         c.w1 = YOSHIDA_W1
         c.w0 = YOSHIDA_W0
         return c
@@ -328,6 +333,26 @@ class NBodyCuda:
         self._scatter(st, [idx], [vals], 2)
         if st["inv_kind"][idx] > 0:
             st["am_h"][st["inv_pos"][idx]] = mass
+
+    def set_asteroids(self, st: dict, idx, vals, radii) -> None:
+        """Set asteroids completely and make them visible: vals [m][2*dim+1]
+        (x, y, (z), vx, vy, (vz), mass) and contact radii [m] at original
+        indices idx (unique asteroids), in one scatter. The fragments of a
+        fragmenting impact take their parents' and free slots this way (no
+        reference counterpart: its client creates fragment bodies)."""
+        idx = np.asarray(idx, np.int64).ravel()
+        if len(idx) == 0:
+            return
+        if len(np.unique(idx)) != len(idx) or np.any(st["inv_kind"][idx] <= 0):
+            raise ValueError("set_asteroids: idx must be unique asteroid indices")
+        self._scatter(st, idx, vals, 2)
+        pos = st["inv_pos"][idx]
+        dev = torch.device("cuda", self.device)
+        p_t = torch.from_numpy(pos).to(dev)
+        st["ar"][p_t] = torch.from_numpy(np.asarray(radii, np.float64)).to(dev)
+        st["avis"][p_t] = 1
+        st["am_h"][pos] = np.asarray(vals, np.float64).reshape(len(idx), -1)[:, -1]
+        st["avis_h"][pos] = 1
 
     def set_radius(self, st: dict, idx: int, wert: float) -> None:
         """Contact radius of one body (nbody_kernel.py:1012-1025)."""

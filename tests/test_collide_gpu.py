@@ -272,3 +272,94 @@ def test_merges_match_reference_golden(load_golden, scene):
     assert np.array_equal(cr.mass, g["mass1"]) and np.array_equal(cr.vis, g["vis1"])
     assert np.array_equal(cr.real_r, g["rr1"])
     assert (sh is not None) == bool(int(g["shatter_flag"]))
+
+
+# ------------------------------------------------ fragmentation of fast impacts
+
+def _fast_impacts(seed=41, n=3000):
+    """A clump of small asteroids (2 g/cm^3) with random speeds: most bounce
+    pairs hit far above their escape speed, slow ones below it; some bodies
+    hidden (free slots for fragments)."""
+    rng = np.random.default_rng(seed)
+    x = (1.5 + rng.normal(0, 1e-4, n)).astype(np.float32)
+    y = rng.normal(0, 1e-4, n).astype(np.float32)
+    sp = 10 ** rng.uniform(-7, -2, n)                      # AU / yr: from below to far above v_esc
+    th = rng.uniform(0, 2 * np.pi, n)
+    vx, vy = (sp * np.cos(th)).astype(np.float32), (sp * np.sin(th)).astype(np.float32)
+    rr = 10 ** rng.uniform(-6.5, -5.5, n)
+    mass = (4.0 / 3.0) * np.pi * (rr * 1.495978707e13) ** 3 * 2.0 / 1.98847e33
+    vis = np.ones(n, np.uint8)
+    vis[rng.choice(n, n // 3, replace=False)] = 0
+    return np.stack([x, y, vx, vy]), rr, mass, vis
+
+
+def test_fragments_match_oracle_and_conserve():
+    from solarsystemsimulator_b200 import broadphase as bp
+    from solarsystemsimulator_b200.collide import CollisionResponse, FRAG_V_ESC, G_AU
+    g, rr, mass, vis = _fast_impacts()
+    n = g.shape[1]
+    ones = np.ones(n, np.uint8)
+    dt_y = 0.5 / 365.25
+    buf, k, _ = bp.bounce_hits_device(*g, dt_y, 1e-4, 2e-4 + 2 * float(rr.max()), rr=rr.astype(np.float32),
+                                      vis=vis)
+    cr = CollisionResponse(mass, rr, vis, ones, m_idx=np.zeros(0, np.int64))
+    gd = torch.as_tensor(g).cuda()
+    res = cr.bounce_deltas(gd, buf, k, dt_y)
+    assert res is not None
+    parents, frags = cr.fragment(gd, res, FRAG_V_ESC, seed=1234)
+    act = np.stack([res[0].cpu().numpy(), res[1].cpu().numpy()], 1)
+    ref = oc.fragment_events(*g, rr, mass, act, G_AU, FRAG_V_ESC, 1234)
+    assert 0 < len(ref) < len(act)                          # some pairs fragment, some only bounce
+    assert np.array_equal(parents, np.array([(a, b) for a, b, _ in ref]))
+    want = np.stack([f for _, _, f in ref])
+    scale = np.abs(want).max(axis=(0, 1))
+    assert np.all(np.abs(frags - want) <= 1e-12 * scale)
+    # mass and momentum of every event are those of its parents
+    for (a, b), f in zip(parents, frags):
+        mt = mass[a] + mass[b]
+        assert abs(f[:, 4].sum() - mt) <= 1e-15 * mt
+        for c, vc in ((2, 2), (3, 3)):
+            p0 = mass[a] * float(g[vc][a]) + mass[b] * float(g[vc][b])
+            assert abs((f[:, 4] * f[:, c]).sum() - p0) <= 1e-13 * mt * np.abs(f[:, c]).max()
+    # a different seed scatters differently; factor 0 turns it off
+    p2, f2 = cr.fragment(gd, res, FRAG_V_ESC, seed=99)
+    assert np.array_equal(p2, parents) and not np.array_equal(f2, frags)
+    assert len(cr.fragment(gd, res, 0.0, seed=1)[0]) == 0
+
+
+def test_fragments_enter_the_simulation():
+    from solarsystemsimulator_b200 import broadphase as bp
+    from solarsystemsimulator_b200.collide import CollisionResponse, FRAG_V_ESC
+    from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
+    g, rr, mass, vis = _fast_impacts(seed=42, n=2000)
+    n = g.shape[1]
+    is_ast = np.ones(n, np.uint8)
+    is_ast[0] = 0                                          # a star far away keeps the film's shape
+    x = g[0].astype(np.float64); y = g[1].astype(np.float64)
+    x[0], y[0] = 0.0, 0.0
+    mass = mass.copy(); mass[0] = 1.0
+    vis[0] = 1
+    gg = np.stack([x, y, g[2], g[3]]).astype(np.float32)
+    dt_y = 0.5 / 365.25
+    buf, k, _ = bp.bounce_hits_device(*gg, dt_y, 1e-4, 2e-4 + 2 * float(rr.max()), rr=rr.astype(np.float32),
+                                      is_ast=is_ast, vis=vis)
+    cr = CollisionResponse(mass, rr, vis, is_ast, m_idx=np.array([0]))
+    sim = NBodyCuda([0])
+    st = sim.load_state(x, y, gg[2].astype(np.float64), gg[3].astype(np.float64), mass, vis, is_ast, rr)
+    gd = torch.as_tensor(gg).cuda()
+    res = cr.bounce_deltas(gd, buf, k, dt_y)
+    cr.apply_bounce(sim, st, res)
+    parents, frags = cr.fragment(gd, res, FRAG_V_ESC, seed=7)
+    n_hidden = int(((vis == 0) & (is_ast != 0)).sum())
+    events, used, skipped = cr.apply_fragments(sim, st, parents, frags)
+    assert len(events) + skipped == len(parents) and len(events) > 0
+    assert skipped == max(0, len(parents) - n_hidden // 3)
+    out = sim.export_f64(st)
+    slots = np.array(used)
+    assert len(np.unique(slots)) == slots.size                 # every fragment has its own slot
+    for sl, f in zip(used, frags[:len(used)]):
+        assert np.array_equal(out[sl], f[:, 0]) and np.array_equal(out[n + np.array(sl)], f[:, 1])
+        assert np.array_equal(out[2 * n + np.array(sl)], f[:, 2])
+        assert np.all(cr.vis[sl] == 1) and np.array_equal(cr.mass[sl], f[:, 4])
+    # the fragments fly on with the rest
+    sim.step_batch(st, dt_y, 1)

@@ -162,7 +162,10 @@ def test_checkpoint_round_trip_selfgrav(precision):
 
 def test_checkpoint_round_trip_pm():
     """NBodyPM: the same round trip (the grid geometry and the force are
-    recomputed from the positions at load_state)."""
+    recomputed from the positions at load_state). The deposit adds f64
+    masses with atomics, as CuPy's bincount does, so two runs of the same
+    steps differ in the last bits: the bar is the PM parity bar, 1e-9 of the
+    state scale."""
     from solarsystemsimulator_b200 import pm_kernel as pk
     rng = np.random.default_rng(5)
     n = 2000
@@ -179,4 +182,8 @@ def test_checkpoint_round_trip_pm():
     c = pk.NBodyPM([0], grid_n=256)
     st_c = c.load_state(f[0:n], f[n:2 * n], f[2 * n:3 * n], f[3 * n:4 * n], m)
     c.step_batch(st_c, 0.01, 3)
-    assert np.array_equal(c.export_f64(st_c), a.export_f64(st))
+    ref = a.export_f64(st)
+    got = c.export_f64(st_c)
+    for q in range(4):
+        part = slice(q * n, (q + 1) * n)
+        assert np.abs(got[part] - ref[part]).max() <= 1e-9 * np.abs(ref[part]).max()

@@ -319,3 +319,29 @@ def test_argument_errors():
         sim.step_batch(st, 0.01, nk.K_MAX + 1)
     with pytest.raises(ValueError):
         nk.NBodyCuda(0, m_sub=nk.SUB_SAMPLES_MAX + 1)
+
+
+def test_f32_pair_forces_on_the_asteroid_clouds():
+    """pair_f32 (FP32 pair forces, FP64 state) on the asteroid-cloud
+    configuration's bodies (star, 7 planets, 5 clouds): the accelerations
+    against the f64 path within 1e-6 median and 1e-4 maximum relative error,
+    and one 0.5-day raster of positions within 1e-9 AU."""
+    from solarsystemsimulator_b200 import workloads
+    nk = _nk()
+    w = workloads.asteroid_clouds(n_per_cloud=4000)
+    x, y = w["pos"][0], w["pos"][1]
+    vx, vy = w["vel"][0] * 365.25, w["vel"][1] * 365.25
+    vis = np.ones(len(x), np.uint8)
+    args = (x, y, vx, vy, w["mass"], vis, w["is_ast"], w["radius"])
+    sims = [nk.NBodyCuda([0]), nk.NBodyCuda([0], pair_f32=True)]
+    sts = [s.load_state(*args) for s in sims]
+    for s, st in zip(sims, sts):
+        s.step_batch(st, 0.0, 1)                        # no step: the accelerations at the loaded positions
+    a64, a32 = (st["aacc"][:, :st["n_ast"]].cpu().numpy() for st in sts)
+    rel = np.linalg.norm(a32 - a64, axis=0) / np.linalg.norm(a64, axis=0)
+    assert np.median(rel) <= 1e-6 and rel.max() <= 1e-4
+    outs = [s.step_batch(st, 0.5 / 365.25, 1) for s, st in zip(sims, sts)]
+    f64s = [s.export_f64(st) for s, st in zip(sims, sts)]
+    n = len(x)
+    assert np.abs(f64s[1][:2 * n] - f64s[0][:2 * n]).max() <= 1e-9
+    assert outs[0].shape == outs[1].shape
