@@ -38,6 +38,9 @@ N_TRACER = 524_288
 EPS = 1e-3
 DT = 1e-3
 FLOP_PER_PAIR = 20          # the reference's own convention (TODO.md:73-74)
+# nominal SIMT peaks of a B200 at 1965 MHz: 148 SMs x 64 DFMA / 128 FFMA lanes x 2 flops
+NOMINAL_FP64 = 148 * 64 * 2 * 1.965e9 / 1e12
+NOMINAL_FP32 = 148 * 128 * 2 * 1.965e9 / 1e12
 # DRAM bytes (read + write) of one k_force_mixed launch on this workload, from an
 # ncu capture of the full-size launch (profiles/k_force_mixed_dram_traffic_262k.md)
 MIXED_DRAM_BYTES_PER_LAUNCH = 270_845_568
@@ -184,9 +187,11 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "steps_are_samples": True, "ms_per_step_extrapolated": True,
             "note": "the reference's CPU path of this force (its f64 NumPy formula) restated in C "
-                    "with OpenMP over targets (oracle/allpairs.c); steps/s extrapolated from the "
-                    "sampled pair rate"}
+                    "with OpenMP over targets (oracle/allpairs.c); each of the `steps` is a bounded sample "
+                    "(strided targets x all sources), and ms_per_step is extrapolated from the sampled "
+                    "pair rate to a full step"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -298,15 +303,25 @@ def run_ours(args, rank, world, local_rank):
     rel_or = np.linalg.norm(am.cpu().numpy()[samp] - a_or, axis=1) / np.linalg.norm(a_or, axis=1)
     rel_f64_or = np.linalg.norm(af.cpu().numpy()[samp] - a_or, axis=1) / np.linalg.norm(a_or, axis=1)
 
-    # ---- plain f64 path, same workload
+    # ---- plain f64 path, same workload: args.drift_steps timed steps from the
+    #      initial state, so its energy drift covers them too
     sim_f, st_f = make("f64")
-    sim_f.step_batch_device(st_f, DT, 1, snapshots=True)   # warm-up
     e_f0 = sim_f.energy(st_f)
     barrier()
-    k_f64 = max(1, args.steps // 2)
+    k_f64 = max(1, args.drift_steps)
     t_f64 = max_over_ranks(timed_steps(sim_f, st_f, k_f64))
     e_f1 = sim_f.energy(st_f)
     del sim_f, st_f
+
+    # ---- mixed energy drift over the same number of steps from the initial state
+    #      (untimed; the timed region above starts after the warm-up steps)
+    sim_d, st_d = make("mixed")
+    e_d0 = sim_d.energy(st_d)
+    for _ in range(k_f64):
+        sim_d.step_batch_device(st_d, DT, 1, snapshots=True)
+    e_d1 = sim_d.energy(st_d)
+    ctx.status(stream.cuda_stream)
+    del sim_d, st_d
 
     # ---- e2e through the public API: load_state from host arrays, K steps,
     #      host snapshots back (every step's snapshot is D2H-copied)
@@ -361,9 +376,13 @@ def run_ours(args, rank, world, local_rank):
                     "steps_per_s": k_f64 / t_f64, "steps": k_f64,
                     "kernel_ms": t_kernel_f64 * 1e3,
                     "fp64_frac": (n_src * n_tgt * FLOP_PER_PAIR / t_kernel_f64 / 1e12) / peak["fp64"],
-                    "energy_drift": abs((e_f1 - e_f0) / e_f0)},
+                    "fp64_frac_of_nominal": (n_src * n_tgt * FLOP_PER_PAIR / t_kernel_f64 / 1e12) / NOMINAL_FP64,
+                    "energy_drift": abs((e_f1 - e_f0) / e_f0),
+                    "energy_drift_steps": k_f64},
             "mixed_over_f64_steps": (args.steps / t_mixed) / (k_f64 / t_f64),
             "force_error_vs_f64": ferr,
+            "energy_drift_mixed_same_steps": {"drift": abs((e_d1 - e_d0) / e_d0), "steps": k_f64,
+                                              "from": "the initial state, Yoshida-4 dt 1e-3"},
             "force_error_vs_cpu_oracle_sample": {"median": float(np.median(rel_or)),
                                                  "max": float(rel_or.max()),
                                                  "f64_kernel_max": float(rel_f64_or.max()),
@@ -371,8 +390,14 @@ def run_ours(args, rank, world, local_rank):
             "energy_drift": abs((e_m1 - e_m0) / e_m0),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak["fp32"],
                          "unit": "TFLOP/s", "frac": achieved / peak["fp32"],
+                         "frac_of_nominal": achieved / NOMINAL_FP32,
                          "traffic": MIXED_DRAM_BYTES_PER_LAUNCH if (n_src, n_tgt) == (262144, 786432) else None,
                          "traffic_unit": "bytes per launch (ncu capture)",
+                         "traffic_over_algorithmic": MIXED_DRAM_BYTES_PER_LAUNCH / (32 * (n_src + 2 * n_tgt))
+                         if (n_src, n_tgt) == (262144, 786432) else None,
+                         "traffic_note": "algorithmic bytes: sources and targets read once, accelerations "
+                                         "written once (32 B records); the rest is the f64 chunk partials "
+                                         "written and read back (compute-bound kernel, L2-resident sources)",
                          "kernel": "k_force_mixed", "kernel_ms": t_kernel_mixed * 1e3,
                          "flop_per_pair": FLOP_PER_PAIR,
                          "peak_source": "FFMA-chain probe measured in this run (no FP32 "
@@ -540,10 +565,13 @@ def measure_pm2d(dev, stream, steps=10):
                              "sample": "oracle/pm.py (NumPy f64 FFT) one force evaluation"}}
 
 
-def measure_batched(dev, stream, steps=10_000):
+def measure_batched(dev, stream, steps=100_000, subset=32):
     """4,096 independent systems (512 perturbed figure-8s, planetary systems of
-    3-64 bodies), f64 Yoshida-4, dt = 1e-3 of each innermost period; all
-    systems in one graph-captured launch set vs one launch per system."""
+    3-64 bodies), f64 Yoshida-4, dt = 1e-3 of each innermost period: the
+    configured 100,000 steps of all systems in one graph-captured launch set,
+    against one launch per system, measured directly (the same 100,000 steps)
+    on a subset of systems spread over the sizes, beside the batched launch
+    of that subset alone."""
     import time
     from oracle import batched as ob
     from solarsystemsimulator_b200 import batched, workloads
@@ -553,16 +581,18 @@ def measure_batched(dev, stream, steps=10_000):
     ens.replay()                                          # warm-up
     t = _ev_time(ens.replay, stream)
     pairs = ens.pairs_per_step() * steps
-    # one launch per system, on 64 systems spread over the sizes, 1/10 of the steps
-    sample = list(np.linspace(0, len(systems) - 1, 64).astype(int))
-    t1 = _ev_time(lambda: ens.run_one_launch_per_system(steps // 10, systems=set(sample)), stream)
-    share = sum(systems[i]["mass"].size * (systems[i]["mass"].size - 1) for i in sample) / \
+    sample = sorted(set(np.linspace(0, len(systems) - 1, subset).astype(int).tolist()))
+    sub = [systems[i] for i in sample]
+    ens_sub = batched.BatchedSystems(sub, device=dev)
+    ens_sub.run_one_launch_per_system(10)                 # warm-up
+    t_single = _ev_time(lambda: ens_sub.run_one_launch_per_system(steps), stream)
+    ens_sub.run(10)
+    t_sub_batched = _ev_time(lambda: ens_sub.run(steps), stream)
+    # CPU: the oracle on the same subset, 10 steps, scaled by the pair share
+    share = sum(s["mass"].size * (s["mass"].size - 1) for s in sub) / \
         max(1, sum(s["mass"].size * (s["mass"].size - 1) for s in systems))
-    t1_full = t1 * 10 / max(share, 1e-12)
-    # CPU: the oracle on the same 64 systems, 10 steps
     t0 = time.perf_counter()
-    for i in sample:
-        s = systems[i]
+    for s in sub:
         ob.yoshida(s["pos"], s["vel"], s["mass"], s["G"], s["dt"], 10)
     tc = (time.perf_counter() - t0) / 10 / max(share, 1e-12)
     maps = {str(g["max_n"]): list(g["map"]) for g in ens.groups}
@@ -574,57 +604,93 @@ def measure_batched(dev, stream, steps=10_000):
     ctx.check(ctx.lib.sss_probe_fma(ctx.ptr, 0, 4096, ctypes.byref(probe)))
     achieved = pairs * FLOP_PER_PAIR / t / 1e12
     return {"workload": "4096 systems (512 figure-8 + planetary 3-64 bodies), f64 Yoshida-4, dt = 1e-3 "
-                        f"innermost period, {steps} steps in one captured graph",
+                        f"innermost period, {steps} steps (the configured length) in one captured graph",
+            "steps": steps, "seconds": t,
             "steps_per_s": steps / t, "system_steps_per_s": len(systems) * steps / t,
             "g_interactions_per_s": pairs / t / 1e9,
-            "one_launch_per_system_steps_per_s_est": steps / t1_full,
-            "speedup_vs_one_launch_per_system": t1_full / t,
+            "one_launch_per_system": {"systems": len(sub), "steps": steps, "seconds": t_single,
+                                      "system_steps_per_s": len(sub) * steps / t_single,
+                                      "same_subset_batched_seconds": t_sub_batched,
+                                      "speedup_same_subset": t_single / t_sub_batched,
+                                      "note": "measured directly on the subset (systems spread over the "
+                                              "sizes), every system its own launch, one after another"},
+            "system_steps_per_s_batched_over_one_launch_each": (len(systems) * steps / t) /
+                                                               (len(sub) * steps / t_single),
             "team_mapping_by_group_max_n": maps,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": probe.value, "unit": "TFLOP/s",
-                         "frac": achieved / probe.value, "flop_per_pair": FLOP_PER_PAIR,
+                         "frac": achieved / probe.value, "frac_of_nominal": achieved / NOMINAL_FP64,
+                         "flop_per_pair": FLOP_PER_PAIR,
                          "peak_source": "DFMA-chain probe measured in this run (sss_probe_fma)"},
             "cpu_baseline": {"value": 1.0 / tc, "unit": "ensemble steps/s", "cores": 1, "kind": "port",
-                             "sample": "oracle/batched.py, 64 systems x 10 steps, scaled by pair share"}}
+                             "sample": f"oracle/batched.py, {len(sub)} systems x 10 steps, scaled by pair share"}}
 
 
-def measure_collisions(dev, stream, samples=16):
-    """The asteroid-clouds film on the device: 200,000 asteroids in 5 clouds,
-    a star and 7 planets (2-D film units AU / yr), raster 0.5 day. Per
-    sample: frame integration (NBodyCuda, 8 samples per launch), broadphase,
-    bounce response applied on the device, merge sweep + runaways, merges."""
+def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve=20_000):
+    """The asteroid-cloud film on the device for the configured 20,000 steps
+    of 0.5 day: 200,000 asteroids in 5 clouds, a star and 7 planets (2-D film
+    units AU / yr), FP32 pair forces with FP64 state. Per sample: frame
+    integration (NBodyCuda, 8 samples per launch), ring slot, stream frame,
+    broadphase with bounce_suche's cell size, bounce response on the device,
+    fragmentation of impacts above 5 v_esc into free slots (n_reserve hidden
+    slots at the start), merge sweep + runaways, merges. Every check_every-th
+    sample the ordered pair list is compared with the C oracle's (outside the
+    timed phases)."""
     import time
     import torch
+    from oracle import broadphase as obp
     from oracle import collide as oc
     from solarsystemsimulator_b200 import broadphase as bp
     from solarsystemsimulator_b200 import ring
-    from solarsystemsimulator_b200.collide import CollisionResponse
+    from solarsystemsimulator_b200.collide import FRAG_V_ESC, CollisionResponse
     from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
     from solarsystemsimulator_b200.stream import LOD_MAX, StreamFrames
     from solarsystemsimulator_b200.workloads import asteroid_clouds
     w = asteroid_clouds()
-    n = w["pos"].shape[1]
-    x, y = w["pos"][0], w["pos"][1]
-    vx, vy = w["vel"][0] * 365.25, w["vel"][1] * 365.25
-    rr = w["radius"].copy()
+    n0 = w["pos"].shape[1]
+    n = n0 + n_reserve
+    x = np.concatenate([w["pos"][0], np.zeros(n_reserve)])
+    y = np.concatenate([w["pos"][1], np.zeros(n_reserve)])
+    vx = np.concatenate([w["vel"][0] * 365.25, np.zeros(n_reserve)])
+    vy = np.concatenate([w["vel"][1] * 365.25, np.zeros(n_reserve)])
+    mass = np.concatenate([w["mass"], np.zeros(n_reserve)])
+    is_ast = np.concatenate([w["is_ast"], np.ones(n_reserve, np.uint8)])
+    rr = np.concatenate([w["radius"], np.zeros(n_reserve)])
     rng = np.random.default_rng(5)
     rr[0] = 0.00465
     rr[1:8] = 10 ** rng.uniform(-5, -4.3, 7)
     vis = np.ones(n, np.uint8)
-    sim = NBodyCuda([dev])
-    st = sim.load_state(x, y, vx, vy, w["mass"], vis, w["is_ast"], rr)
-    cr = CollisionResponse(w["mass"], rr, vis, w["is_ast"])
+    vis[n0:] = 0                                         # free slots for fragments
+    # the FP32-pair force error against f64 on the starting state
+    errs = {}
+    for pf in (False, True):
+        s_ = NBodyCuda([dev], pair_f32=pf)
+        st_ = s_.load_state(x, y, vx, vy, mass, vis, is_ast, rr)
+        s_.step_batch(st_, 0.0, 1)
+        errs[pf] = st_["aacc"][:, :st_["n_ast"]].double()
+        del s_, st_
+    a64, a32 = errs[False][:, :n0 - 8], errs[True][:, :n0 - 8]      # the visible asteroids (compact order)
+    rel = (torch.linalg.norm(a32 - a64, dim=0) / torch.linalg.norm(a64, dim=0)).cpu().numpy()
+    force_err = {"median": float(np.median(rel)), "max": float(rel.max()),
+                 "of": "asteroid accelerations, pair_f32 against the f64 path, starting state"}
+    sim = NBodyCuda([dev], pair_f32=True)
+    st = sim.load_state(x, y, vx, vy, mass, vis, is_ast, rr)
+    cr = CollisionResponse(mass, rr, vis, is_ast)
     dt_y = 0.5 / 365.25
     K = 8
-    rr32 = torch.as_tensor(rr.astype(np.float32)).to(f"cuda:{dev}")
     ast_max = float(rr[8:].max())
     sub_max = ring.sub_max_fuer(n)
     nbytes = ring.slot_bytes(n, sim.m_sub, sub_max)
     slot_dev = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{dev}")
     slot_host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
-    sf = StreamFrames(w["is_ast"], device=dev)
+    sf = StreamFrames(is_ast, device=dev)
+    sf.kill(np.arange(n0, n), float("-inf"))             # the free slots are not in the frames until used
     box = None
-    t = {"frame": 0.0, "ring": 0.0, "stream": 0.0, "broadphase": 0.0, "bounce": 0.0, "sweep": 0.0, "merges": 0.0}
-    counts = {"hits": 0, "bounces": 0, "merge_pairs": 0, "runaways": 0, "candidates": 0, "frame_points": 0}
+    phases = ("frame", "ring", "stream", "broadphase", "bounce", "fragment", "sweep", "merges")
+    t = {k: 0.0 for k in phases}
+    keys = ("hits", "bounces", "merge_pairs", "runaways", "candidates", "frame_points", "fragment_events",
+            "fragment_events_applied", "fragment_events_no_room")
+    counts = {k: 0 for k in keys}
+    checks = []
     last = None
 
     def sync():
@@ -633,10 +699,8 @@ def measure_collisions(dev, stream, samples=16):
     done = -K                                            # one untimed batch first (kernel loading, scratch)
     while done < samples:
         if done == 0:
-            for key in t:
-                t[key] = 0.0
-            for key in counts:
-                counts[key] = 0
+            t = {k: 0.0 for k in phases}
+            counts = {k: 0 for k in keys}
         t0 = time.perf_counter()
         snap = sim.step_batch_device(st, dt_y, K)            # (K, 4, n) f32, device
         sync()
@@ -655,10 +719,10 @@ def measure_collisions(dev, stream, samples=16):
             counts["frame_points"] += sel.numel()
             t["stream"] += time.perf_counter() - t0
             t0 = time.perf_counter()
-            alive = torch.nonzero((cr.d_ast != 0) & (cr.d_vis != 0)).flatten()
-            v95 = float(torch.quantile(torch.hypot(g[2][alive], g[3][alive]).double(), 0.95))
-            h = max(1e-4, 2.0 * v95 * dt_y)
-            buf, nh, nc = bp.bounce_hits_device(g[0], g[1], g[2], g[3], dt_y, h, 2.0 * h + 2.0 * ast_max, rr=rr32,
+            alive = (cr.d_ast != 0) & (cr.d_vis != 0)
+            h = bp.search_cell(g[2], g[3], alive, dt_y)
+            halo = 2.0 * h + 2.0 * ast_max
+            buf, nh, nc = bp.bounce_hits_device(g[0], g[1], g[2], g[3], dt_y, h, halo, rr=cr.d_rr32,
                                                 is_ast=cr.d_ast, vis=cr.d_vis, device=dev)
             sync()
             t1 = time.perf_counter()
@@ -666,8 +730,14 @@ def measure_collisions(dev, stream, samples=16):
             nb = cr.apply_bounce(sim, st, res)
             sync()
             t2 = time.perf_counter()
-            pairs, run = cr.analyze_merge(g, dt_y)
+            parents, frags = cr.fragment(g, res, FRAG_V_ESC, seed=20261204 + done)
+            ev, used, no_room = cr.apply_fragments(sim, st, parents, frags)
+            if used:                                     # fragments in free slots enter the frames
+                sf.kill_t[torch.as_tensor([q for u in used for q in u[2:]]).to(sf.kill_t.device)] = float("inf")
+            sync()
             t3 = time.perf_counter()
+            pairs, run = cr.analyze_merge(g, dt_y)
+            t4 = time.perf_counter()
             if pairs or run is not None:
                 sample = g.reshape(-1).cpu().numpy()
                 vis_before = cr.vis.copy()
@@ -676,16 +746,31 @@ def measure_collisions(dev, stream, samples=16):
                 gone = np.flatnonzero((vis_before != 0) & (cr.vis == 0))
                 if len(gone):
                     sf.kill(gone, float(done + 1))
-            t4 = time.perf_counter()
+            t5 = time.perf_counter()
             t["broadphase"] += t1 - t0
             t["bounce"] += t2 - t1
-            t["sweep"] += t3 - t2
-            t["merges"] += t4 - t3
+            t["fragment"] += t3 - t2
+            t["sweep"] += t4 - t3
+            t["merges"] += t5 - t4
             counts["hits"] += nh
             counts["bounces"] += nb
             counts["candidates"] += nc
             counts["merge_pairs"] += len(pairs)
             counts["runaways"] += 0 if run is None else len(run)
+            counts["fragment_events"] += len(parents)
+            counts["fragment_events_applied"] += len(ev)
+            counts["fragment_events_no_room"] += no_room
+            if done >= 0 and done % check_every == 0:
+                # the ordered pair list of this sample against the C oracle (untimed)
+                gh = g.cpu().numpy()
+                rr_h = cr.real_r.astype(np.float32)
+                got, gc = bp.bounce_hits(*gh, dt_y, h, halo, rr=rr_h, is_ast=cr.is_ast, vis=cr.vis, device=dev)
+                ref, rc = obp.hits_c(*gh, rr_h, dt_y, h, halo, is_ast=cr.is_ast, vis=cr.vis)
+                same = (got is None and ref is None) or (got is not None and ref is not None and
+                                                         np.array_equal(got[0], ref[0]) and
+                                                         np.array_equal(got[1], ref[1]))
+                checks.append({"sample": done, "hits": 0 if ref is None else len(ref[0]), "candidates": rc,
+                               "identical": bool(same and gc == rc)})
             last = (g.cpu().numpy(), buf.cpu().numpy())
             done += 1
     total = sum(t.values())
@@ -694,16 +779,25 @@ def measure_collisions(dev, stream, samples=16):
     order = np.lexsort((hits[:, 2], hits[:, 1], hits[:, 0]))
     hits = hits[order]
     t0 = time.perf_counter()
-    oc.merge_sweep(*g, g[0], g[1], rr.astype(np.float32), cr.vis, w["is_ast"], cr.mass, np.arange(8), dt_y)
+    oc.merge_sweep(*g, g[0], g[1], cr.real_r.astype(np.float32), cr.vis, is_ast, cr.mass, np.arange(8), dt_y)
     oc.bounce_deltas(*g, cr.real_r, cr.mass, hits[:, 1], hits[:, 2], dt_y)
     tc = time.perf_counter() - t0
-    return {"workload": "5 Gaussian clouds x 40,000 asteroids + star + 7 planets, 2-D film (AU, yr), raster 0.5 day, "
-                        f"{samples} samples: frame integration, ring slot to a pinned host buffer, stream frame "
-                        "(automatic box, LOD 120,000), broadphase, bounce response, merge sweep, merges",
+    return {"workload": "5 Gaussian clouds x 40,000 asteroids + star + 7 planets (+ 20,000 free slots), 2-D film "
+                        f"(AU, yr), raster 0.5 day, {samples} samples (the configured 20,000 steps), FP32 pair "
+                        "forces / FP64 state: frame integration, ring slot to a pinned host buffer, stream frame "
+                        "(automatic box, LOD 120,000), broadphase, bounce response, fragmentation above 5 v_esc, "
+                        "merge sweep, merges",
+            "samples": samples, "seconds": total,
             "samples_per_s": samples / total,
+            "sim_days_per_s": samples * 0.5 / total,
             "ms_per_sample": {k: v / samples * 1e3 for k, v in t.items()},
             "per_sample": {k: v / samples for k, v in counts.items()},
-            "response_ms_per_sample": (t["bounce"] + t["sweep"] + t["merges"]) / samples * 1e3,
+            "response_ms_per_sample": (t["bounce"] + t["fragment"] + t["sweep"] + t["merges"]) / samples * 1e3,
+            "pair_set_checks": {"every": check_every, "checked": len(checks),
+                                "identical": sum(c["identical"] for c in checks), "samples": checks,
+                                "against": "oracle/broadphase.c (restatement of _hits, pinned by the reference's "
+                                           "hit list of the starting scene)"},
+            "pair_f32_force_error_vs_f64": force_err,
             "cpu_baseline": {"value": 1.0 / tc, "unit": "samples/s (sweep + bounce response only)", "cores": 1,
                              "kind": "port", "sample": "oracle/collide.py merge_sweep + bounce_deltas on one sample"}}
 
@@ -861,12 +955,21 @@ def measure_pm3d_learned(dev, stream, steps=500):
     recs = sim.run(st, dt, steps)
     torch.cuda.synchronize(dev)
     t_run = time.perf_counter() - t0
-    # stepping alone (no judge / training), corrected and mesh only
+    # stepping alone (no judge / training), with and without the network, each
+    # timing from the same saved state (the state collapses as it steps)
     pm, net = sim.pm, sim.net
     k = 20
     pm.step_batch(st, dt, 2, net)
-    t_learn = _ev_time(lambda: pm.step_batch(st, dt, k, net), stream) / k
-    t_method = _ev_time(lambda: pm.step_batch(st, dt, k), stream) / k
+    saved = st["buf"].clone()
+
+    def from_saved(fn):
+        def run():
+            st["buf"].copy_(saved)
+            fn()
+        return run
+    t_learn = _ev_time(from_saved(lambda: pm.step_batch(st, dt, k, net)), stream) / k
+    t_method = _ev_time(from_saved(lambda: pm.step_batch(st, dt, k)), stream) / k
+    st["buf"].copy_(saved)
     # the mesh alone (r_split 0.6 cells, no pair term) on the same state: speed and error
     pm_mesh = pm3d.PMPeriodic3D(w["mesh_n"], 1.0, 1.0, dev, 2, 0.6)
     p_now, v_now = pm.export_f64(st)
@@ -964,6 +1067,8 @@ def main():
     ap.add_argument("--n-side", type=int, default=N_SIDE,
                     help="sources = n_side^3 (64 is the configuration; smaller only for profiling)")
     ap.add_argument("--n-tracer", type=int, default=N_TRACER)
+    ap.add_argument("--drift-steps", type=int, default=100,
+                    help="f64 steps timed from the initial state, and the energy-drift length of both paths")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

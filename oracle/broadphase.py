@@ -76,3 +76,40 @@ def hits(gx, gy, gvx, gvy, rr, dt_y, h, halo, is_ast=None, vis=None, lo=-np.inf,
     if not sel.any():
         return None, cand
     return (ci[sel], cj[sel]), cand
+
+
+def hits_c(gx, gy, gvx, gvy, rr, dt_y, h, halo, is_ast=None, vis=None, lo=-np.inf, hi=np.inf, threads=None):
+    """The same pair list from the C restatement (oracle/broadphase.c),
+    multithreaded, for scenes the NumPy form takes minutes on."""
+    import ctypes
+    import os
+    from . import build as _build
+    L = ctypes.CDLL(_build.build())
+    f = L.oracle_broadphase_hits
+    f.restype = ctypes.c_int64
+    vp = ctypes.c_void_p
+    f.argtypes = [vp, vp, vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_float, ctypes.c_float, vp, vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
+                  ctypes.c_int]
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (gx, gy, gvx, gvy, rr)]
+    n = len(arrs[0])
+    ast = None if is_ast is None else np.ascontiguousarray(np.asarray(is_ast) != 0, np.uint8)
+    vv = None if vis is None else np.ascontiguousarray(np.asarray(vis) != 0, np.uint8)
+    nthreads = threads or int(os.environ.get("SSS_ORACLE_THREADS", os.cpu_count() or 1))
+    cap = max(1024, n)
+    while True:
+        oi = np.empty(cap, np.int64)
+        oj = np.empty(cap, np.int64)
+        nc = ctypes.c_int64()
+        k = f(*(a.ctypes.data for a in arrs), None if ast is None else ast.ctypes.data,
+              None if vv is None else vv.ctypes.data, n, float(dt_y), float(h), float(halo),
+              float(np.float32(lo)), float(np.float32(hi)), oi.ctypes.data, oj.ctypes.data, cap, ctypes.byref(nc),
+              nthreads)
+        if k < 0:
+            raise MemoryError("oracle_broadphase_hits: allocation failed")
+        if k <= cap:
+            break
+        cap = int(k)
+    if k == 0:
+        return None, int(nc.value)
+    return (oi[:k], oj[:k]), int(nc.value)

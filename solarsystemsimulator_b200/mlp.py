@@ -86,6 +86,20 @@ class ShortRangeMLP:
         self.out_scale = snap["out_scale"]
         self.pack()
 
+    def rescale_output(self, factor: float) -> None:
+        """Multiply the output layer (W3, b3) by `factor`, with Adam's
+        moments to match (m by factor, v by factor^2): the network's output
+        in units of out_scale / factor is the same function as before."""
+        off = 0
+        for name, shape in SHAPES:
+            size = int(np.prod(shape))
+            if name in ("W3", "b3"):
+                self.params[off:off + size] *= factor
+                self.m[off:off + size] *= factor
+                self.v[off:off + size] *= factor * factor
+            off += size
+        self.pack()
+
     # ---- compute
     def features(self, pm, parts, idx: torch.Tensor | None, rho_mean: float, rows: int | None = None) -> torch.Tensor:
         """bf16 inputs (rows, 80) of particles idx (int64 device tensor) from

@@ -253,7 +253,7 @@ class NBodyPMLearned:
                  softening: float = 1e-3, check_every: int = 50, samples: int = 16384, tol: float | None = None,
                  iters: int = 200, batch: int = 2048, lr: float = 1e-3, seed: int = 0, fallback: str = "mesh",
                  learned: bool = True, deconv: int = 2, r_split_cells: float = 0.6, short_range: bool = False,
-                 x_cut: float = 3.5):
+                 x_cut: float = 3.5, window: int = 4):
         if fallback not in ("mesh", "direct"):
             raise ValueError("fallback must be 'mesh' or 'direct'")
         self.pm = PMPeriodic3D(mesh_n, box, G, device, deconv, r_split_cells, short_range, softening, x_cut)
@@ -267,8 +267,10 @@ class NBodyPMLearned:
         self.fallback = fallback
         self.active = False             # network in use for the force
         self.accepted = None            # snapshot of the last accepted network
+        self.window = int(window)       # checks whose samples form the training set
         self.X = None                   # training inputs (rows, 80) bf16 bits
         self.R = None                   # residuals direct - mesh (rows, 3) f64
+        self._rows: list[int] = []      # rows contributed by each check in the window
         self.records: list[CheckRecord] = []
         self.steps_done = 0
 
@@ -359,14 +361,24 @@ class NBodyPMLearned:
         t1 = time.perf_counter()
         rec = CheckRecord(self.steps_done, err_mesh, err_corr, accepted, reverted)
         if self.net is not None:
+            # training set: the samples of the last `window` checks; targets in
+            # units of their current rms (the residuals grow as halos collapse),
+            # the output layer rescaled so the network's force is unchanged
             R = (a_dir - a_mesh).T.contiguous()
             if self.X is None:
-                self.net.out_scale = float(torch.sqrt(torch.mean(R * R)))
                 self.X, self.R = X, R
             else:
                 self.X = torch.cat([self.X, X])
                 self.R = torch.cat([self.R, R])
-            T = (self.R / self.net.out_scale).float()
+            self._rows.append(int(R.shape[0]))
+            if len(self._rows) > self.window:
+                drop = self._rows.pop(0)
+                self.X, self.R = self.X[drop:], self.R[drop:]
+            scale = float(torch.sqrt(torch.mean(self.R * self.R)))
+            if len(self._rows) > 1 and scale > 0.0:
+                self.net.rescale_output(self.net.out_scale / scale)
+            self.net.out_scale = scale
+            T = (self.R / scale).float()
             losses = self.net.train(self.X, T, self.iters, self.batch, self.lr, self.rng)
             rec.loss_first, rec.loss_last = losses[0], losses[-1]
             self.active = True

@@ -283,7 +283,7 @@ def _fast_impacts(seed=41, n=3000):
     rng = np.random.default_rng(seed)
     x = (1.5 + rng.normal(0, 1e-4, n)).astype(np.float32)
     y = rng.normal(0, 1e-4, n).astype(np.float32)
-    sp = 10 ** rng.uniform(-7, -2, n)                      # AU / yr: from below to far above v_esc
+    sp = 10 ** rng.uniform(-3, 0.5, n)                     # AU / yr: v_esc is ~0.02 AU / yr at r = 1e-6 AU
     th = rng.uniform(0, 2 * np.pi, n)
     vx, vy = (sp * np.cos(th)).astype(np.float32), (sp * np.sin(th)).astype(np.float32)
     rr = 10 ** rng.uniform(-6.5, -5.5, n)
@@ -300,8 +300,8 @@ def test_fragments_match_oracle_and_conserve():
     n = g.shape[1]
     ones = np.ones(n, np.uint8)
     dt_y = 0.5 / 365.25
-    buf, k, _ = bp.bounce_hits_device(*g, dt_y, 1e-4, 2e-4 + 2 * float(rr.max()), rr=rr.astype(np.float32),
-                                      vis=vis)
+    h = max(1e-4, 2.0 * float(np.percentile(np.hypot(g[2], g[3]), 95)) * dt_y)
+    buf, k, _ = bp.bounce_hits_device(*g, dt_y, h, 2 * h + 2 * float(rr.max()), rr=rr.astype(np.float32), vis=vis)
     cr = CollisionResponse(mass, rr, vis, ones, m_idx=np.zeros(0, np.int64))
     gd = torch.as_tensor(g).cuda()
     res = cr.bounce_deltas(gd, buf, k, dt_y)
@@ -341,7 +341,8 @@ def test_fragments_enter_the_simulation():
     vis[0] = 1
     gg = np.stack([x, y, g[2], g[3]]).astype(np.float32)
     dt_y = 0.5 / 365.25
-    buf, k, _ = bp.bounce_hits_device(*gg, dt_y, 1e-4, 2e-4 + 2 * float(rr.max()), rr=rr.astype(np.float32),
+    h = max(1e-4, 2.0 * float(np.percentile(np.hypot(gg[2], gg[3]), 95)) * dt_y)
+    buf, k, _ = bp.bounce_hits_device(*gg, dt_y, h, 2 * h + 2 * float(rr.max()), rr=rr.astype(np.float32),
                                       is_ast=is_ast, vis=vis)
     cr = CollisionResponse(mass, rr, vis, is_ast, m_idx=np.array([0]))
     sim = NBodyCuda([0])
