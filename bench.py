@@ -726,18 +726,10 @@ def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve
                                                 is_ast=cr.d_ast, vis=cr.d_vis, device=dev)
             sync()
             t1 = time.perf_counter()
-            res = cr.bounce_deltas(g, buf, nh, dt_y)
-            nb = cr.apply_bounce(sim, st, res)
-            sync()
-            t2 = time.perf_counter()
-            parents, frags = cr.fragment(g, res, FRAG_V_ESC, seed=20261204 + done)
-            ev, used, no_room = cr.apply_fragments(sim, st, parents, frags)
-            if used:                                     # fragments in free slots enter the frames
-                sf.kill_t[torch.as_tensor([q for u in used for q in u[2:]]).to(sf.kill_t.device)] = float("inf")
-            sync()
-            t3 = time.perf_counter()
+            # merge sweep and merges first (the producer's order: analysis of the sample, merges, then
+            # bounces), then the bounce response and the fragments of this sample's fast impacts
             pairs, run = cr.analyze_merge(g, dt_y)
-            t4 = time.perf_counter()
+            t2 = time.perf_counter()
             if pairs or run is not None:
                 sample = g.reshape(-1).cpu().numpy()
                 vis_before = cr.vis.copy()
@@ -746,12 +738,22 @@ def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve
                 gone = np.flatnonzero((vis_before != 0) & (cr.vis == 0))
                 if len(gone):
                     sf.kill(gone, float(done + 1))
+            t3 = time.perf_counter()
+            res = cr.bounce_deltas(g, buf, nh, dt_y)
+            nb = cr.apply_bounce(sim, st, res)
+            sync()
+            t4 = time.perf_counter()
+            parents, frags = cr.fragment(g, res, FRAG_V_ESC, seed=20261204 + done)
+            ev, used, no_room = cr.apply_fragments(sim, st, parents, frags)
+            if used:                                     # fragments in free slots enter the frames
+                sf.kill_t[torch.as_tensor([q for u in used for q in u[2:]]).to(sf.kill_t.device)] = float("inf")
+            sync()
             t5 = time.perf_counter()
             t["broadphase"] += t1 - t0
-            t["bounce"] += t2 - t1
-            t["fragment"] += t3 - t2
-            t["sweep"] += t4 - t3
-            t["merges"] += t5 - t4
+            t["sweep"] += t2 - t1
+            t["merges"] += t3 - t2
+            t["bounce"] += t4 - t3
+            t["fragment"] += t5 - t4
             counts["hits"] += nh
             counts["bounces"] += nb
             counts["candidates"] += nc

@@ -211,31 +211,35 @@ class CollisionResponse:
         enough free slots is left out (its bounce stands). Returns
         (events (a, b, fragment mass, 3, 0.0, x, y), slots used per event,
         events left out)."""
-        events, used, skipped = [], [], 0
         if len(parents) == 0:
-            return events, used, skipped
+            return [], [], 0
         n_frag = frags.shape[1]
-        free = list(np.flatnonzero((self.vis == 0) & self.is_ast)[::-1])       # pop() gives the lowest
-        idx, vals, radii = [], [], []
-        for (a, b), f in zip(parents, frags):
-            if len(free) < n_frag - 2:
-                skipped += 1
-                continue
-            slots = [int(a), int(b)] + [int(free.pop()) for _ in range(n_frag - 2)]
-            for s_, row in zip(slots, f):
-                idx.append(s_)
-                vals.append([row[0], row[1], row[2], row[3], row[4]] if st["dim"] == 2 else
-                            [row[0], row[1], 0.0, row[2], row[3], 0.0, row[4]])
-                radii.append(row[5])
-                self.mass[s_] = row[4]
-                self.real_r[s_] = row[5]
-                self.vis[s_] = 1
-            used.append(slots)
-            events.append((int(a), int(b), float(f[0, 4]), 3, 0.0, float(f[:, 0].mean()), float(f[:, 1].mean())))
-        if idx:
-            sim.set_asteroids(st, idx, vals, radii)
-            self.refresh()
-        return events, used, skipped
+        free = np.flatnonzero((self.vis == 0) & self.is_ast)                  # ascending
+        e = min(len(parents), len(free) // (n_frag - 2))                      # events with room, in order
+        skipped = len(parents) - e
+        if e == 0:
+            return [], [], skipped
+        slots = np.concatenate([parents[:e], free[:e * (n_frag - 2)].reshape(e, n_frag - 2)], 1)
+        f = frags[:e].reshape(e * n_frag, 6)
+        idx = slots.reshape(-1)
+        if st["dim"] == 2:
+            vals = f[:, 0:5]
+        else:
+            z = np.zeros((len(f), 1))
+            vals = np.concatenate([f[:, 0:2], z, f[:, 2:4], z, f[:, 4:5]], 1)
+        sim.set_asteroids(st, idx, vals, f[:, 5])
+        self.mass[idx] = f[:, 4]
+        self.real_r[idx] = f[:, 5]
+        self.vis[idx] = 1
+        if self.prev is not None:          # the fragments' sweep segments start where they are placed
+            p_idx = torch.as_tensor(idx).to(self.dev)
+            self.prev[0][p_idx] = torch.as_tensor(f[:, 0].astype(np.float32)).to(self.dev)
+            self.prev[1][p_idx] = torch.as_tensor(f[:, 1].astype(np.float32)).to(self.dev)
+        self.refresh()
+        fr = frags[:e]
+        events = [(int(a), int(b), float(q[0, 4]), 3, 0.0, float(q[:, 0].mean()), float(q[:, 1].mean()))
+                  for (a, b), q in zip(parents[:e], fr)]
+        return events, slots.tolist(), skipped
 
     def apply_bounce(self, sim, st, res) -> int:
         """Add the bounce deltas to the simulation on the device (apply_bounce,
