@@ -464,14 +464,17 @@ int sss_ewald_gtab(double* out, int64_t cap, int* n_int, double* h);
  * A per-particle MLP 67 -> 128 -> 128 -> 3 (SiLU) that adds the short-range
  * force the mesh cannot resolve. Inputs: log1p(rho / rho_mean) on the 4x4x4
  * mesh cells around the particle's cell (i0-1 .. i0+2 per axis), then the
- * sub-cell offsets - 1/2 (padded with zeros to 80). Weights are bf16 on the
- * tensor cores (mma.sync m16n8k16), accumulation f32. Parameters are one
- * f32 array of SSS_MLP_N_PARAMS: W1[80][128], b1[128], W2[128][128], b2[128],
- * W3[128][8], b3[8] (rows 67..79 of W1 and columns 3..7 of W3 zero);
- * sss_mlp_pack turns them into the bf16 fragment arrays (SSS_MLP_N_FRAGS
- * uint32) the kernels read. No reference counterpart. */
+ * sub-cell offsets - 1/2 (padded with zeros to 80). Weights and activations
+ * are bf16 on the tensor cores (tcgen05.mma, accumulators in tensor memory),
+ * accumulation f32; forward, backward and the weight gradients all run
+ * there. Parameters are one f32 array of SSS_MLP_N_PARAMS: W1[80][128],
+ * b1[128], W2[128][128], b2[128], W3[128][8], b3[8] (rows 67..79 of W1 and
+ * columns 3..7 of W3 zero); sss_mlp_pack turns them into the bf16 operand
+ * images (SSS_MLP_N_FRAGS uint32: W1^T, W2^T and W2 in the tensor cores'
+ * shared-memory layout, W3) that the kernels copy to shared memory. No
+ * reference counterpart. */
 #define SSS_MLP_N_PARAMS 27912
-#define SSS_MLP_N_FRAGS  23040
+#define SSS_MLP_N_FRAGS  22016
 #define SSS_MLP_IN_PAD   80
 int sss_mlp_pack(sss_ctx* ctx, const float* params, uint32_t* frags, void* stream);
 /* X[r] (bf16 bits, 80 per row) <- inputs of particle idx[r] (idx NULL: r) */

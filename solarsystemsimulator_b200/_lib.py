@@ -72,7 +72,7 @@ PM3_FORCE = 0
 PM3_KICK = 1
 PM3_KICK_DRIFT = 2
 MLP_N_PARAMS = 27912
-MLP_N_FRAGS = 23040
+MLP_N_FRAGS = 22016
 MLP_IN_PAD = 80
 COLLIDE_MAX_BODIES = 1600000
 

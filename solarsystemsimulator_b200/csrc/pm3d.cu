@@ -184,6 +184,7 @@ void pm3_free(sss_pm3* p) {
     if (p->fwd) cufftDestroy(p->fwd);
     if (p->inv3) cufftDestroy(p->inv3);
     cudaFree(p->rho);
+    cudaFree(p->lrho);
     cudaFree(p->rk);
     cudaFree(p->ak);
     cudaFree(p->acc);
@@ -217,6 +218,7 @@ extern "C" int sss_pm3_create(sss_ctx* ctx, int mesh_n, double box, sss_pm3** ou
     const size_t m = (size_t)mesh_n * mesh_n * (mesh_n / 2 + 1);
     cudaError_t e = cudaSuccess;
     e = e ? e : cudaMalloc(&p->rho, n3 * sizeof(float));
+    e = e ? e : cudaMalloc(&p->lrho, n3 * sizeof(float));
     e = e ? e : cudaMalloc(&p->rk, m * sizeof(float2));
     e = e ? e : cudaMalloc(&p->ak, 3 * m * sizeof(float2));
     e = e ? e : cudaMalloc(&p->acc, 3 * n3 * sizeof(float));

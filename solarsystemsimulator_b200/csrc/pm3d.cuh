@@ -12,6 +12,7 @@ struct sss_pm3 {
     int n;              // mesh side
     double box;         // periodic box side
     float* rho;         // n^3 density (mass / h^3)
+    float* lrho;        // n^3 log1p(rho / rho_mean): the correction network's inputs
     float2* rk;         // n * n * (n/2 + 1) spectrum of rho
     float2* ak;         // 3 spectra of the acceleration components (contiguous)
     float* acc;         // 3 n^3 acceleration meshes (contiguous)

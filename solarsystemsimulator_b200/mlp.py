@@ -1,7 +1,7 @@
 """The learned short-range correction of the 3-D mesh force: a per-particle
-MLP 67 -> 128 -> 128 -> 3 (SiLU) with bf16 weights on the tensor cores and
-f32 accumulation, trained online by the library's own forward and backward
-kernels (sss_mlp_*).
+MLP 67 -> 128 -> 128 -> 3 (SiLU) with bf16 weights on the tensor cores
+(tcgen05, f32 accumulators in tensor memory), trained online by the
+library's own forward, backward and weight-gradient kernels (sss_mlp_*).
 
     net = ShortRangeMLP(device=0, seed=0)
     X = net.features(pm, parts, idx, rho_mean)    # uint16 (rows, 80) bf16 bits
@@ -71,7 +71,7 @@ class ShortRangeMLP:
 
     # ---- state
     def pack(self) -> None:
-        """Rebuild the bf16 fragment arrays from the f32 parameters."""
+        """Rebuild the bf16 operand images from the f32 parameters."""
         self._call("sss_mlp_pack", self.params.data_ptr(), self.frags.data_ptr())
 
     def snapshot(self) -> dict:
