@@ -207,16 +207,28 @@ class CollisionResponse:
         """Replace each fragmenting pair by its fragments (after the bounce
         deltas of the sample were applied: the parents' states are set anew).
         Fragments 0 and 1 take the parents' slots, the others free asteroid
-        slots (hidden asteroids, lowest index first); an event without
-        enough free slots is left out (its bounce stands). Returns
-        (events (a, b, fragment mass, 3, 0.0, x, y), slots used per event,
-        events left out)."""
+        slots (hidden asteroids, lowest index first). A body can sit in
+        several active bounce pairs; only the first event (in pair order)
+        that names a body fragments it, and a later event sharing a parent
+        with an earlier one is left out, as is an event with a parent hidden
+        by a merge of the same sample and an event without enough free slots
+        (the bounce of a left-out event stands). Returns (events (a, b,
+        fragment mass, 3, 0.0, x, y), slots used per event, events left out)."""
         if len(parents) == 0:
             return [], [], 0
+        n_events = len(parents)
+        used, keep = set(), []
+        for q, (a, b) in enumerate(parents):
+            # a parent hidden since the broadphase ran (absorbed by a merge of
+            # the same sample) does not fragment; neither does a body twice
+            if self.vis[a] and self.vis[b] and int(a) not in used and int(b) not in used:
+                keep.append(q)
+                used.update((int(a), int(b)))
+        parents, frags = parents[keep], frags[keep]
         n_frag = frags.shape[1]
         free = np.flatnonzero((self.vis == 0) & self.is_ast)                  # ascending
         e = min(len(parents), len(free) // (n_frag - 2))                      # events with room, in order
-        skipped = len(parents) - e
+        skipped = n_events - e
         if e == 0:
             return [], [], skipped
         slots = np.concatenate([parents[:e], free[:e * (n_frag - 2)].reshape(e, n_frag - 2)], 1)

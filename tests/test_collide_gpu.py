@@ -364,3 +364,42 @@ def test_fragments_enter_the_simulation():
         assert np.all(cr.vis[sl] == 1) and np.array_equal(cr.mass[sl], f[:, 4])
     # the fragments fly on with the rest
     sim.step_batch(st, dt_y, 1)
+
+
+def test_fragment_events_sharing_a_body():
+    """A body in two fast active pairs fragments once: the later event that
+    names an already fragmented body is left out (its bounce stands), so is
+    an event with a hidden parent, and the slots stay distinct."""
+    from solarsystemsimulator_b200.collide import CollisionResponse, FRAG_V_ESC, N_FRAG
+    from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
+    g, rr, mass, vis = _fast_impacts(seed=43, n=600)
+    n = g.shape[1]
+    is_ast = np.ones(n, np.uint8)
+    is_ast[0] = 0
+    x = g[0].astype(np.float64)
+    y = g[1].astype(np.float64)
+    x[0], y[0] = 0.0, 0.0
+    mass = mass.copy()
+    mass[0] = 1.0
+    vis[0] = 1
+    gg = np.stack([x, y, g[2], g[3]]).astype(np.float32)
+    cr = CollisionResponse(mass, rr, vis, is_ast, m_idx=np.array([0]))
+    sim = NBodyCuda([0])
+    st = sim.load_state(x, y, gg[2].astype(np.float64), gg[3].astype(np.float64), mass, vis, is_ast, rr)
+    a, b, c, d, e5 = [int(q) for q in np.flatnonzero((vis != 0) & (is_ast != 0))[:5]]
+    hid = int(np.flatnonzero((vis == 0) & (is_ast != 0))[0])
+    # (b, c) shares b with the first event; (hid, e5) names a body hidden since the broadphase
+    parents = np.array([[a, b], [b, c], [c, d], [hid, e5]], np.int64)
+    frags = np.zeros((4, N_FRAG, 6))
+    for e, (p, q) in enumerate(parents):
+        frags[e, :, 0] = x[p] + 1e-6 * np.arange(N_FRAG)
+        frags[e, :, 1] = y[q]
+        frags[e, :, 4] = (mass[p] + mass[q]) / N_FRAG
+        frags[e, :, 5] = rr[p]
+    events, used, skipped = cr.apply_fragments(sim, st, parents, frags)
+    assert [ev[:2] for ev in events] == [(a, b), (c, d)] and skipped == 2
+    slots = np.array(used)
+    assert len(np.unique(slots)) == slots.size
+    out = sim.export_f64(st)
+    assert np.array_equal(out[slots[1]], frags[2, :, 0])
+    assert FRAG_V_ESC > 0
