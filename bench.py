@@ -254,6 +254,9 @@ def run_ours(args, rank, world, local_rank):
         v = ctypes_double()
         ctx.check(ctx.lib.sss_probe_fma(ctx.ptr, kind, 4096, __import__("ctypes").byref(v)))
         peak[name] = v.value
+    v = ctypes_double()
+    ctx.check(ctx.lib.sss_probe_fma(ctx.ptr, 3, 1024, __import__("ctypes").byref(v)))
+    rsqrt_tops = v.value                # f32 rsqrt.approx operations per second / 1e12
 
     # ---- mixed: warm-up, then the timed region
     sim_m, st_m = make("mixed")
@@ -403,6 +406,18 @@ def run_ours(args, rank, world, local_rank):
                          "peak_source": "FFMA-chain probe measured in this run (no FP32 "
                                         "SIMT peak in MEASURED_PEAKS.json)"},
             "peaks_measured_tflops": peak,
+            "rsqrt_measured_tops": rsqrt_tops,
+            # what bounds the mixed pair loop: 11 f32 operations on the FMA pipe and one rsqrt on
+            # the special function unit per pair; the f64 path is measured above
+            "mixed_ceiling": {
+                "fp32_ops_per_pair": 11, "rsqrt_per_pair": 1,
+                "fp32_bound": peak["fp32"] * 1e12 / 2 / 11 / 1e9,
+                "rsqrt_bound": rsqrt_tops * 1e12 / 1e9,
+                "unit": UNIT,
+                "achieved_over_fp32_bound": value / (world * peak["fp32"] * 1e12 / 2 / 11 / 1e9),
+                "ratio_over_f64_at_fp32_bound": (peak["fp32"] * 1e12 / 2 / 11) / (pps * k_f64 / t_f64),
+                "ratio_over_f64_at_rsqrt_bound": (rsqrt_tops * 1e12) / (pps * k_f64 / t_f64),
+            },
             "cpu_baseline": cpu,
             "e2e": {"value": world * pps * args.steps / t_e2e / 1e9, "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -625,9 +640,10 @@ def measure_batched(dev, stream, steps=100_000, subset=32):
                              "sample": f"oracle/batched.py, {len(sub)} systems x 10 steps, scaled by pair share"}}
 
 
-def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve=20_000):
-    """The asteroid-cloud film on the device for the configured 20,000 steps
-    of 0.5 day: 200,000 asteroids in 5 clouds, a star and 7 planets (2-D film
+def measure_collisions(dev, stream, samples=2_000, check_every=500, n_reserve=20_000):
+    """The asteroid-cloud film on the device: the first `samples` of the
+    configured 20,000 steps of 0.5 day (the whole run: bench.py --row
+    collisions --row-steps 20000): 200,000 asteroids in 5 clouds, a star and 7 planets (2-D film
     units AU / yr), FP32 pair forces with FP64 state. Per sample: frame
     integration (NBodyCuda, 8 samples per launch), ring slot, stream frame,
     broadphase with bounce_suche's cell size, bounce response on the device,
@@ -648,10 +664,16 @@ def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve
     w = asteroid_clouds()
     n0 = w["pos"].shape[1]
     n = n0 + n_reserve
-    x = np.concatenate([w["pos"][0], np.zeros(n_reserve)])
-    y = np.concatenate([w["pos"][1], np.zeros(n_reserve)])
-    vx = np.concatenate([w["vel"][0] * 365.25, np.zeros(n_reserve)])
-    vy = np.concatenate([w["vel"][1] * 365.25, np.zeros(n_reserve)])
+    # the free slots wait hidden on circular orbits at 20-25 AU (inside the frames' automatic box,
+    # away from the clouds), where they integrate as calm massless bodies until a fragment takes one
+    q = np.arange(n_reserve, dtype=np.float64)
+    r_res = 20.0 + 5.0 * q / max(n_reserve, 1)
+    th_res = 2.0 * np.pi * ((q * 0.6180339887498949) % 1.0)
+    v_res = 2.0 * np.pi / np.sqrt(r_res)                 # AU / yr about 1 Msun
+    x = np.concatenate([w["pos"][0], r_res * np.cos(th_res)])
+    y = np.concatenate([w["pos"][1], r_res * np.sin(th_res)])
+    vx = np.concatenate([w["vel"][0] * 365.25, -v_res * np.sin(th_res)])
+    vy = np.concatenate([w["vel"][1] * 365.25, v_res * np.cos(th_res)])
     mass = np.concatenate([w["mass"], np.zeros(n_reserve)])
     is_ast = np.concatenate([w["is_ast"], np.ones(n_reserve, np.uint8)])
     rr = np.concatenate([w["radius"], np.zeros(n_reserve)])
@@ -703,6 +725,9 @@ def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve
             counts = {k: 0 for k in keys}
         t0 = time.perf_counter()
         snap = sim.step_batch_device(st, dt_y, K)            # (K, 4, n) f32, device
+        new = cr.activate_fragments(snap[0].reshape(4, n))  # fragments of the last batch join the analysis
+        if len(new):                                         # and the frames
+            sf.kill_t[torch.as_tensor(new).to(sf.kill_t.device)] = float("inf")
         sync()
         t["frame"] += time.perf_counter() - t0
         for k in range(K):
@@ -745,8 +770,6 @@ def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve
             t4 = time.perf_counter()
             parents, frags = cr.fragment(g, res, FRAG_V_ESC, seed=20261204 + done)
             ev, used, no_room = cr.apply_fragments(sim, st, parents, frags)
-            if used:                                     # fragments in free slots enter the frames
-                sf.kill_t[torch.as_tensor([q for u in used for q in u[2:]]).to(sf.kill_t.device)] = float("inf")
             sync()
             t5 = time.perf_counter()
             t["broadphase"] += t1 - t0
@@ -785,7 +808,7 @@ def measure_collisions(dev, stream, samples=20_000, check_every=2_000, n_reserve
     oc.bounce_deltas(*g, cr.real_r, cr.mass, hits[:, 1], hits[:, 2], dt_y)
     tc = time.perf_counter() - t0
     return {"workload": "5 Gaussian clouds x 40,000 asteroids + star + 7 planets (+ 20,000 free slots), 2-D film "
-                        f"(AU, yr), raster 0.5 day, {samples} samples (the configured 20,000 steps), FP32 pair "
+                        f"(AU, yr), raster 0.5 day, {samples} samples (of the configured 20,000 steps), FP32 pair "
                         "forces / FP64 state: frame integration, ring slot to a pinned host buffer, stream frame "
                         "(automatic box, LOD 120,000), broadphase, bounce response, fragmentation above 5 v_esc, "
                         "merge sweep, merges",
@@ -1092,7 +1115,7 @@ def main():
         if args.row == "stream" and args.row_steps:
             kw = {"samples": args.row_steps}
         if args.row == "collisions" and args.row_steps:
-            kw = {"samples": args.row_steps}
+            kw = {"samples": args.row_steps, "check_every": max(500, args.row_steps // 10)}
         if args.row == "broadphase" and args.row_steps:
             kw = {"reps": args.row_steps}
         print(json.dumps(fn(local_rank, torch.cuda.current_stream(local_rank), **kw)), flush=True)

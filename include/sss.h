@@ -562,9 +562,11 @@ int sss_allpairs_accel_noalloc(int device, int dim, int precision,
 
 /* ------------------------------------------------------------ diagnostics */
 
-/* Measured FMA throughput of the device in TFLOP/s (2 flops per FMA lane):
- * kind 0 = f64 DFMA, 1 = f32 FFMA, 2 = packed f32x2 FMA. Synchronous; the
- * roofline denominator of the all-pairs kernels. No reference counterpart. */
+/* Measured throughput of the device: kind 0 = f64 DFMA, 1 = f32 FFMA,
+ * 2 = packed f32x2 FMA in TFLOP/s (2 flops per FMA lane); kind 3 = f32
+ * rsqrt.approx in T operations/s (the special function unit). Synchronous;
+ * the roofline denominators of the all-pairs kernels. No reference
+ * counterpart. */
 int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops);
 
 /* Self-test of the bounded waits: runs one wait that nothing completes, with

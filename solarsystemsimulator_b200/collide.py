@@ -8,6 +8,7 @@ analysis of the reference's film producer with its array parts on the device.
     cr.apply_bounce(sim, st, res)                        # apply_bounce, :1021-1040 (deltas on the device)
     parents, frags = cr.fragment(g, res, FRAG_V_ESC, seed)  # fast impacts break up (no reference counterpart)
     cr.apply_fragments(sim, st, parents, frags)
+    cr.activate_fragments(g0)                            # after the next batch's integration (g0: its first sample)
 
 `g` is the sample on the device as f32 rows (4, n) [x|y|vx|vy] (the row the
 detection card holds); `sample` the same row on the host (f32, 4n). The
@@ -44,6 +45,7 @@ class CollisionResponse:
         self.is_ast = np.asarray(is_ast) != 0
         self.n = len(self.mass)
         self.is_star_bh = (np.zeros(self.n, bool) if is_star_bh is None else np.asarray(is_star_bh) != 0)
+        self.pending = np.zeros(self.n, bool)   # fragment slots placed, visible from the next batch
         self.m_idx = np.flatnonzero(~self.is_ast) if m_idx is None else np.asarray(m_idx, np.int64)
         if len(self.m_idx) > 64:
             raise ValueError(f"zu viele massive Koerper: {len(self.m_idx)} > 64")
@@ -213,7 +215,13 @@ class CollisionResponse:
         with an earlier one is left out, as is an event with a parent hidden
         by a merge of the same sample and an event without enough free slots
         (the bounce of a left-out event stands). Returns (events (a, b,
-        fragment mass, 3, 0.0, x, y), slots used per event, events left out)."""
+        fragment mass, 3, 0.0, x, y), slots used per event, events left out).
+
+        The samples of a batch are integrated before they are analysed, so
+        the rest of the batch still shows the free slots where they were; the
+        new slots join the analysis (vis) with the next batch, when
+        activate_fragments() is called after its integration. The simulation
+        integrates them from now on."""
         if len(parents) == 0:
             return [], [], 0
         n_events = len(parents)
@@ -226,7 +234,7 @@ class CollisionResponse:
                 used.update((int(a), int(b)))
         parents, frags = parents[keep], frags[keep]
         n_frag = frags.shape[1]
-        free = np.flatnonzero((self.vis == 0) & self.is_ast)                  # ascending
+        free = np.flatnonzero((self.vis == 0) & self.is_ast & ~self.pending)  # ascending
         e = min(len(parents), len(free) // (n_frag - 2))                      # events with room, in order
         skipped = n_events - e
         if e == 0:
@@ -242,16 +250,34 @@ class CollisionResponse:
         sim.set_asteroids(st, idx, vals, f[:, 5])
         self.mass[idx] = f[:, 4]
         self.real_r[idx] = f[:, 5]
-        self.vis[idx] = 1
-        if self.prev is not None:          # the fragments' sweep segments start where they are placed
-            p_idx = torch.as_tensor(idx).to(self.dev)
-            self.prev[0][p_idx] = torch.as_tensor(f[:, 0].astype(np.float32)).to(self.dev)
-            self.prev[1][p_idx] = torch.as_tensor(f[:, 1].astype(np.float32)).to(self.dev)
+        self.pending[slots[:, 2:].reshape(-1)] = True
+        if self.prev is not None:          # fragments 0 and 1: their sweep segments start where they are placed
+            p_idx = torch.as_tensor(slots[:, :2].reshape(-1)).to(self.dev)
+            f01 = frags[:e, :2].reshape(2 * e, 6)
+            self.prev[0][p_idx] = torch.as_tensor(f01[:, 0].astype(np.float32)).to(self.dev)
+            self.prev[1][p_idx] = torch.as_tensor(f01[:, 1].astype(np.float32)).to(self.dev)
         self.refresh()
         fr = frags[:e]
         events = [(int(a), int(b), float(q[0, 4]), 3, 0.0, float(q[:, 0].mean()), float(q[:, 1].mean()))
                   for (a, b), q in zip(parents[:e], fr)]
         return events, slots.tolist(), skipped
+
+    def activate_fragments(self, g0: torch.Tensor | None = None) -> np.ndarray:
+        """Make the fragments placed in free slots visible to the analysis
+        (call after the integration of the next batch, with g0 its first
+        sample (4, n) on the device: the new bodies' first sweep segments
+        start there, as a body without a previous sample); returns their
+        indices."""
+        idx = np.flatnonzero(self.pending)
+        if len(idx):
+            self.vis[idx] = 1
+            self.pending[idx] = False
+            if self.prev is not None and g0 is not None:
+                p_idx = torch.as_tensor(idx).to(self.dev)
+                self.prev[0][p_idx] = g0[0][p_idx]
+                self.prev[1][p_idx] = g0[1][p_idx]
+            self.refresh()
+        return idx
 
     def apply_bounce(self, sim, st, res) -> int:
         """Add the bounce deltas to the simulation on the device (apply_bounce,

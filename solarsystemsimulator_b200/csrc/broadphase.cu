@@ -708,10 +708,10 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const unsigned nb_n = (unsigned)((nn + 255) / 256);
     k_sub_keys<<<nb_n, 256, 0, s>>>(x, y, ai, cx, cy, d_na, nn, h, k0, v0);
     SSS_LAUNCH_CHECK(ctx, "k_sub_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s, 12));
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s, ctx->d_status, 12));
     k_gather_keys<<<nb_n, 256, 0, s>>>(rowkey, v0, d_na, nn, k0);
     SSS_LAUNCH_CHECK(ctx, "k_gather_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s));
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s, ctx->d_status));
     k_sorted_records<<<nb_n, 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, d_na, rec, rec2);
     SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
     const long long n_chunks = (nn + 31) / 32;
@@ -720,7 +720,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     // 3) cell runs of the sorted order
     k_run_flags<<<nb_n, 256, 0, s>>>(cx, cy, v0, d_na, nn, flags);
     SSS_LAUNCH_CHECK(ctx, "k_run_flags");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, nn, scan_tmp, s));
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, nn, scan_tmp, s, ctx->d_status));
     // the run count: the scan's total, kept after the items' tile starts
     const long long ntiles_n = (nn + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
     long long* d_nrun = tile_st + 5 * nn + 1;
@@ -733,7 +733,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     k_items<<<(unsigned)((max_items + 255) / 256), 256, 0, s>>>(cx, cy, v0, k0, d_na, run_start, d_nrun, max_items,
                                                                 item_b0, item_nb, tile_st, d_ncand);
     SSS_LAUNCH_CHECK(ctx, "k_items");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(tile_st, tile_st, max_items, scan_tmp, s));
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(tile_st, tile_st, max_items, scan_tmp, s, ctx->d_status));
     const long long itiles = (max_items + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
     long long* d_ntiles = tile_st + 5 * nn + 2;
     SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tile_st + max_items, scan_tmp + itiles, sizeof(long long),
@@ -801,7 +801,7 @@ extern "C" int sss_broadphase_order(sss_ctx* ctx, int* hits, int64_t k, int64_t 
     const unsigned nb = (unsigned)((k + 255) / 256);
     k_hit_keys<<<nb, 256, 0, s>>>((const Hit*)hits, k, B, k0, v0);
     SSS_LAUNCH_CHECK(ctx, "k_hit_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, k, (long long*)(S + o_rs), s, 3 + 2 * B));
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, k, (long long*)(S + o_rs), s, ctx->d_status, 3 + 2 * B));
     SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tmp, hits, 12 * (size_t)k, cudaMemcpyDeviceToDevice, s));
     k_hit_gather<<<nb, 256, 0, s>>>(tmp, v0, k, (Hit*)hits);
     SSS_LAUNCH_CHECK(ctx, "k_hit_gather");

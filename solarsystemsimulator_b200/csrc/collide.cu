@@ -451,10 +451,10 @@ extern "C" int sss_collide_sweep(sss_ctx* ctx, int64_t n, const float* gx, const
     SSS_LAUNCH_CHECK(ctx, "k_sweep_head");
     k_sweep_flags<<<nblk(cells, SW_NT), SW_NT, 0, st>>>(in, head, m_count, flags);
     SSS_LAUNCH_CHECK(ctx, "k_sweep_flags");
-    SSS_CUDA_TRY(ctx, exclusive_scan(flags, pos, cells, scan, st));
+    SSS_CUDA_TRY(ctx, exclusive_scan(flags, pos, cells, scan, st, ctx->d_status));
     k_run_flags<<<nblk(n, SW_NT), SW_NT, 0, st>>>(in, head, rflags);
     SSS_LAUNCH_CHECK(ctx, "k_run_flags");
-    SSS_CUDA_TRY(ctx, exclusive_scan(rflags, rpos, n, rscan, st));
+    SSS_CUDA_TRY(ctx, exclusive_scan(rflags, rpos, n, rscan, st, ctx->d_status));
     long long tot[2];
     const long long tiles = (cells + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
     const long long rtiles = (n + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
@@ -526,7 +526,7 @@ extern "C" int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const
     long long* tscan = (long long*)(b + o_tscan);
     k_hit_keys<<<nblk(n_hits, 256), 256, 0, st>>>(hits, n_hits, k0, v0);
     SSS_LAUNCH_CHECK(ctx, "k_hit_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n_hits, (long long*)(b + o_rs), st));
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n_hits, (long long*)(b + o_rs), st, ctx->d_status));
     k_bounce_filter<<<1, MATCH_NT, 0, st>>>(k0, n_hits, (int*)(b + o_minh), (unsigned char*)(b + o_taken),
                                             (unsigned char*)(b + o_state), keep);
     SSS_LAUNCH_CHECK(ctx, "k_bounce_filter");
@@ -535,8 +535,8 @@ extern "C" int sss_collide_bounce(sss_ctx* ctx, int64_t n, const float* x, const
     BounceIn in{x, y, vx, vy, real_r, mass, (long long)n, dt_y, e};
     k_bounce_apply<<<nblk(n_hits, BF_NT), BF_NT, 0, st>>>(in, k0, keep, n_hits, act, dd, tch);
     SSS_LAUNCH_CHECK(ctx, "k_bounce_apply");
-    SSS_CUDA_TRY(ctx, exclusive_scan(act, apos, n_hits, ascan, st));
-    SSS_CUDA_TRY(ctx, exclusive_scan(tch, tpos, n, tscan, st));
+    SSS_CUDA_TRY(ctx, exclusive_scan(act, apos, n_hits, ascan, st, ctx->d_status));
+    SSS_CUDA_TRY(ctx, exclusive_scan(tch, tpos, n, tscan, st, ctx->d_status));
     k_bounce_pairs_out<<<nblk(n_hits, 256), 256, 0, st>>>(k0, act, apos, n_hits, pairs_out);
     SSS_LAUNCH_CHECK(ctx, "k_bounce_pairs_out");
     k_bounce_touched_out<<<nblk(n, 256), 256, 0, st>>>(n, tch, tpos, dd, (long long*)touched_out, deltas_out);
@@ -688,7 +688,7 @@ extern "C" int sss_collide_fragment(sss_ctx* ctx, int64_t n, const float* x, con
     FragIn in{x, y, vx, vy, real_r, mass, G, factor, (unsigned long long)seed, n_frag};
     k_frag_flags<<<nblk(n_pairs, FRAG_NT), FRAG_NT, 0, st>>>(in, pairs, n_pairs, flags);
     SSS_LAUNCH_CHECK(ctx, "k_frag_flags");
-    SSS_CUDA_TRY(ctx, exclusive_scan(flags, pos, n_pairs, scan, st));
+    SSS_CUDA_TRY(ctx, exclusive_scan(flags, pos, n_pairs, scan, st, ctx->d_status));
     k_frag_write<<<nblk(n_pairs, FRAG_NT), FRAG_NT, 0, st>>>(in, pairs, n_pairs, flags, pos, cap, parents_out,
                                                              frags_out);
     SSS_LAUNCH_CHECK(ctx, "k_frag_write");

@@ -408,7 +408,7 @@ extern "C" int sss_ewald_accel(sss_ctx* ctx, const sss_pm3_particles* src, const
         const unsigned nb = (unsigned)((n + 255) / 256);
         k_src_keys<<<nb, 256, 0, st>>>(ps, 1.0 / box, k0, v0);
         SSS_LAUNCH_CHECK(ctx, "k_src_keys");
-        SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n, (long long*)(base + o_rs), st));
+        SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n, (long long*)(base + o_rs), st, ctx->d_status));
         k_src_gather<<<nb, 256, 0, st>>>(ps, v0, sorted, rank);
         SSS_LAUNCH_CHECK(ctx, "k_src_gather");
     }

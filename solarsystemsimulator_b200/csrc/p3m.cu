@@ -374,7 +374,7 @@ extern "C" int sss_pm3_short(sss_pm3* p, const sss_pm3_particles* s, double G, d
     const double l = p->box / M;
     k_pp_keys<<<blocks_for(n, 256), 256, 0, st>>>(parts, M, 1.0 / l, k0, v0);
     SSS_LAUNCH_CHECK(ctx, "k_pp_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n, (long long*)(B + o_rs), st, bits));
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, n, (long long*)(B + o_rs), st, ctx->d_status, bits));
     k_pp_gather<<<blocks_for(n, 256), 256, 0, st>>>(parts, v0, src);
     SSS_LAUNCH_CHECK(ctx, "k_pp_gather");
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(first, 0, 4 * (size_t)cells, st));
@@ -383,7 +383,7 @@ extern "C" int sss_pm3_short(sss_pm3* p, const sss_pm3_particles* s, double G, d
     SSS_LAUNCH_CHECK(ctx, "k_pp_bounds");
     k_pp_groups<<<blocks_for(cells, 256), 256, 0, st>>>(first, last, cells, groups);
     SSS_LAUNCH_CHECK(ctx, "k_pp_groups");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(groups, offs, cells, (long long*)(B + o_rs), st));
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(groups, offs, cells, (long long*)(B + o_rs), st, ctx->d_status));
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(counters, 0, 8, st));
     k_pp_items<<<blocks_for(cells, 256), 256, 0, st>>>(first, offs, cells, groups, items, counters);
     SSS_LAUNCH_CHECK(ctx, "k_pp_items");

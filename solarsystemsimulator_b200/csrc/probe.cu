@@ -1,6 +1,8 @@
-// FMA-throughput probe: the FP64 / FP32 SIMT peaks the all-pairs kernels
-// are measured against (the driver-measured peaks cover only HBM copy and
-// bf16 tensor GEMM). Diagnostic entry point, no reference counterpart.
+// Throughput probe: the FP64 / FP32 SIMT FMA peaks the all-pairs kernels are
+// measured against (the driver-measured peaks cover only HBM copy and bf16
+// tensor GEMM), and the rate of the f32 reciprocal square root (the special
+// function unit) that bounds the mixed-precision pair loop. Diagnostic entry
+// point, no reference counterpart.
 #include "sss_internal.cuh"
 
 namespace {
@@ -48,11 +50,27 @@ __global__ void __launch_bounds__(256) k_fma_chain_x2(float* out, int iters, flo
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// chains of rsqrt.approx.f32: one special-function operation per step
+__global__ void __launch_bounds__(256) k_rsqrt_chain(float* out, int iters) {
+    float x[CHAINS];
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) x[c] = 1.5f + (float)(threadIdx.x + c) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < CHAINS; ++c) x[c] = sss_rsqrt_approx_f32(x[c]) + 1.0f;
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) s += x[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
 
 extern "C" int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops) {
     if (!ctx || !tflops) return SSS_ERR_ARG;
-    if (kind < 0 || kind > 2) return sss_set_err(ctx, SSS_ERR_ARG, "kind must be 0 (f64), 1 (f32), 2 (f32x2)");
+    if (kind < 0 || kind > 3)
+        return sss_set_err(ctx, SSS_ERR_ARG, "kind must be 0 (f64), 1 (f32), 2 (f32x2), 3 (f32 rsqrt)");
     if (iters < 1) return sss_set_err(ctx, SSS_ERR_ARG, "iters must be >= 1");
     SSS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     const int blocks = ctx->num_sms * 8, threads = 256;
@@ -67,7 +85,8 @@ extern "C" int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops) 
         cudaEventRecord(e0);
         if (kind == 0) k_fma_chain<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
         else if (kind == 1) k_fma_chain<float><<<blocks, threads>>>((float*)out, iters, 0.9999f, 1e-4f);
-        else k_fma_chain_x2<<<blocks, threads>>>((float*)out, iters, 0.9999f, 1e-4f);
+        else if (kind == 2) k_fma_chain_x2<<<blocks, threads>>>((float*)out, iters, 0.9999f, 1e-4f);
+        else k_rsqrt_chain<<<blocks, threads>>>((float*)out, iters);
         cudaEventRecord(e1);
         cudaError_t e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) return sss_cuda_err(ctx, e, "probe kernel");
@@ -77,8 +96,9 @@ extern "C" int sss_probe_fma(sss_ctx* ctx, int kind, int iters, double* tflops) 
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    const double lanes_per_fma = (kind == 2) ? 2.0 : 1.0;
-    const double flops = 2.0 * lanes_per_fma * CHAINS * (double)iters * blocks * threads;
+    // FMA kinds: 2 flops per lane and FMA; rsqrt: 1 operation per step
+    const double per_step = (kind == 2) ? 4.0 : (kind == 3 ? 1.0 : 2.0);
+    const double flops = per_step * CHAINS * (double)iters * blocks * threads;
     *tflops = flops / (best_ms * 1e-3) / 1e12;
     return SSS_OK;
 }

@@ -111,7 +111,7 @@ extern "C" int sss_ring_slot(sss_ctx* ctx, const float* row, int64_t n, const fl
     const unsigned nb = (unsigned)((n_ast + 255) / 256);
     k_hot_flags<<<nb, 256, 0, st>>>(sub_n, n_ast, m_sub, flags);
     SSS_LAUNCH_CHECK(ctx, "k_hot_flags");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, n_ast, scan, st));
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, n_ast, scan, st, ctx->d_status));
     const long long tiles = (n_ast + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
     k_count<<<1, 1, 0, st>>>(scan + tiles, sub_max, count);
     SSS_LAUNCH_CHECK(ctx, "k_count");

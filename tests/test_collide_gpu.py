@@ -358,6 +358,9 @@ def test_fragments_enter_the_simulation():
     out = sim.export_f64(st)
     slots = np.array(used)
     assert len(np.unique(slots)) == slots.size                 # every fragment has its own slot
+    new_slots = np.array([q for sl in used for q in sl[2:]])
+    assert np.all(cr.vis[new_slots] == 0) and np.all(cr.pending[new_slots])   # visible from the next batch
+    assert np.array_equal(np.sort(cr.activate_fragments(gd)), np.sort(new_slots))
     for sl, f in zip(used, frags[:len(used)]):
         assert np.array_equal(out[sl], f[:, 0]) and np.array_equal(out[n + np.array(sl)], f[:, 1])
         assert np.array_equal(out[2 * n + np.array(sl)], f[:, 2])
