@@ -32,6 +32,13 @@ namespace {
 
 constexpr int BP_NT = 256;
 
+// The call's scalars, in device memory: the kernels read them there, so one
+// captured graph of the pipeline serves every call of the same size.
+struct BpParams {
+    float lo, hi_halo, hi, dtf;
+    double h, dt;
+};
+
 __device__ __forceinline__ long long cell_key(long long cx, long long cy) {
     // int64 wrap-around multiply (the reference's `cx * int64(73856093) ^ cy * int64(19349663)`)
     const unsigned long long a = (unsigned long long)cx * 73856093ull;
@@ -46,8 +53,10 @@ __device__ __forceinline__ bool alive_of(const unsigned char* is_ast, const unsi
 
 __global__ void __launch_bounds__(BP_NT) k_alive_count(const unsigned char* __restrict__ is_ast,
                                                        const unsigned char* __restrict__ vis,
-                                                       const float* __restrict__ x, long long n, float lo,
-                                                       float hi_halo, long long* __restrict__ counts) {
+                                                       const float* __restrict__ x, long long n,
+                                                       const BpParams* __restrict__ P,
+                                                       long long* __restrict__ counts) {
+    const float lo = P->lo, hi_halo = P->hi_halo;
     const long long base = (long long)blockIdx.x * sss_dev::SCAN_TILE;
     long long c = 0;
     for (int k = 0; k < sss_dev::SCAN_ITEMS; ++k) {
@@ -63,12 +72,14 @@ __global__ void __launch_bounds__(BP_NT) k_alive_count(const unsigned char* __re
 __global__ void __launch_bounds__(BP_NT) k_alive_scatter(const unsigned char* __restrict__ is_ast,
                                                          const unsigned char* __restrict__ vis,
                                                          const float* __restrict__ x, const float* __restrict__ y,
-                                                         long long n, float lo, float hi_halo, double h,
+                                                         long long n, const BpParams* __restrict__ P,
                                                          const long long* __restrict__ offs,
                                                          unsigned* __restrict__ ai, long long* __restrict__ cx,
                                                          long long* __restrict__ cy,
                                                          unsigned long long* __restrict__ skey,
                                                          unsigned* __restrict__ sval) {
+    const float lo = P->lo, hi_halo = P->hi_halo;
+    const double h = P->h;
     const long long base = (long long)blockIdx.x * sss_dev::SCAN_TILE;
     bool f[sss_dev::SCAN_ITEMS];
     long long c = 0;
@@ -210,10 +221,11 @@ __device__ __forceinline__ unsigned spread2(unsigned v) {
 
 __global__ void k_sub_keys(const float* __restrict__ x, const float* __restrict__ y, const unsigned* __restrict__ ai,
                            const long long* __restrict__ cx, const long long* __restrict__ cy,
-                           const long long* __restrict__ d_na, long long n, double h,
+                           const long long* __restrict__ d_na, long long n, const BpParams* __restrict__ P,
                            unsigned long long* __restrict__ sk, unsigned* __restrict__ sv) {
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
+    const double h = P->h;
     if (r >= *d_na) {                                              // padding up to n: sorts after every row
         sk[r] = 0xFFFull;
         sv[r] = (unsigned)r;
@@ -365,6 +377,7 @@ struct TileArgs {
     const long long* na;         // alive bodies, runs and tiles (device counts)
     const long long* n_run;
     const long long* n_tiles;
+    const BpParams* P;           // dtf, dt, hi of tp come from here
     TestParams tp;
 };
 
@@ -517,7 +530,11 @@ __device__ __forceinline__ void span_walk(const TileArgs& a, int o, const Body& 
 // [-dt, dt] exceeds 2 rs: the f32 test rejects it (its own rounding below
 // 1e-7 AU while the boxes' extents P and V dt stay below 0.5 AU, rs >= 1e-6
 // AU); 4.01 for 4 covers the rounding of the box arithmetic.
-__global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a) {
+__global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a_in) {
+    TileArgs a = a_in;
+    a.tp.dtf = a_in.P->dtf;
+    a.tp.dt = a_in.P->dt;
+    a.tp.hi = a_in.P->hi;
     __shared__ int q_j[BP_NT / 32][QCAP];
     __shared__ unsigned char q_l[BP_NT / 32][QCAP];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -628,6 +645,140 @@ __global__ void k_hit_gather(const Hit* __restrict__ in, const unsigned* __restr
     if (i < k) out[i] = in[order[i]];
 }
 
+// The call's inputs into the staging arrays the captured pipeline reads.
+__global__ void k_bp_stage(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ vx,
+                           const float* __restrict__ vy, const float* __restrict__ rr,
+                           const unsigned char* __restrict__ is_ast, const unsigned char* __restrict__ vis,
+                           long long n, float* __restrict__ f5, unsigned char* __restrict__ u2) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f5[i] = x[i];
+    f5[n + i] = y[i];
+    f5[2 * n + i] = vx[i];
+    f5[3 * n + i] = vy[i];
+    f5[4 * n + i] = rr[i];
+    u2[i] = is_ast[i];
+    u2[n + i] = vis[i];
+}
+
+}  // namespace
+
+// One instantiated graph of the broadphase pipeline per context: the launch
+// sequence depends only on n, the hit capacity and the scratch address, so a
+// call of the same size replays it (one graph launch instead of ~30 launches
+// and clears). Counts come back through pinned host memory.
+struct sss_bp_graph {
+    long long n = -1, cap = -1;
+    void* base = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BpParams* h_par = nullptr;               // pinned
+    unsigned long long* h_cnt = nullptr;     // pinned: hits, candidates, alive
+};
+
+void sss_bp_graph_free(sss_bp_graph* g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->h_par) cudaFreeHost(g->h_par);
+    if (g->h_cnt) cudaFreeHost(g->h_cnt);
+    delete g;
+}
+
+namespace {
+
+// Device pointers of one call's pipeline (all inside the context scratch).
+struct BpBufs {
+    const float *x, *y, *vx, *vy, *rr;
+    const unsigned char *is_ast, *vis;
+    const BpParams* P;
+    long long* counts;
+    long long* scan_tmp;
+    long long *cx, *cy;
+    unsigned long long *k0, *k1;
+    unsigned *v0, *v1, *ai;
+    long long *flags, *pos, *run_start, *item_b0, *item_nb, *tile_st;
+    float4* rec;
+    uint2* rec2;
+    unsigned long long* rowkey;
+    ChunkBox* boxes;
+    unsigned long long* d_nh;   // hits, candidates
+    Hit* hits;
+};
+
+// The launch sequence of one call on stream s (captured into a graph). Every
+// size after the alive count stays on the device: the launches are sized for
+// n bodies (5 n items, a persistent tile grid) and read the counts there.
+int enqueue_pipeline(sss_ctx* ctx, const BpBufs& B, long long nn, long long capacity, cudaStream_t s) {
+    const long long tiles = (nn + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    // 1) alive compaction (ascending body order) + cells + keys
+    k_alive_count<<<(unsigned)tiles, BP_NT, 0, s>>>(B.is_ast, B.vis, B.x, nn, B.P, B.counts);
+    sss_dev::k_scan_sums<<<1, sss_dev::SCAN_NT, 0, s>>>(B.counts, tiles);
+    const long long* d_na = B.counts + tiles;
+    k_alive_scatter<<<(unsigned)tiles, BP_NT, 0, s>>>(B.is_ast, B.vis, B.x, B.y, nn, B.P, B.counts, B.ai, B.cx,
+                                                       B.cy, B.rowkey, B.v0);
+    SSS_LAUNCH_CHECK(ctx, "k_alive_scatter");
+    // 2) sort by the position inside the cell, then stably by the cell key
+    //    (ascending signed order): key, then sub-cell, then body order; the
+    //    n - na padding entries sort last in both
+    const unsigned nb_n = (unsigned)((nn + 255) / 256);
+    k_sub_keys<<<nb_n, 256, 0, s>>>(B.x, B.y, B.ai, B.cx, B.cy, d_na, nn, B.P, B.k0, B.v0);
+    SSS_LAUNCH_CHECK(ctx, "k_sub_keys");
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(B.k0, B.v0, B.k1, B.v1, nn, B.scan_tmp, s, ctx->d_status, 12));
+    k_gather_keys<<<nb_n, 256, 0, s>>>(B.rowkey, B.v0, d_na, nn, B.k0);
+    SSS_LAUNCH_CHECK(ctx, "k_gather_keys");
+    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(B.k0, B.v0, B.k1, B.v1, nn, B.scan_tmp, s, ctx->d_status));
+    k_sorted_records<<<nb_n, 256, 0, s>>>(B.x, B.y, B.vx, B.vy, B.rr, B.ai, B.v0, d_na, B.rec, B.rec2);
+    SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
+    const long long n_chunks = (nn + 31) / 32;
+    k_chunk_boxes<<<(unsigned)((n_chunks * 32 + 255) / 256), 256, 0, s>>>(B.rec, B.rec2, d_na, B.boxes);
+    SSS_LAUNCH_CHECK(ctx, "k_chunk_boxes");
+    // 3) cell runs of the sorted order
+    k_run_flags<<<nb_n, 256, 0, s>>>(B.cx, B.cy, B.v0, d_na, nn, B.flags);
+    SSS_LAUNCH_CHECK(ctx, "k_run_flags");
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(B.flags, B.pos, nn, B.scan_tmp, s, ctx->d_status));
+    // the run count: the scan's total, kept after the items' tile starts
+    const long long ntiles_n = (nn + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    long long* d_nrun = B.tile_st + 5 * nn + 1;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(d_nrun, B.scan_tmp + ntiles_n, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+    k_run_starts<<<nb_n, 256, 0, s>>>(B.flags, B.pos, d_na, B.run_start);
+    SSS_LAUNCH_CHECK(ctx, "k_run_starts");
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(B.d_nh, 0, 2 * sizeof(unsigned long long), s));
+    // 4) (run, offset) items: partner ranges, tiles, candidates
+    const long long max_items = 5 * nn;
+    k_items<<<(unsigned)((max_items + 255) / 256), 256, 0, s>>>(B.cx, B.cy, B.v0, B.k0, d_na, B.run_start, d_nrun,
+                                                                max_items, B.item_b0, B.item_nb, B.tile_st,
+                                                                B.d_nh + 1);
+    SSS_LAUNCH_CHECK(ctx, "k_items");
+    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(B.tile_st, B.tile_st, max_items, B.scan_tmp, s, ctx->d_status));
+    const long long itiles = (max_items + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
+    long long* d_ntiles = B.tile_st + 5 * nn + 2;
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(B.tile_st + max_items, B.scan_tmp + itiles, sizeof(long long),
+                                      cudaMemcpyDeviceToDevice, s));
+    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ntiles, B.scan_tmp + itiles, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+    // 5) tiles: keep rule + tests (a persistent grid; warps split the tiles)
+    TileArgs ta;
+    ta.rec = B.rec;
+    ta.rec2 = B.rec2;
+    ta.run_start = B.run_start;
+    ta.item_b0 = B.item_b0;
+    ta.item_nb = B.item_nb;
+    ta.tile_start = B.tile_st;
+    ta.ks = B.k0;
+    ta.boxes = B.boxes;
+    ta.na = d_na;
+    ta.n_run = d_nrun;
+    ta.n_tiles = d_ntiles;
+    ta.P = B.P;
+    ta.tp.dtf = 0.0f;      // from P in the kernel
+    ta.tp.dt = 0.0;
+    ta.tp.hi = 0.0f;
+    ta.tp.hits = B.hits;
+    ta.tp.cap = capacity;
+    ta.tp.n_hits = B.d_nh;
+    k_tiles<<<(unsigned)(ctx->num_sms * 32), BP_NT, 0, s>>>(ta);
+    SSS_LAUNCH_CHECK(ctx, "k_tiles");
+    return SSS_OK;
+}
+
 }  // namespace
 
 extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, const float* vx, const float* vy,
@@ -647,7 +798,6 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     SSS_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = (cudaStream_t)stream;
     if (n < 2) return SSS_OK;
-    const float hi_halo = hi + (float)halo;      // f32, as `self.hi + cp.float32(halo)`
 
     // scratch layout (long long units)
     const long long tiles = (n + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
@@ -666,111 +816,106 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_rowkey = take(nn);                          // cell key per alive row
     const size_t o_box = take((nn + 31) / 32 * (sizeof(ChunkBox) / 8));
     const size_t o_nh = take(2);
+    const size_t o_par = take(sizeof(BpParams) / 8 + 1);
+    const size_t o_f5 = take((5 * nn + 1) / 2);                // staged x, y, vx, vy, rr (f32)
+    const size_t o_u2 = take((2 * nn + 7) / 8);                // staged is_ast, vis (u8)
+    const size_t o_hits = take(((size_t)capacity * sizeof(Hit) + 7) / 8);
     void* scr = nullptr;
     int rc = sss_scratch(ctx, off * sizeof(long long), &scr);
     if (rc) return rc;
     long long* S = (long long*)scr;
-    long long* counts = S + o_counts;
-    long long* scan_tmp = S + o_scan;
-    long long* cx = S + o_cx;
-    long long* cy = S + o_cy;
-    unsigned long long* k0 = (unsigned long long*)(S + o_k0);
-    unsigned long long* k1 = (unsigned long long*)(S + o_k1);
-    unsigned* v0 = (unsigned*)(S + o_v);
-    unsigned* v1 = v0 + nn;
-    unsigned* ai = (unsigned*)(S + o_ai);
-    long long* flags = S + o_flag;
-    long long* pos = S + o_pos;
-    long long* run_start = S + o_run;
-    long long* item_b0 = S + o_ib0;
-    long long* item_nb = S + o_inb;
-    long long* tile_st = S + o_tst;
-    float4* rec = (float4*)(S + o_rec);
-    uint2* rec2 = (uint2*)(S + o_rec2);
-    unsigned long long* d_nh = (unsigned long long*)(S + o_nh);
-    unsigned long long* rowkey = (unsigned long long*)(S + o_rowkey);
-    ChunkBox* boxes = (ChunkBox*)(S + o_box);
-    unsigned long long* d_ncand = d_nh + 1;
+    BpBufs B;
+    float* f5 = (float*)(S + o_f5);
+    unsigned char* u2 = (unsigned char*)(S + o_u2);
+    B.x = f5;
+    B.y = f5 + nn;
+    B.vx = f5 + 2 * nn;
+    B.vy = f5 + 3 * nn;
+    B.rr = f5 + 4 * nn;
+    B.is_ast = u2;
+    B.vis = u2 + nn;
+    B.P = (const BpParams*)(S + o_par);
+    B.counts = S + o_counts;
+    B.scan_tmp = S + o_scan;
+    B.cx = S + o_cx;
+    B.cy = S + o_cy;
+    B.k0 = (unsigned long long*)(S + o_k0);
+    B.k1 = (unsigned long long*)(S + o_k1);
+    B.v0 = (unsigned*)(S + o_v);
+    B.v1 = B.v0 + nn;
+    B.ai = (unsigned*)(S + o_ai);
+    B.flags = S + o_flag;
+    B.pos = S + o_pos;
+    B.run_start = S + o_run;
+    B.item_b0 = S + o_ib0;
+    B.item_nb = S + o_inb;
+    B.tile_st = S + o_tst;
+    B.rec = (float4*)(S + o_rec);
+    B.rec2 = (uint2*)(S + o_rec2);
+    B.rowkey = (unsigned long long*)(S + o_rowkey);
+    B.boxes = (ChunkBox*)(S + o_box);
+    B.d_nh = (unsigned long long*)(S + o_nh);
+    B.hits = (Hit*)(S + o_hits);
 
-    // Every size after the alive count stays on the device: the launches are
-    // sized for n bodies (5 n items, a persistent tile grid) and read the
-    // counts there, so the call has one host readback, at the end.
-    // 1) alive compaction (ascending body order) + cells + keys
-    k_alive_count<<<(unsigned)tiles, BP_NT, 0, s>>>(is_ast, vis, x, nn, lo, hi_halo, counts);
-    sss_dev::k_scan_sums<<<1, sss_dev::SCAN_NT, 0, s>>>(counts, tiles);
-    const long long* d_na = counts + tiles;
-    k_alive_scatter<<<(unsigned)tiles, BP_NT, 0, s>>>(is_ast, vis, x, y, nn, lo, hi_halo, h, counts, ai, cx, cy,
-                                                       rowkey, v0);
-    SSS_LAUNCH_CHECK(ctx, "k_alive_scatter");
-    // 2) sort by the position inside the cell, then stably by the cell key
-    //    (ascending signed order): key, then sub-cell, then body order; the
-    //    n - na padding entries sort last in both
-    const unsigned nb_n = (unsigned)((nn + 255) / 256);
-    k_sub_keys<<<nb_n, 256, 0, s>>>(x, y, ai, cx, cy, d_na, nn, h, k0, v0);
-    SSS_LAUNCH_CHECK(ctx, "k_sub_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s, ctx->d_status, 12));
-    k_gather_keys<<<nb_n, 256, 0, s>>>(rowkey, v0, d_na, nn, k0);
-    SSS_LAUNCH_CHECK(ctx, "k_gather_keys");
-    SSS_CUDA_TRY(ctx, sss_dev::radix_sort(k0, v0, k1, v1, nn, scan_tmp, s, ctx->d_status));
-    k_sorted_records<<<nb_n, 256, 0, s>>>(x, y, vx, vy, rr, ai, v0, d_na, rec, rec2);
-    SSS_LAUNCH_CHECK(ctx, "k_sorted_records");
-    const long long n_chunks = (nn + 31) / 32;
-    k_chunk_boxes<<<(unsigned)((n_chunks * 32 + 255) / 256), 256, 0, s>>>(rec, rec2, d_na, boxes);
-    SSS_LAUNCH_CHECK(ctx, "k_chunk_boxes");
-    // 3) cell runs of the sorted order
-    k_run_flags<<<nb_n, 256, 0, s>>>(cx, cy, v0, d_na, nn, flags);
-    SSS_LAUNCH_CHECK(ctx, "k_run_flags");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(flags, pos, nn, scan_tmp, s, ctx->d_status));
-    // the run count: the scan's total, kept after the items' tile starts
-    const long long ntiles_n = (nn + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
-    long long* d_nrun = tile_st + 5 * nn + 1;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(d_nrun, scan_tmp + ntiles_n, sizeof(long long), cudaMemcpyDeviceToDevice, s));
-    k_run_starts<<<nb_n, 256, 0, s>>>(flags, pos, d_na, run_start);
-    SSS_LAUNCH_CHECK(ctx, "k_run_starts");
-    SSS_CUDA_TRY(ctx, cudaMemsetAsync(d_nh, 0, 2 * sizeof(unsigned long long), s));
-    // 4) (run, offset) items: partner ranges, tiles, candidates
-    const long long max_items = 5 * nn;
-    k_items<<<(unsigned)((max_items + 255) / 256), 256, 0, s>>>(cx, cy, v0, k0, d_na, run_start, d_nrun, max_items,
-                                                                item_b0, item_nb, tile_st, d_ncand);
-    SSS_LAUNCH_CHECK(ctx, "k_items");
-    SSS_CUDA_TRY(ctx, sss_dev::exclusive_scan(tile_st, tile_st, max_items, scan_tmp, s, ctx->d_status));
-    const long long itiles = (max_items + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
-    long long* d_ntiles = tile_st + 5 * nn + 2;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(tile_st + max_items, scan_tmp + itiles, sizeof(long long),
-                                      cudaMemcpyDeviceToDevice, s));
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(d_ntiles, scan_tmp + itiles, sizeof(long long), cudaMemcpyDeviceToDevice, s));
-    // 5) tiles: keep rule + tests (a persistent grid; warps split the tiles)
-    TileArgs ta;
-    ta.rec = rec;
-    ta.rec2 = rec2;
-    ta.run_start = run_start;
-    ta.item_b0 = item_b0;
-    ta.item_nb = item_nb;
-    ta.tile_start = tile_st;
-    ta.ks = k0;
-    ta.boxes = boxes;
-    ta.na = d_na;
-    ta.n_run = d_nrun;
-    ta.n_tiles = d_ntiles;
-    ta.tp.dtf = (float)dt_y;
-    ta.tp.dt = dt_y;
-    ta.tp.hi = hi;
-    ta.tp.hits = (Hit*)out_hits;
-    ta.tp.cap = capacity;
-    ta.tp.n_hits = d_nh;
-    k_tiles<<<(unsigned)(ctx->num_sms * 32), BP_NT, 0, s>>>(ta);
-    SSS_LAUNCH_CHECK(ctx, "k_tiles");
-    unsigned long long res[2] = {0, 0};
-    long long na = 0;
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(res, d_nh, sizeof(res), cudaMemcpyDeviceToHost, s));
-    SSS_CUDA_TRY(ctx, cudaMemcpyAsync(&na, d_na, sizeof(na), cudaMemcpyDeviceToHost, s));
+    // the graph of this size (captured on the first call of a size)
+    sss_bp_graph* g = ctx->bp_graph;
+    if (!g || g->n != nn || g->cap != capacity || g->base != scr) {
+        sss_bp_graph_free(g);
+        ctx->bp_graph = nullptr;
+        g = new sss_bp_graph();
+        cudaError_t e = cudaMallocHost((void**)&g->h_par, sizeof(BpParams));
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&g->h_cnt, 3 * sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            sss_bp_graph_free(g);
+            return sss_cuda_err(ctx, e, "cudaMallocHost (broadphase graph)");
+        }
+        // capture on a private stream, so that the caller's stream never is in capture mode
+        cudaStream_t cs;
+        SSS_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        int prc = SSS_OK;
+        if (e == cudaSuccess) {
+            e = cudaMemcpyAsync((void*)B.P, g->h_par, sizeof(BpParams), cudaMemcpyHostToDevice, cs);
+            if (e == cudaSuccess) prc = enqueue_pipeline(ctx, B, nn, capacity, cs);
+            if (e == cudaSuccess && prc == SSS_OK)
+                e = cudaMemcpyAsync(g->h_cnt, B.d_nh, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, cs);
+            if (e == cudaSuccess && prc == SSS_OK)
+                e = cudaMemcpyAsync(g->h_cnt + 2, B.counts + tiles, sizeof(long long), cudaMemcpyDeviceToHost, cs);
+            const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+            if (e == cudaSuccess) e = e2;
+        }
+        if (e == cudaSuccess && prc == SSS_OK) e = cudaGraphInstantiate(&g->exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (prc != SSS_OK || e != cudaSuccess) {
+            sss_bp_graph_free(g);
+            return prc != SSS_OK ? prc : sss_cuda_err(ctx, e, "broadphase graph capture");
+        }
+        g->n = nn;
+        g->cap = capacity;
+        g->base = scr;
+        ctx->bp_graph = g;
+    }
+    g->h_par->lo = lo;
+    g->h_par->hi_halo = hi + (float)halo;    // f32, as `self.hi + cp.float32(halo)`
+    g->h_par->hi = hi;
+    g->h_par->dtf = (float)dt_y;
+    g->h_par->h = h;
+    g->h_par->dt = dt_y;
+    k_bp_stage<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(x, y, vx, vy, rr, is_ast, vis, nn, f5, u2);
+    SSS_LAUNCH_CHECK(ctx, "k_bp_stage");
+    SSS_CUDA_TRY(ctx, cudaGraphLaunch(g->exec, s));
     SSS_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    const unsigned long long nh = g->h_cnt[0], nc = g->h_cnt[1];
+    const long long na = (long long)g->h_cnt[2];
     if (na < 2) return SSS_OK;                   // fewer than two alive asteroids: no candidates, no hits
-    *n_cand = (int64_t)res[1];
-    *n_hits = (int64_t)res[0];
-    if ((long long)res[0] > capacity)
-        return sss_set_err(ctx, SSS_ERR_CAPACITY, "hit buffer holds %lld, %llu hits found", (long long)capacity,
-                           res[0]);
+    *n_cand = (int64_t)nc;
+    *n_hits = (int64_t)nh;
+    if ((long long)nh > capacity)
+        return sss_set_err(ctx, SSS_ERR_CAPACITY, "hit buffer holds %lld, %llu hits found", (long long)capacity, nh);
+    if (nh > 0)
+        SSS_CUDA_TRY(ctx, cudaMemcpyAsync(out_hits, B.hits, (size_t)nh * sizeof(Hit), cudaMemcpyDeviceToDevice, s));
     return SSS_OK;
 }
 

@@ -88,6 +88,7 @@ extern "C" void sss_destroy(sss_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    sss_bp_graph_free(ctx->bp_graph);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->d_status) cudaFree(ctx->d_status);

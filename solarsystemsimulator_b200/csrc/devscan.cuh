@@ -105,28 +105,45 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_1pass(const long long* in, lon
     }
     long long tot;
     long long run = block_exclusive_scan(s, &tot);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // warp 0 walks back 32 tiles at a time: lane l reads tile pos - l; the
+        // nearest tile with its inclusive prefix published ends the walk
+        const int lane = threadIdx.x;
         long long excl = 0;
         if (tile > 0) {
-            st.agg[tile] = tot;
-            __threadfence();
-            atomicExch(&st.flag[tile], 1);
-            for (long long t = tile - 1; t >= 0; --t) {
-                int f;
-                if (!spin_until<int>(st.flag + t, f, [](int q) { return q != 0; }, err)) break;
+            if (lane == 0) {
+                st.agg[tile] = tot;
                 __threadfence();
-                if (f == 2) {
-                    excl += *(volatile long long*)(st.inc + t);
-                    break;
+                atomicExch(&st.flag[tile], 1);
+            }
+            for (long long pos = tile - 1;; pos -= 32) {
+                const long long idx = pos - lane;
+                int f = 2;                      // before tile 0: an inclusive prefix of 0
+                long long val = 0;
+                if (idx >= 0) {
+                    if (spin_until<int>(st.flag + idx, f, [](int q) { return q != 0; }, err)) {
+                        __threadfence();
+                        val = (f == 2) ? *(volatile long long*)(st.inc + idx) : *(volatile long long*)(st.agg + idx);
+                    } else {
+                        f = 2;                  // timed out (status set): stop here
+                    }
                 }
-                excl += *(volatile long long*)(st.agg + t);
+                const unsigned incm = __ballot_sync(0xffffffffu, f == 2);
+                const int first = incm ? __ffs(incm) - 1 : 32;
+                if (lane > first) val = 0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+                excl += val;
+                if (incm) break;
             }
         }
-        st.inc[tile] = excl + tot;
-        __threadfence();
-        atomicExch(&st.flag[tile], 2);
-        if (tile == tiles - 1) *st.total = excl + tot;
-        s_excl = excl;
+        if (lane == 0) {
+            st.inc[tile] = excl + tot;
+            __threadfence();
+            atomicExch(&st.flag[tile], 2);
+            if (tile == tiles - 1) *st.total = excl + tot;
+            s_excl = excl;
+        }
     }
     __syncthreads();
     run += s_excl;

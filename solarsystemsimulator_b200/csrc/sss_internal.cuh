@@ -26,7 +26,11 @@ struct sss_ctx {
     size_t n_counters;
     // cached CTAs-per-SM of the all-pairs kernels (0 = not yet queried)
     int occ[8];
+    // the broadphase pipeline as an instantiated graph (broadphase.cu)
+    struct sss_bp_graph* bp_graph;
 };
+
+void sss_bp_graph_free(struct sss_bp_graph* g);
 
 int sss_set_err(sss_ctx* ctx, int code, const char* fmt, ...);
 int sss_cuda_err(sss_ctx* ctx, cudaError_t e, const char* what);
