@@ -540,6 +540,7 @@ def measure_broadphase(dev, stream, reps=5):
     res, cand = bp.bounce_hits(*dev_t, dt, h, halo, rr=rr_t, device=dev)   # warm-up
     t = _ev_time(lambda: bp.bounce_hits(*dev_t, dt, h, halo, rr=rr_t, device=dev), stream, reps)
     ones = torch.ones(len(rr), dtype=torch.uint8, device=f"cuda:{dev}")
+    bp.bounce_hits_device(*dev_t, dt, h, halo, rr=rr_t, is_ast=ones, vis=ones, device=dev)   # warm-up
     t_dev = _ev_time(lambda: bp.bounce_hits_device(*dev_t, dt, h, halo, rr=rr_t, is_ast=ones, vis=ones,
                                                    device=dev), stream, max(reps, 20))
     fs, rrs, dts, hs, halos = scene(4_000)
