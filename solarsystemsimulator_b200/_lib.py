@@ -22,6 +22,7 @@ SSS_ERR_CAPACITY = 6
 
 PREC_F64 = 0
 PREC_MIXED = 1
+PREC_MIXED_TC = 2
 INT_KDK = 0
 INT_YOSHIDA4 = 1
 

@@ -28,7 +28,7 @@
 // MIX_SUB sources and folded into f64 accumulators. The f32 arithmetic is
 // issued as packed f32x2 instructions (two targets per instruction).
 
-#include "sss_internal.cuh"
+#include "allpairs.cuh"
 
 #include <pthread.h>
 
@@ -53,16 +53,8 @@ constexpr int WAVES = 16;       // target number of CTA waves per evaluation
 // r2 below this is outside the integer-seeded rsqrt's range (2^-126)
 constexpr double kIseedMinR2 = 1.1754943508222875e-38;
 
-struct Epi {
-    int mode;            // 0: write accelerations only; 1: integrator step
-    int last;            // mode 1: no opening kick / drift after this force
-    double4* acc;        // out: accelerations (both modes)
-    double4* vel;        // mode 1
-    double4* pos_nxt;    // mode 1: drifted positions
-    float* snap;         // mode 1: snapshot row or nullptr
-    double kc, ko, kd;   // closing kick, opening kick, drift factors
-    int64_t n_src, n_tr; // snapshot layout
-};
+using sss_ap::Epi;
+using sss_ap::epilogue;
 
 struct ForceArgs {
     const double4* src;      // f64 path: sources
@@ -80,48 +72,6 @@ struct ForceArgs {
     int* status;
     Epi epi;
 };
-
-template <int D>
-__device__ __forceinline__ void epilogue(const Epi& e, int64_t i, double ax, double ay,
-                                         double az, const double4& p) {
-    e.acc[i] = make_double4(ax, ay, az, 0.0);
-    if (e.mode == 0) return;
-    double4 v = e.vel[i];
-    // closing half kick, as `vx[i] += a0 * (0.5 * dt)` (selfgrav_kernel.py:366-367)
-    v.x += ax * e.kc;
-    v.y += ay * e.kc;
-    if (D == 3) v.z += az * e.kc;
-    if (e.snap != nullptr) {
-        if (i < e.n_src) {
-            const int64_t n = e.n_src;
-            e.snap[i] = (float)p.x;
-            e.snap[n + i] = (float)p.y;
-            if (D == 3) e.snap[2 * n + i] = (float)p.z;
-            float* sv = e.snap + D * n;
-            sv[i] = (float)v.x;
-            sv[n + i] = (float)v.y;
-            if (D == 3) sv[2 * n + i] = (float)v.z;
-        } else {
-            const int64_t t = i - e.n_src, m = e.n_tr;
-            float* st = e.snap + 2 * D * e.n_src;
-            st[t] = (float)p.x;
-            st[m + t] = (float)p.y;
-            if (D == 3) st[2 * m + t] = (float)p.z;
-        }
-    }
-    double4 q = p;
-    if (!e.last) {
-        // next opening half kick + drift (selfgrav_kernel.py:335-346)
-        v.x += ax * e.ko;
-        v.y += ay * e.ko;
-        if (D == 3) v.z += az * e.ko;
-        q.x = p.x + v.x * e.kd;
-        q.y = p.y + v.y * e.kd;
-        if (D == 3) q.z = p.z + v.z * e.kd;
-    }
-    e.vel[i] = v;
-    e.pos_nxt[i] = q;
-}
 
 // Chunk partial -> (last arriving CTA) fixed-order sum -> epilogue.
 template <int D, int R, int NT>
@@ -695,6 +645,8 @@ int force_eval(sss_ctx* ctx, int dim, int precision, const double4* src, int64_t
     if (n_src <= 0) return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: n_src must be >= 1");
     if (n_src > ((int64_t)1 << 40) || n_tgt > ((int64_t)1 << 40))
         return sss_set_err(ctx, SSS_ERR_ARG, "all-pairs: size out of range");
+    if (precision == SSS_PREC_MIXED_TC)
+        return sss_ap::force_eval_tc(ctx, dim, src, n_src, tgt, n_tgt, eps2, epi, stream);
     const KSel ks = select_kernel(dim, precision, eps2);
     if (ctx->occ[ks.key] == 0) {
         int per_sm = 0;
@@ -748,8 +700,9 @@ int force_eval(sss_ctx* ctx, int dim, int precision, const double4* src, int64_t
 int check_common(sss_ctx* ctx, int dim, int precision) {
     if (!ctx) return SSS_ERR_ARG;
     if (dim != 2 && dim != 3) return sss_set_err(ctx, SSS_ERR_ARG, "dim must be 2 or 3 (got %d)", dim);
-    if (precision != SSS_PREC_F64 && precision != SSS_PREC_MIXED)
-        return sss_set_err(ctx, SSS_ERR_ARG, "precision must be SSS_PREC_F64 or SSS_PREC_MIXED (got %d)", precision);
+    if (precision != SSS_PREC_F64 && precision != SSS_PREC_MIXED && precision != SSS_PREC_MIXED_TC)
+        return sss_set_err(ctx, SSS_ERR_ARG,
+                           "precision must be SSS_PREC_F64, SSS_PREC_MIXED or SSS_PREC_MIXED_TC (got %d)", precision);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return sss_set_err(ctx, SSS_ERR_CUDA, "cudaSetDevice failed");
     return SSS_OK;
 }

@@ -10,8 +10,9 @@ bodies, Kernel B: massless tracers). Same call surface:
 
 Additive keyword arguments (absent in the reference): `G` (default G_AU, the
 reference's AU/year/Msun constant), `integrator` ("kdk" = the reference's
-leapfrog, "yoshida4"), `precision` ("f64" or "mixed"; by default
-kraft_f32=True selects "mixed", kraft_f32=False "f64"), and for 3-D states
+leapfrog, "yoshida4"), `precision` ("f64", "mixed" or "mixed_tc", the
+mixed pair terms formed on the tensor cores; by default kraft_f32=True
+selects "mixed", kraft_f32=False "f64"), and for 3-D states
 `z=`, `vz=` in load_state plus `tracer_z=(tz, tvz)`. With z given the
 snapshot rows are [x|y|z|vx|vy|vz | tx|ty|tz] (6N + 3T).
 
@@ -33,7 +34,7 @@ G_MAX = 8                         # reference multi-GPU limit (gpu_verbund.py:30
 
 _INTEGRATORS = {"kdk": _lib.INT_KDK, "leapfrog": _lib.INT_KDK,
                 "yoshida4": _lib.INT_YOSHIDA4, "yoshida": _lib.INT_YOSHIDA4}
-_PRECISIONS = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED}
+_PRECISIONS = {"f64": _lib.PREC_F64, "mixed": _lib.PREC_MIXED, "mixed_tc": _lib.PREC_MIXED_TC}
 
 
 def _dev(device: int) -> torch.device:
