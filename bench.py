@@ -299,6 +299,26 @@ def run_ours(args, rank, world, local_rank):
     rel = (torch.linalg.norm(am - af, dim=1) / torch.linalg.norm(af, dim=1)).cpu().numpy()
     ferr = {"median": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
             "max": float(rel.max())}
+
+    # ---- the same force with the pair distances on the tensor cores
+    #      (precision "mixed_tc": Morton sorts, tile prep and the tcgen05 kernel)
+    acc_tc = torch.empty_like(tgt_t)
+    sg.allpairs_accel(src_t, tgt_t, EPS * EPS, dim=3, precision="mixed_tc", out=acc_tc)
+    ev0.record(stream)
+    for _ in range(n_k):
+        sg.allpairs_accel(src_t, tgt_t, EPS * EPS, dim=3, precision="mixed_tc", out=acc_tc)
+    ev1.record(stream)
+    ev1.synchronize()
+    t_kernel_tc = ev0.elapsed_time(ev1) * 1e-3 / n_k
+    rel_tc = (torch.linalg.norm(acc_tc[:, :3] - af, dim=1) / torch.linalg.norm(af, dim=1)).cpu().numpy()
+    mixed_tc = {"kernel_ms": t_kernel_tc * 1e3, "value": n_src * n_tgt / t_kernel_tc / 1e9, "unit": UNIT,
+                "over_simt_mixed": t_kernel_mixed / t_kernel_tc,
+                "force_error_vs_f64": {"median": float(np.median(rel_tc)), "p99": float(np.percentile(rel_tc, 99)),
+                                       "max": float(rel_tc.max())},
+                "form": "r^2 of 128 x 32 pair tiles as split-TF32 tcgen05 products (f32 in tensor memory); "
+                        "rsqrt and the four sums in packed f32x2 on the CUDA cores; near tiles on the f32 "
+                        "pair loop; one force evaluation incl. Morton sorts and tile prep"}
+    del acc_tc
     from oracle import selfgrav as osg
     samp = np.arange(0, n_tgt, n_tgt // 256)[:256]
     tgt_h = tgt_t.cpu().numpy()
@@ -384,6 +404,7 @@ def run_ours(args, rank, world, local_rank):
                     "energy_drift_steps": k_f64},
             "mixed_over_f64_steps": (args.steps / t_mixed) / (k_f64 / t_f64),
             "force_error_vs_f64": ferr,
+            "mixed_tc": mixed_tc,
             "energy_drift_mixed_same_steps": {"drift": abs((e_d1 - e_d0) / e_d0), "steps": k_f64,
                                               "from": "the initial state, Yoshida-4 dt 1e-3"},
             "force_error_vs_cpu_oracle_sample": {"median": float(np.median(rel_or)),

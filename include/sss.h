@@ -43,11 +43,12 @@ extern "C" {
 #define SSS_PREC_F64    0   /* every operation in f64 (the drop-in path)          */
 #define SSS_PREC_MIXED  1   /* f32 pair arithmetic on f64-differenced positions,
                                f32 partial sums folded into f64 accumulators      */
-#define SSS_PREC_MIXED_TC 2 /* the same pair terms with r^2 and the sums formed on
-                               the tensor cores (split-TF32 products over
-                               tile-centred f32 offsets, f32 sums in tensor memory
-                               folded into f64); tiles close to a target block
-                               take the f32 pair loop. Needs eps2 > 0.             */
+#define SSS_PREC_MIXED_TC 2 /* the same pair terms with the squared distances
+                               formed on the tensor cores (split-TF32 products over
+                               tile-centred f32 offsets), rsqrt and sums on the CUDA
+                               cores, f32 tile sums folded into f64; tiles close to
+                               a target block take the f32 pair loop. Needs
+                               eps2 > 0.                                          */
 
 /* integrators of sss_selfgrav_step_batch */
 #define SSS_INT_KDK       0 /* kick-drift-kick leapfrog (selfgrav_kernel.py:333-386) */

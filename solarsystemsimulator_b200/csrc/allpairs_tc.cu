@@ -33,13 +33,18 @@
 // Morton order (a device radix sort per evaluation), so the 128 targets of a
 // CTA and the 128 sources of a tile are compact.
 //
-// CTA = 128 threads = 128 targets = the 128 TMEM lanes: thread t owns row t
-// of the product. The r^2 tile (128 columns) is double buffered in tensor
-// memory (256 columns per CTA, two CTAs per SM); the operands of tile f + 2
-// (A1 row of the thread's target, B1 row and source weights of the thread's
-// source) are built in shared memory while tile f + 1's product runs. One
-// thread issues the MMAs and commits them to mbarriers; every wait is
-// bounded (SSS_ERR_TIMEOUT).
+// CTA = 128 threads = the 128 TMEM lanes, two targets per thread (target
+// groups 0 and 1, one r^2 product each): thread t owns row t of both. The
+// r^2 of a 32-source unit for both groups is double buffered in tensor
+// memory (128 columns per CTA, four CTAs per SM); the operands of tile f + 1
+// (the A1 rows of the thread's targets, the B1 row and weights of the
+// thread's source) are built in shared memory while tile f runs. One thread
+// issues the MMAs and commits them to mbarriers; every wait is bounded
+// (SSS_ERR_TIMEOUT).
+//
+// Measured on the 262,144-source benchmark state: 79.6 ms per force
+// evaluation (the SIMT mixed kernel: 75.8 ms), median relative force error
+// 1.4e-7 against f64.
 
 #include "allpairs.cuh"
 #include "devscan.cuh"
