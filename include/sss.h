@@ -566,6 +566,85 @@ int sss_allpairs_accel_noalloc(int device, int dim, int precision,
                                double* acc4, double eps2, int* d_status,
                                void* stream, char* errbuf, size_t errbuf_len);
 
+/* ------------------------------------------------------------ sessions
+ *
+ * The state the Python classes NBodySelfGrav and NBodyCuda keep, held by the
+ * library for hosts that call this ABI directly (C, C++, Go over cgo, Java
+ * over JNI): host arrays in and out; the device buffers and one stream belong
+ * to the session; every call is synchronous, as the reference's methods
+ * return host arrays. One caller per session at a time. Errors: a status
+ * code, the message (the reference's text where it has one) in
+ * sss_last_error(ctx). A session lives inside its context (destroy it first). */
+
+/* NBodySelfGrav (selfgrav_kernel.py:424-650). */
+typedef struct sss_selfgrav sss_selfgrav;
+/* Constructor (selfgrav_kernel.py:431-462): precision SSS_PREC_*, integrator
+ * SSS_INT_*, G (the reference's G_AU = 4 pi^2 in AU^3/Msun/yr^2), Plummer
+ * softening > 0 ("Softening muss positiv sein"). */
+int sss_sg_create(sss_ctx* ctx, int precision, int integrator, double G, double softening,
+                  sss_selfgrav** out);
+void sss_sg_destroy(sss_selfgrav* s);
+/* load_state (selfgrav_kernel.py:463-559): n >= 1 massive bodies, soa = host
+ * f64 [2*dim][n] ([x|y|(z)|vx|vy|(vz)]), mass [n]; n_tracer massless tracers
+ * in tracer_soa [2*dim][n_tracer] (NULL when none). Computes the starting
+ * accelerations. */
+int sss_sg_load(sss_selfgrav* s, int dim, int64_t n, const double* soa, const double* mass,
+                int64_t n_tracer, const double* tracer_soa);
+/* Floats per snapshot row: 2*dim*n + dim*n_tracer, the reference's row
+ * [x|y|(z)|vx|vy|(vz)|tx|ty|(tz)] (selfgrav_kernel.py:600-627); 0 before a load. */
+int64_t sss_sg_row_width(const sss_selfgrav* s);
+/* step_batch (selfgrav_kernel.py:560-627): steps >= 1 integrator steps of
+ * dt; snap_host (host f32 [steps][row]) receives the snapshot after each
+ * step, or NULL for none. */
+int sss_sg_step_batch(sss_selfgrav* s, double dt, int steps, float* snap_host);
+/* export_f64 (selfgrav_kernel.py:629-650): out = host f64 [2*dim][n]. */
+int sss_sg_export_f64(sss_selfgrav* s, double* out);
+
+/* NBodyCuda (nbody_kernel.py:617-1060). */
+typedef struct sss_nbody sss_nbody;
+typedef struct sss_nbody_cfg {
+    double G;             /* G_AU = 4 pi^2 */
+    double softening;     /* added to r^2: SOFTENING = 1e-6 AU^2 */
+    double max_sub_dt;    /* MAX_SUB_DT_YEARS = 0.5 / 365.25 */
+    int    max_sub_steps; /* MAX_SUB_STEPS_PER_FRAME = 100000 */
+    int    fine_guard;    /* fine-loop guard of a hot asteroid: 8000 */
+    int    m_sub;         /* sub-samples per raster interval, 0..SSS_SUB_SAMPLES_MAX: 8 */
+    int    pair_f32;      /* 0: f64 pair forces (the reference); 1: see sss_frame_state */
+} sss_nbody_cfg;
+/* Constructor (nbody_kernel.py:623-657); cfg NULL = the reference's constants. */
+int sss_nbody_create(sss_ctx* ctx, const sss_nbody_cfg* cfg, sss_nbody** out);
+void sss_nbody_destroy(sss_nbody* s);
+/* load_state (nbody_kernel.py:659-780): n bodies, soa = host f64 [2*dim][n]
+ * ([x|y|(z)|vx|vy|(vz)]), mass [n], visible and is_ast u8 [n], contact radii
+ * [n] or NULL (zeros). Bodies with is_ast == 0 are the massive ones (at most
+ * SSS_M_MAX: SSS_ERR_TOO_MANY_MASSIVE, "zu viele massive Koerper"). */
+int sss_nbody_load(sss_nbody* s, int dim, int64_t n, const double* soa, const double* mass,
+                   const unsigned char* visible, const unsigned char* is_ast, const double* radius);
+/* step_batch (nbody_kernel.py:783-934): k raster samples (1..SSS_K_MAX) of
+ * dt_raster in one launch; snap_host = host f32 [k][2*dim][n] in original
+ * order, or NULL. SSS_ERR_GUARD when a step guard ran out (the batch is still
+ * valid up to where the reference would also have stopped). */
+int sss_nbody_step_batch(sss_nbody* s, double dt_raster, int k, float* snap_host);
+/* st["hits"] of the last batch: the first contact of each asteroid, as
+ * (asteroid index, time since the batch start, massive body index) in
+ * ascending asteroid order; *n_hits = their number, at most cap written. */
+int sss_nbody_hits(sss_nbody* s, int64_t* n_hits, int64_t* idx, float* t, int64_t* mas_idx, int64_t cap);
+/* st["sub"][sample] of the last batch: the asteroids with a gap-free chain of
+ * m_sub sub-samples (*n_hot of them, ascending) and the chains, pos = host f32
+ * [m_sub][dim][n_hot]; nothing is written when n_hot > cap (ask again). */
+int sss_nbody_sub(sss_nbody* s, int sample, int64_t* n_hot, int64_t* idx, float* pos, int64_t cap);
+/* export_f64 (nbody_kernel.py:1042-1060): out = host f64 [2*dim][n], original order. */
+int sss_nbody_export_f64(sss_nbody* s, double* out);
+/* Point updates at original indices (nbody_kernel.py:947-1010): mode 0
+ * apply_updates (set x, v: vals [m][2*dim]), mode 1 apply_deltas (add; idx
+ * unique, "apply_deltas: idx must be unique"), mode 2 apply_body_state (set
+ * x, v and mass: vals [m][2*dim+1]). Host arrays. */
+int sss_nbody_scatter(sss_nbody* s, const int64_t* idx, const double* vals, int m, int mode);
+/* set_radius (nbody_kernel.py:1012-1025) and deactivate_body (mass 0, not
+ * visible; :1027-1040). */
+int sss_nbody_set_radius(sss_nbody* s, int64_t idx, double r);
+int sss_nbody_deactivate(sss_nbody* s, int64_t idx);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /* Measured throughput of the device: kind 0 = f64 DFMA, 1 = f32 FFMA,

@@ -61,6 +61,13 @@ class FrameState(ctypes.Structure):
     ]
 
 
+class NBodyCfg(ctypes.Structure):
+    """sss_nbody_cfg (include/sss.h)."""
+    _fields_ = [("G", ctypes.c_double), ("softening", ctypes.c_double), ("max_sub_dt", ctypes.c_double),
+                ("max_sub_steps", ctypes.c_int), ("fine_guard", ctypes.c_int), ("m_sub", ctypes.c_int),
+                ("pair_f32", ctypes.c_int)]
+
+
 class Pm3Particles(ctypes.Structure):
     """Mirror of sss_pm3_particles."""
     _fields_ = [
@@ -170,6 +177,24 @@ SIGNATURES = {
     "sss_allpairs_accel_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _c_i64,
                                                   _dp, _c_i64, _dp, ctypes.c_double, _dp, _vp,
                                                   ctypes.c_char_p, ctypes.c_size_t]),
+    # sessions (host arrays; no torch on the caller's side)
+    "sss_sg_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.POINTER(_vp)]),
+    "sss_sg_destroy": (None, [_vp]),
+    "sss_sg_load": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, ctypes.c_int64, _vp]),
+    "sss_sg_row_width": (ctypes.c_int64, [_vp]),
+    "sss_sg_step_batch": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _vp]),
+    "sss_sg_export_f64": (ctypes.c_int, [_vp, _vp]),
+    "sss_nbody_create": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+    "sss_nbody_destroy": (None, [_vp]),
+    "sss_nbody_load": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    "sss_nbody_step_batch": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, _vp]),
+    "sss_nbody_hits": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int64]),
+    "sss_nbody_sub": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int64]),
+    "sss_nbody_export_f64": (ctypes.c_int, [_vp, _vp]),
+    "sss_nbody_scatter": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]),
+    "sss_nbody_set_radius": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double]),
+    "sss_nbody_deactivate": (ctypes.c_int, [_vp, ctypes.c_int64]),
 }
 
 _lib = None
