@@ -55,9 +55,14 @@ __global__ void __launch_bounds__(BP_NT) k_alive_count(const unsigned char* __re
                                                        const unsigned char* __restrict__ vis,
                                                        const float* __restrict__ x, long long n,
                                                        const BpParams* __restrict__ P,
-                                                       long long* __restrict__ counts) {
+                                                       long long* __restrict__ counts,
+                                                       unsigned long long* __restrict__ kmin) {
     const float lo = P->lo, hi_halo = P->hi_halo;
     const long long base = (long long)blockIdx.x * sss_dev::SCAN_TILE;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {                   // the alive scatter narrows them
+        kmin[0] = ~0ull;
+        kmin[1] = 0ull;
+    }
     long long c = 0;
     for (int k = 0; k < sss_dev::SCAN_ITEMS; ++k) {
         const long long i = base + (long long)threadIdx.x * sss_dev::SCAN_ITEMS + k;
@@ -77,7 +82,8 @@ __global__ void __launch_bounds__(BP_NT) k_alive_scatter(const unsigned char* __
                                                          unsigned* __restrict__ ai, long long* __restrict__ cx,
                                                          long long* __restrict__ cy,
                                                          unsigned long long* __restrict__ skey,
-                                                         unsigned* __restrict__ sval) {
+                                                         unsigned* __restrict__ sval,
+                                                         unsigned long long* __restrict__ kmin) {   // [min, max]
     const float lo = P->lo, hi_halo = P->hi_halo;
     const double h = P->h;
     const long long base = (long long)blockIdx.x * sss_dev::SCAN_TILE;
@@ -90,6 +96,7 @@ __global__ void __launch_bounds__(BP_NT) k_alive_scatter(const unsigned char* __
     }
     long long tot;
     long long r = sss_dev::block_exclusive_scan(c, &tot) + offs[blockIdx.x];
+    unsigned long long kl = ~0ull, kh = 0ull;                       // this thread's smallest and largest key
     for (int k = 0; k < sss_dev::SCAN_ITEMS; ++k) {
         if (!f[k]) continue;
         const long long i = base + (long long)threadIdx.x * sss_dev::SCAN_ITEMS + k;
@@ -99,9 +106,22 @@ __global__ void __launch_bounds__(BP_NT) k_alive_scatter(const unsigned char* __
         cx[r] = ix;
         cy[r] = iy;
         // signed int64 order as unsigned: flip the sign bit
-        skey[r] = (unsigned long long)cell_key(ix, iy) ^ 0x8000000000000000ull;
+        const unsigned long long kk = (unsigned long long)cell_key(ix, iy) ^ 0x8000000000000000ull;
+        skey[r] = kk;
         sval[r] = (unsigned)r;
+        kl = kk < kl ? kk : kl;
+        kh = kk > kh ? kk : kh;
         ++r;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, kl, o);
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, kh, o);
+        kl = v < kl ? v : kl;
+        kh = w > kh ? w : kh;
+    }
+    if ((threadIdx.x & 31) == 0 && kl <= kh) {
+        atomicMin(&kmin[0], kl);
+        atomicMax(&kmin[1], kh);
     }
 }
 
@@ -240,10 +260,17 @@ __global__ void k_sub_keys(const float* __restrict__ x, const float* __restrict_
     sv[r] = (unsigned)r;
 }
 
+// Cell keys in sub-cell order, as offsets from the smallest alive key
+// (kmin = [smallest, largest]): the same order and the same equal groups,
+// and the high digits of a compact key range are zero, so the radix sort
+// copies those passes instead of ranking them. Padding rows take the largest
+// offset: they come after every alive row in this order, so the stable sort
+// keeps them last.
 __global__ void k_gather_keys(const unsigned long long* __restrict__ rowkey, const unsigned* __restrict__ order,
-                              const long long* __restrict__ d_na, long long n, unsigned long long* __restrict__ keys) {
+                              const long long* __restrict__ d_na, long long n,
+                              const unsigned long long* __restrict__ kmin, unsigned long long* __restrict__ keys) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < n) keys[p] = p < *d_na ? rowkey[order[p]] : ~0ull;   // padding sorts after every row (stable)
+    if (p < n) keys[p] = (p < *d_na ? rowkey[order[p]] : kmin[1]) - kmin[0];
 }
 
 // Bounding box of every aligned chunk of 32 sorted records: x, y, vx, vy
@@ -331,6 +358,7 @@ constexpr int TILE_B = 992;       // partners per tile (at most 32 aligned chunk
 __global__ void __launch_bounds__(256) k_items(const long long* __restrict__ cx, const long long* __restrict__ cy,
                                                const unsigned* __restrict__ order,
                                                const unsigned long long* __restrict__ ks,
+                                               const unsigned long long* __restrict__ kmin,
                                                const long long* __restrict__ d_na,
                                                const long long* __restrict__ run_start,
                                                const long long* __restrict__ d_nrun, long long max_items,
@@ -346,8 +374,9 @@ __global__ void __launch_bounds__(256) k_items(const long long* __restrict__ cx,
         const long long q = t - (long long)o * n_run;
         const long long p0 = run_start[q], p1 = q + 1 < n_run ? run_start[q + 1] : na;
         const unsigned r = order[p0];
+        // (a key below the smallest wraps to a value no alive key has)
         const unsigned long long k2 =
-            (unsigned long long)cell_key(cx[r] + c_off[o][0], cy[r] + c_off[o][1]) ^ 0x8000000000000000ull;
+            ((unsigned long long)cell_key(cx[r] + c_off[o][0], cy[r] + c_off[o][1]) ^ 0x8000000000000000ull) - kmin[0];
         const long long lo = lower_bound(ks, na, k2);
         const long long nb = upper_bound(ks, na, k2) - lo;
         item_b0[t] = lo;
@@ -700,7 +729,7 @@ struct BpBufs {
     uint2* rec2;
     unsigned long long* rowkey;
     ChunkBox* boxes;
-    unsigned long long* d_nh;   // hits, candidates
+    unsigned long long* d_nh;   // hits, candidates, smallest and largest alive cell key
     Hit* hits;
 };
 
@@ -710,11 +739,11 @@ struct BpBufs {
 int enqueue_pipeline(sss_ctx* ctx, const BpBufs& B, long long nn, long long capacity, cudaStream_t s) {
     const long long tiles = (nn + sss_dev::SCAN_TILE - 1) / sss_dev::SCAN_TILE;
     // 1) alive compaction (ascending body order) + cells + keys
-    k_alive_count<<<(unsigned)tiles, BP_NT, 0, s>>>(B.is_ast, B.vis, B.x, nn, B.P, B.counts);
+    k_alive_count<<<(unsigned)tiles, BP_NT, 0, s>>>(B.is_ast, B.vis, B.x, nn, B.P, B.counts, B.d_nh + 2);
     sss_dev::k_scan_sums<<<1, sss_dev::SCAN_NT, 0, s>>>(B.counts, tiles);
     const long long* d_na = B.counts + tiles;
     k_alive_scatter<<<(unsigned)tiles, BP_NT, 0, s>>>(B.is_ast, B.vis, B.x, B.y, nn, B.P, B.counts, B.ai, B.cx,
-                                                       B.cy, B.rowkey, B.v0);
+                                                       B.cy, B.rowkey, B.v0, B.d_nh + 2);
     SSS_LAUNCH_CHECK(ctx, "k_alive_scatter");
     // 2) sort by the position inside the cell, then stably by the cell key
     //    (ascending signed order): key, then sub-cell, then body order; the
@@ -723,7 +752,7 @@ int enqueue_pipeline(sss_ctx* ctx, const BpBufs& B, long long nn, long long capa
     k_sub_keys<<<nb_n, 256, 0, s>>>(B.x, B.y, B.ai, B.cx, B.cy, d_na, nn, B.P, B.k0, B.v0);
     SSS_LAUNCH_CHECK(ctx, "k_sub_keys");
     SSS_CUDA_TRY(ctx, sss_dev::radix_sort(B.k0, B.v0, B.k1, B.v1, nn, B.scan_tmp, s, ctx->d_status, 12));
-    k_gather_keys<<<nb_n, 256, 0, s>>>(B.rowkey, B.v0, d_na, nn, B.k0);
+    k_gather_keys<<<nb_n, 256, 0, s>>>(B.rowkey, B.v0, d_na, nn, B.d_nh + 2, B.k0);
     SSS_LAUNCH_CHECK(ctx, "k_gather_keys");
     SSS_CUDA_TRY(ctx, sss_dev::radix_sort(B.k0, B.v0, B.k1, B.v1, nn, B.scan_tmp, s, ctx->d_status));
     k_sorted_records<<<nb_n, 256, 0, s>>>(B.x, B.y, B.vx, B.vy, B.rr, B.ai, B.v0, d_na, B.rec, B.rec2);
@@ -744,7 +773,8 @@ int enqueue_pipeline(sss_ctx* ctx, const BpBufs& B, long long nn, long long capa
     SSS_CUDA_TRY(ctx, cudaMemsetAsync(B.d_nh, 0, 2 * sizeof(unsigned long long), s));
     // 4) (run, offset) items: partner ranges, tiles, candidates
     const long long max_items = 5 * nn;
-    k_items<<<(unsigned)((max_items + 255) / 256), 256, 0, s>>>(B.cx, B.cy, B.v0, B.k0, d_na, B.run_start, d_nrun,
+    k_items<<<(unsigned)((max_items + 255) / 256), 256, 0, s>>>(B.cx, B.cy, B.v0, B.k0, B.d_nh + 2, d_na,
+                                                                B.run_start, d_nrun,
                                                                 max_items, B.item_b0, B.item_nb, B.tile_st,
                                                                 B.d_nh + 1);
     SSS_LAUNCH_CHECK(ctx, "k_items");
@@ -815,7 +845,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_rec = take(2 * nn), o_rec2 = take(nn);      // float4 and uint2 per alive body
     const size_t o_rowkey = take(nn);                          // cell key per alive row
     const size_t o_box = take((nn + 31) / 32 * (sizeof(ChunkBox) / 8));
-    const size_t o_nh = take(2);
+    const size_t o_nh = take(4);                               // hits, candidates, smallest and largest cell key
     const size_t o_par = take(sizeof(BpParams) / 8 + 1);
     const size_t o_f5 = take((5 * nn + 1) / 2);                // staged x, y, vx, vy, rr (f32)
     const size_t o_u2 = take((2 * nn + 7) / 8);                // staged is_ast, vis (u8)
