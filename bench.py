@@ -786,11 +786,11 @@ def measure_collisions(dev, stream, samples=2_000, check_every=500, n_reserve=20
             pairs, run = cr.analyze_merge(g, dt_y)
             t2 = time.perf_counter()
             if pairs or run is not None:
-                sample = g.reshape(-1).cpu().numpy()
-                vis_before = cr.vis.copy()
-                cr.apply_merges(sim, st, sample, pairs, run, k_ev=done)
-                cr.refresh()
-                gone = np.flatnonzero((vis_before != 0) & (cr.vis == 0))
+                # the merges read the sample's columns of the bodies they name; the simulation's
+                # updates go in one batch, the device mirrors of the changed bodies after them
+                cr.apply_merges(sim, st, g, pairs, run, k_ev=done, batched=True)
+                cr.refresh(cr.changed)
+                gone = cr.changed[cr.vis[cr.changed] == 0]
                 if len(gone):
                     sf.kill(gone, float(done + 1))
             t3 = time.perf_counter()

@@ -55,14 +55,35 @@ class CollisionResponse:
         self.prev = None                # (px, py) device f32 of the previous analysed sample
         self.d_ast = torch.as_tensor(self.is_ast.astype(np.uint8)).to(self.dev)
         self.d_midx = torch.as_tensor(self.m_idx.astype(np.int64)).to(self.dev)
+        self.changed = np.zeros(0, np.int64)   # bodies whose host mirrors the last apply_merges changed
+        self._free = None                      # free asteroid slots, ascending (None: recompute)
         self.refresh()
 
-    def refresh(self) -> None:
-        """Copy the host mirrors (vis, radii, masses) to the device."""
-        self.d_vis = torch.as_tensor(self.vis).to(self.dev)
-        self.d_rr32 = torch.as_tensor(self.real_r.astype(np.float32)).to(self.dev)
-        self.d_rr = torch.as_tensor(self.real_r).to(self.dev)
-        self.d_mass = torch.as_tensor(self.mass).to(self.dev)
+    def refresh(self, idx=None) -> None:
+        """Copy the host mirrors (vis, radii, masses) to the device: all of
+        them (the reference's stammdaten_laden, film_producer.py:636-643), or
+        only the bodies idx (e.g. `self.changed` after apply_merges)."""
+        if idx is None:
+            self.d_vis = torch.as_tensor(self.vis).to(self.dev)
+            self.d_rr32 = torch.as_tensor(self.real_r.astype(np.float32)).to(self.dev)
+            self.d_rr = torch.as_tensor(self.real_r).to(self.dev)
+            self.d_mass = torch.as_tensor(self.mass).to(self.dev)
+            self._free = None
+            return
+        idx = np.asarray(idx, np.int64).ravel()
+        if len(idx) == 0:
+            return
+        i_t = torch.as_tensor(idx).to(self.dev)
+        self.d_vis[i_t] = torch.as_tensor(self.vis[idx]).to(self.dev)
+        self.d_rr32[i_t] = torch.as_tensor(self.real_r[idx].astype(np.float32)).to(self.dev)
+        self.d_rr[i_t] = torch.as_tensor(self.real_r[idx]).to(self.dev)
+        self.d_mass[i_t] = torch.as_tensor(self.mass[idx]).to(self.dev)
+
+    def _free_slots(self) -> np.ndarray:
+        """Hidden asteroid slots not yet taken by a fragment, ascending."""
+        if self._free is None:
+            self._free = np.flatnonzero((self.vis == 0) & self.is_ast & ~self.pending)
+        return self._free
 
     def _s(self):
         return ctypes.c_void_p(_lib.stream_handle(self.device))
@@ -119,19 +140,63 @@ class CollisionResponse:
         return pairs[:na.value, 0], pairs[:na.value, 1], touched[:nt.value], deltas[:nt.value]
 
     # ---------------------------------------------------------- application
-    def apply_merges(self, sim, st, sample: np.ndarray, pairs, runaways, k_ev: int = 0, contact: dict | None = None):
+    def apply_merges(self, sim, st, sample, pairs, runaways, k_ev: int = 0, contact: dict | None = None,
+                     batched: bool = False):
         """Apply merges and runaway removals in order (apply_merges,
         film_producer.py:781-861) to the simulation and the host mirrors.
         Returns (events, shatter): events (a, b, new_mass, kind, frac, x, y),
         kind 0 merge / 2 runaway; shatter (a, b, frac) when a body x body
         impact at >= 1.5 v_esc stopped the processing (the reference freezes
-        the film there and leaves the fragments to its client)."""
+        the film there and leaves the fragments to its client).
+
+        `sample` is the sample as host f32 (4n), or the device tensor (4, n):
+        then only the columns of the bodies named in `pairs` and `runaways`
+        come to the host. By default each merge and removal reaches the
+        simulation at once, through the reference's calls in the reference's
+        order (apply_body_state, deactivate_body, set_radius). With
+        batched=True (a simulation with apply_body_states, set_radii and
+        deactivate_bodies, as NBodyCuda) they are applied in one go after the
+        loop (each body's last state, then the removals); the loop reads host
+        data only, so the simulation ends in the same state. `self.changed`
+        lists the bodies whose host mirrors changed (for refresh(self.changed))."""
         n = self.n
-        sx, sy = sample[0:n], sample[n:2 * n]
-        svx, svy = sample[2 * n:3 * n], sample[3 * n:4 * n]
+        if isinstance(sample, torch.Tensor):
+            need = {int(a) for a, _, _ in pairs} | {int(b) for _, b, _ in pairs}
+            if runaways is not None:
+                need |= {int(j) for j in runaways}
+            sx, sy, svx, svy = (np.empty(n, np.float32) for _ in range(4))
+            if need:
+                ni = np.fromiter(sorted(need), np.int64, len(need))
+                cols = sample.reshape(4, n)[:, torch.as_tensor(ni).to(sample.device)].cpu().numpy()
+                sx[ni], sy[ni], svx[ni], svy[ni] = cols[0], cols[1], cols[2], cols[3]
+        else:
+            sx, sy = sample[0:n], sample[n:2 * n]
+            svx, svy = sample[2 * n:3 * n], sample[3 * n:4 * n]
         mass, vis, rr = self.mass, self.vis, self.real_r
         events = []
         contact = {} if contact is None else contact
+        states, radii, removed = {}, {}, []     # batched simulation updates, in the loop's order
+        changed = []
+
+        def flush():
+            if sim is None or not batched:
+                return
+            if states:
+                d = st["dim"]
+                rows = [[v[0], v[1], 0.0, v[2], v[3], 0.0, v[4]] if d == 3 else list(v) for v in states.values()]
+                sim.apply_body_states(st, list(states), rows)
+            if radii:
+                sim.set_radii(st, list(radii), list(radii.values()))
+            if removed:
+                sim.deactivate_bodies(st, removed)
+
+        def finish(shatter):
+            flush()
+            self.changed = np.unique(np.asarray(changed, np.int64))
+            if np.any(self.is_ast[self.changed] & (self.vis[self.changed] == 0)):
+                self._free = None          # hidden asteroids are free slots now
+            return events, shatter
+
         for mi, j, frac in pairs:
             tk = contact.pop(j, None)
             if tk is not None:
@@ -144,7 +209,7 @@ class CollisionResponse:
                 touch = max(1e-12, rr[mi] + rr[j])
                 v_esc = float(np.sqrt(2.0 * self.G * (mass[mi] + mass[j]) / touch))
                 if v_imp >= SHATTER_V_ESC * v_esc:
-                    return events, (int(mi), int(j), frac)
+                    return finish((int(mi), int(j), frac))
             if not vis[mi] or not vis[j] or mass[mi] <= 0:
                 continue
             a, b = (mi, j) if mass[mi] >= mass[j] else (j, mi)
@@ -157,14 +222,22 @@ class CollisionResponse:
             nvx = (svx[a] * m_a + svx[b] * m_b) / m_ges
             nvy = (svy[a] * m_a + svy[b] * m_b) / m_ges
             if sim is not None:
-                sim.apply_body_state(st, a, nx, ny, nvx, nvy, m_ges)
-                sim.deactivate_body(st, b)
+                if batched:
+                    states[int(a)] = (float(nx), float(ny), float(nvx), float(nvy), float(m_ges))
+                    removed.append(int(b))
+                else:
+                    sim.apply_body_state(st, a, nx, ny, nvx, nvy, m_ges)
+                    sim.deactivate_body(st, b)
             mass[a] = m_ges
             mass[b] = 0.0
             vis[b] = 0
             rr[a] = (rr[a] ** 3 + rr[b] ** 3) ** (1.0 / 3.0)
+            changed += [int(a), int(b)]
             if sim is not None:
-                sim.set_radius(st, a, float(rr[a]))
+                if batched:
+                    radii[int(a)] = float(rr[a])
+                else:
+                    sim.set_radius(st, a, float(rr[a]))
             events.append((int(a), int(b), float(m_ges), 0, float(frac), float(nx), float(ny)))
         if runaways is not None:
             for j in runaways:
@@ -172,11 +245,15 @@ class CollisionResponse:
                 if not vis[j]:
                     continue
                 if sim is not None:
-                    sim.deactivate_body(st, j)
+                    if batched:
+                        removed.append(j)
+                    else:
+                        sim.deactivate_body(st, j)
                 mass[j] = 0.0
                 vis[j] = 0
+                changed.append(j)
                 events.append((0xFFFFFFFF, j, 0.0, 2, 0.0, float(sx[j]), float(sy[j])))
-        return events, None
+        return finish(None)
 
     def fragment(self, g: torch.Tensor, res, factor: float, seed: int, n_frag: int = N_FRAG):
         """Fragmenting impacts among the active bounce pairs `res` (the
@@ -225,16 +302,22 @@ class CollisionResponse:
         if len(parents) == 0:
             return [], [], 0
         n_events = len(parents)
-        used, keep = set(), []
-        for q, (a, b) in enumerate(parents):
-            # a parent hidden since the broadphase ran (absorbed by a merge of
-            # the same sample) does not fragment; neither does a body twice
-            if self.vis[a] and self.vis[b] and int(a) not in used and int(b) not in used:
-                keep.append(q)
-                used.update((int(a), int(b)))
+        # a parent hidden since the broadphase ran (absorbed by a merge of the
+        # same sample) does not fragment; neither does a body twice
+        flat = parents.reshape(-1)
+        if len(np.unique(flat)) == len(flat):      # disjoint (the one-hit-per-body bounce pairs)
+            keep = np.flatnonzero((self.vis[parents[:, 0]] != 0) & (self.vis[parents[:, 1]] != 0))
+        else:
+            used, keep = set(), []
+            for q, (a, b) in enumerate(parents):
+                if self.vis[a] and self.vis[b] and int(a) not in used and int(b) not in used:
+                    keep.append(q)
+                    used.update((int(a), int(b)))
         parents, frags = parents[keep], frags[keep]
         n_frag = frags.shape[1]
-        free = np.flatnonzero((self.vis == 0) & self.is_ast & ~self.pending)  # ascending
+        if len(parents) == 0:
+            return [], [], n_events
+        free = self._free_slots()                                             # ascending
         e = min(len(parents), len(free) // (n_frag - 2))                      # events with room, in order
         skipped = n_events - e
         if e == 0:
@@ -251,12 +334,13 @@ class CollisionResponse:
         self.mass[idx] = f[:, 4]
         self.real_r[idx] = f[:, 5]
         self.pending[slots[:, 2:].reshape(-1)] = True
+        self._free = free[e * (n_frag - 2):]
         if self.prev is not None:          # fragments 0 and 1: their sweep segments start where they are placed
             p_idx = torch.as_tensor(slots[:, :2].reshape(-1)).to(self.dev)
             f01 = frags[:e, :2].reshape(2 * e, 6)
             self.prev[0][p_idx] = torch.as_tensor(f01[:, 0].astype(np.float32)).to(self.dev)
             self.prev[1][p_idx] = torch.as_tensor(f01[:, 1].astype(np.float32)).to(self.dev)
-        self.refresh()
+        self.refresh(idx)
         fr = frags[:e]
         events = [(int(a), int(b), float(q[0, 4]), 3, 0.0, float(q[:, 0].mean()), float(q[:, 1].mean()))
                   for (a, b), q in zip(parents[:e], fr)]
@@ -276,7 +360,7 @@ class CollisionResponse:
                 p_idx = torch.as_tensor(idx).to(self.dev)
                 self.prev[0][p_idx] = g0[0][p_idx]
                 self.prev[1][p_idx] = g0[1][p_idx]
-            self.refresh()
+            self.refresh(idx)
         return idx
 
     def apply_bounce(self, sim, st, res) -> int:

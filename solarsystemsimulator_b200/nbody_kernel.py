@@ -334,6 +334,53 @@ class NBodyCuda:
         if st["inv_kind"][idx] > 0:
             st["am_h"][st["inv_pos"][idx]] = mass
 
+    def apply_body_states(self, st: dict, idx, vals) -> None:
+        """apply_body_state for several bodies in one scatter: vals [m][2*dim+1]
+        (x, y, (z), vx, vy, (vz), mass) at unique original indices idx (the
+        batched form of nbody_kernel.py:990-1010; additive API)."""
+        idx = np.asarray(idx, np.int64).ravel()
+        if len(idx) == 0:
+            return
+        if len(np.unique(idx)) != len(idx):
+            raise ValueError("apply_body_states: idx must be unique")
+        vals = np.asarray(vals, np.float64).reshape(len(idx), -1)
+        self._scatter(st, idx, vals, 2)
+        ast = st["inv_kind"][idx] > 0
+        st["am_h"][st["inv_pos"][idx[ast]]] = vals[ast, -1]
+
+    def set_radii(self, st: dict, idx, radii) -> None:
+        """set_radius for several bodies at once (additive API)."""
+        idx = np.asarray(idx, np.int64).ravel()
+        if len(idx) == 0:
+            return
+        r = np.asarray(radii, np.float64).ravel()
+        dev = torch.device("cuda", self.device)
+        ast = st["inv_kind"][idx] > 0
+        for sel, key in ((ast, "ar"), (~ast, "mr")):
+            if sel.any():
+                p_t = torch.as_tensor(st["inv_pos"][idx[sel]]).to(dev)
+                st[key][p_t] = torch.as_tensor(r[sel]).to(dev)
+
+    def deactivate_bodies(self, st: dict, idx) -> None:
+        """deactivate_body for several bodies at once: mass 0, not visible
+        (additive API)."""
+        idx = np.asarray(idx, np.int64).ravel()
+        if len(idx) == 0:
+            return
+        dev = torch.device("cuda", self.device)
+        ast = st["inv_kind"][idx] > 0
+        if ast.any():
+            pos = st["inv_pos"][idx[ast]]
+            p_t = torch.as_tensor(pos).to(dev)
+            st["am"][p_t] = 0.0
+            st["avis"][p_t] = 0
+            st["am_h"][pos] = 0.0
+            st["avis_h"][pos] = 0
+        if (~ast).any():
+            p_t = torch.as_tensor(st["inv_pos"][idx[~ast]]).to(dev)
+            st["mm"][p_t] = 0.0
+            st["mvis"][p_t] = 0
+
     def set_asteroids(self, st: dict, idx, vals, radii) -> None:
         """Set asteroids completely and make them visible: vals [m][2*dim+1]
         (x, y, (z), vx, vy, (vz), mass) and contact radii [m] at original

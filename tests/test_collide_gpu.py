@@ -406,3 +406,43 @@ def test_fragment_events_sharing_a_body():
     out = sim.export_f64(st)
     assert np.array_equal(out[slots[1]], frags[2, :, 0])
     assert FRAG_V_ESC > 0
+
+
+def test_batched_merges_equal_immediate_updates():
+    # apply_merges with the sample's columns gathered on the device, the
+    # simulation's updates in one batch and the changed mirrors refreshed
+    # alone leaves exactly the state of the reference's immediate updates
+    # with the whole sample on the host and a full refresh
+    from solarsystemsimulator_b200.nbody_kernel import NBodyCuda
+    f = _film(31, n_per=2000, clouds=2, crossers=30, runaways=8)
+    g = f["g"]
+    x, y, vx, vy = (g[i].astype(np.float64) for i in range(4))
+    runs = {}
+    for batched in (False, True):
+        cr = _cr(f)
+        sim = NBodyCuda([0])
+        st = sim.load_state(x, y, vx, vy, f["mass"], f["vis"], f["is_ast"], f["rr"])
+        gd = torch.as_tensor(g).cuda()
+        cr.prev = (torch.as_tensor(f["prev"][0]).cuda(), torch.as_tensor(f["prev"][1]).cuda())
+        pairs, run = cr.analyze_merge(gd, f["dt_y"])
+        assert len(pairs) > 0 and run is not None and len(run) > 0
+        if batched:
+            events, shatter = cr.apply_merges(sim, st, gd, pairs, run, batched=True)
+            cr.refresh(cr.changed)
+            fresh = np.flatnonzero((cr.vis == 0) & cr.is_ast & ~cr.pending)
+            assert np.array_equal(cr._free_slots(), fresh)
+        else:
+            events, shatter = cr.apply_merges(sim, st, g.reshape(-1), pairs, run, batched=False)
+            cr.refresh()
+        snap = sim.step_batch(st, f["dt_y"], 2)
+        runs[batched] = dict(
+            events=events, shatter=shatter, f64=sim.export_f64(st), snap=snap,
+            mirrors=[cr.mass.copy(), cr.vis.copy(), cr.real_r.copy(), st["am_h"].copy(), st["avis_h"].copy()],
+            device=[t.cpu().numpy() for t in (cr.d_vis, cr.d_rr32, cr.d_rr, cr.d_mass)] +
+                   [st[k].cpu().numpy() for k in ("am", "avis", "ar", "mm", "mvis", "mr")])
+    a, b = runs[False], runs[True]
+    assert a["events"] == b["events"] and a["shatter"] == b["shatter"]
+    assert any(e[3] == 0 for e in a["events"]) and any(e[3] == 2 for e in a["events"])
+    assert np.array_equal(a["f64"], b["f64"]) and np.array_equal(a["snap"], b["snap"])
+    for u, v in zip(a["mirrors"] + a["device"], b["mirrors"] + b["device"]):
+        assert np.array_equal(u, v)
