@@ -407,8 +407,11 @@ struct TileArgs {
     const long long* n_run;
     const long long* n_tiles;
     const BpParams* P;           // dtf, dt, hi of tp come from here
+    unsigned long long* tile_ctr; // the next tile to hand out (zero before the launch)
     TestParams tp;
 };
+
+constexpr int TILE_GRAB = 4;      // tiles a warp takes from the counter at a time
 
 __device__ __forceinline__ float warp_max(float v) {
     for (int d = 16; d; d >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d));
@@ -568,91 +571,96 @@ __global__ void __launch_bounds__(BP_NT, 3) k_tiles(const TileArgs a_in) {
     __shared__ unsigned char q_l[BP_NT / 32][QCAP];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     PairQueue q{q_j[wib], q_l[wib], 0};
-    const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
     const long long na = *a.na, n_run = *a.n_run, n_tiles = *a.n_tiles;
-    const long long per = (n_tiles + warps - 1) / warps;
-    const long long tb = warp0 * per, te = min(tb + per, n_tiles);
-    if (tb >= te) return;
     const long long n_items = 5 * n_run;
-    long long t0 = 0;
-    if (lane == 0) t0 = find_segment(a.tile_start, n_items, tb);
-    long long t = __shfl_sync(0xffffffffu, t0, 0);
-    long long t_start = a.tile_start[t], t_end = a.tile_start[t + 1];
     const float dtf = a.tp.dtf;
-    for (long long tid = tb; tid < te; ++tid) {
-        while (t_end <= tid) {
-            ++t;
-            t_start = t_end;
-            t_end = a.tile_start[t + 1];
-        }
-        const int o = (int)(t / n_run);
-        const long long qr = t - (long long)o * n_run;
-        const long long p0 = a.run_start[qr], p1 = qr + 1 < n_run ? a.run_start[qr + 1] : na;
-        const long long b0 = a.item_b0[t], nb = a.item_nb[t];
-        const long long n_bt = (nb + TILE_B - 1) / TILE_B;
-        const long long local = tid - t_start;
-        const long long ai = local / n_bt, bi = local - ai * n_bt;
-        const long long pa = p0 + ai * 32 + lane;
-        const bool valid = pa < p1;
-        Body A{0.f, 0.f, 0.f, 0.f, 0.f};
-        unsigned ab = 0;
-        if (valid) {
-            const float4 v = a.rec[pa];
-            const uint2 w = a.rec2[pa];
-            A = Body{v.x, v.y, v.z, v.w, __uint_as_float(w.x)};
-            ab = w.y;
-        }
-        const float ax0 = warp_min(valid ? A.x : INFINITY), ax1 = warp_max(valid ? A.x : -INFINITY);
-        const float ay0 = warp_min(valid ? A.y : INFINITY), ay1 = warp_max(valid ? A.y : -INFINITY);
-        const float au0 = warp_min(valid ? A.vx : INFINITY), au1 = warp_max(valid ? A.vx : -INFINITY);
-        const float aw0 = warp_min(valid ? A.vy : INFINITY), aw1 = warp_max(valid ? A.vy : -INFINITY);
-        float arr = valid ? A.rr : 0.0f;
-        for (int d = 16; d; d >>= 1) arr = nan_max(arr, __shfl_xor_sync(0xffffffffu, arr, d));
-        const long long jb = b0 + bi * TILE_B;
-        const long long je = min(jb + TILE_B, b0 + nb);
-        const long long c0 = jb >> 5;
-        const int nch = (int)(((je - 1) >> 5) - c0 + 1);
-        // lane c: chunk c0 + c
-        bool near = false;
-        float Pc = 0.0f, Vc = 0.0f, brr = 0.0f;
-        if (lane < nch) {
-            const ChunkBox bx = a.boxes[c0 + lane];
-            const float dxb = fmaxf(0.0f, fmaxf(bx.pos.x - ax1, ax0 - bx.pos.y));
-            const float dyb = fmaxf(0.0f, fmaxf(bx.pos.z - ay1, ay0 - bx.pos.w));
-            const float Vx = fmaxf(bx.vel.y - au0, au1 - bx.vel.x), Vy = fmaxf(bx.vel.w - aw0, aw1 - bx.vel.z);
-            Pc = fmaxf(fmaxf(bx.pos.y - ax0, ax1 - bx.pos.x), fmaxf(bx.pos.w - ay0, ay1 - bx.pos.z)) * 1.0001f;
-            Vc = fmaxf(Vx, Vy) * 1.0001f;
-            brr = bx.rad.x;
-            const float reach = (Vx + Vy) * 1.0001f * dtf + ((arr + 1e-6f) + brr);
-            const float d2 = dxb * dxb + dyb * dyb;
-            const bool far = Pc < 0.5f && Vc * dtf < 0.5f && reach < 1.0f && d2 > 4.01f * reach * reach;
-            near = !far;
-        }
-        unsigned nm = __ballot_sync(0xffffffffu, near);
-        const int mode = o == 0 ? 0 : (a.ks[b0] != a.ks[p0] ? 1 : 2);
-        const float rsa = A.rr + 1e-6f;
-        while (nm) {
-            const int c = __ffs(nm) - 1;
-            nm &= nm - 1;
-            const float P = __shfl_sync(0xffffffffu, Pc, c), V = __shfl_sync(0xffffffffu, Vc, c);
-            const float br = __shfl_sync(0xffffffffu, brr, c);
-            // a NaN radius or an unbounded box: no line-test skips in the chunk (warp-uniform;
-            // NaN coordinates need nothing here, as their line test never skips)
-            const bool skip_ok =
-                __all_sync(0xffffffffu, P < 0.5f && V * dtf < 0.5f && br == br && (!valid || A.rr == A.rr));
-            const float E = 2.0f * EPS_CROSS * P * V;
-            const float rs = rsa + br;
-            const float kl = 4.01f * rs * rs;
-            const long long cs = (c0 + c) << 5;
-            const long long js = max(cs, jb), jn = min(cs + 32, je);
-            if (mode == 0) span_walk<0>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
-            else if (mode == 1) span_walk<1>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
-            else span_walk<2>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
-        }
-        if (q.cnt > 0) {                               // the rest of the tile's queue
-            queue_flush(q, q.cnt, a, o, A, ab, lane);
-            q.cnt = 0;
+    // the tiles' costs differ by orders of magnitude (culled chunks against
+    // dense ones), so the warps take them in small grabs from a counter
+    // instead of fixed shares
+    for (;;) {
+        long long g0 = 0;
+        if (lane == 0) g0 = (long long)atomicAdd(a.tile_ctr, (unsigned long long)TILE_GRAB);
+        const long long tb = __shfl_sync(0xffffffffu, g0, 0);
+        if (tb >= n_tiles) break;
+        const long long te = min(tb + (long long)TILE_GRAB, n_tiles);
+        long long t0 = 0;
+        if (lane == 0) t0 = find_segment(a.tile_start, n_items, tb);
+        long long t = __shfl_sync(0xffffffffu, t0, 0);
+        long long t_start = a.tile_start[t], t_end = a.tile_start[t + 1];
+        for (long long tid = tb; tid < te; ++tid) {
+            while (t_end <= tid) {
+                ++t;
+                t_start = t_end;
+                t_end = a.tile_start[t + 1];
+            }
+            const int o = (int)(t / n_run);
+            const long long qr = t - (long long)o * n_run;
+            const long long p0 = a.run_start[qr], p1 = qr + 1 < n_run ? a.run_start[qr + 1] : na;
+            const long long b0 = a.item_b0[t], nb = a.item_nb[t];
+            const long long n_bt = (nb + TILE_B - 1) / TILE_B;
+            const long long local = tid - t_start;
+            const long long ai = local / n_bt, bi = local - ai * n_bt;
+            const long long pa = p0 + ai * 32 + lane;
+            const bool valid = pa < p1;
+            Body A{0.f, 0.f, 0.f, 0.f, 0.f};
+            unsigned ab = 0;
+            if (valid) {
+                const float4 v = a.rec[pa];
+                const uint2 w = a.rec2[pa];
+                A = Body{v.x, v.y, v.z, v.w, __uint_as_float(w.x)};
+                ab = w.y;
+            }
+            const float ax0 = warp_min(valid ? A.x : INFINITY), ax1 = warp_max(valid ? A.x : -INFINITY);
+            const float ay0 = warp_min(valid ? A.y : INFINITY), ay1 = warp_max(valid ? A.y : -INFINITY);
+            const float au0 = warp_min(valid ? A.vx : INFINITY), au1 = warp_max(valid ? A.vx : -INFINITY);
+            const float aw0 = warp_min(valid ? A.vy : INFINITY), aw1 = warp_max(valid ? A.vy : -INFINITY);
+            float arr = valid ? A.rr : 0.0f;
+            for (int d = 16; d; d >>= 1) arr = nan_max(arr, __shfl_xor_sync(0xffffffffu, arr, d));
+            const long long jb = b0 + bi * TILE_B;
+            const long long je = min(jb + TILE_B, b0 + nb);
+            const long long c0 = jb >> 5;
+            const int nch = (int)(((je - 1) >> 5) - c0 + 1);
+            // lane c: chunk c0 + c
+            bool near = false;
+            float Pc = 0.0f, Vc = 0.0f, brr = 0.0f;
+            if (lane < nch) {
+                const ChunkBox bx = a.boxes[c0 + lane];
+                const float dxb = fmaxf(0.0f, fmaxf(bx.pos.x - ax1, ax0 - bx.pos.y));
+                const float dyb = fmaxf(0.0f, fmaxf(bx.pos.z - ay1, ay0 - bx.pos.w));
+                const float Vx = fmaxf(bx.vel.y - au0, au1 - bx.vel.x), Vy = fmaxf(bx.vel.w - aw0, aw1 - bx.vel.z);
+                Pc = fmaxf(fmaxf(bx.pos.y - ax0, ax1 - bx.pos.x), fmaxf(bx.pos.w - ay0, ay1 - bx.pos.z)) * 1.0001f;
+                Vc = fmaxf(Vx, Vy) * 1.0001f;
+                brr = bx.rad.x;
+                const float reach = (Vx + Vy) * 1.0001f * dtf + ((arr + 1e-6f) + brr);
+                const float d2 = dxb * dxb + dyb * dyb;
+                const bool far = Pc < 0.5f && Vc * dtf < 0.5f && reach < 1.0f && d2 > 4.01f * reach * reach;
+                near = !far;
+            }
+            unsigned nm = __ballot_sync(0xffffffffu, near);
+            const int mode = o == 0 ? 0 : (a.ks[b0] != a.ks[p0] ? 1 : 2);
+            const float rsa = A.rr + 1e-6f;
+            while (nm) {
+                const int c = __ffs(nm) - 1;
+                nm &= nm - 1;
+                const float P = __shfl_sync(0xffffffffu, Pc, c), V = __shfl_sync(0xffffffffu, Vc, c);
+                const float br = __shfl_sync(0xffffffffu, brr, c);
+                // a NaN radius or an unbounded box: no line-test skips in the chunk (warp-uniform;
+                // NaN coordinates need nothing here, as their line test never skips)
+                const bool skip_ok =
+                    __all_sync(0xffffffffu, P < 0.5f && V * dtf < 0.5f && br == br && (!valid || A.rr == A.rr));
+                const float E = 2.0f * EPS_CROSS * P * V;
+                const float rs = rsa + br;
+                const float kl = 4.01f * rs * rs;
+                const long long cs = (c0 + c) << 5;
+                const long long js = max(cs, jb), jn = min(cs + 32, je);
+                if (mode == 0) span_walk<0>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
+                else if (mode == 1) span_walk<1>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
+                else span_walk<2>(a, o, A, ab, valid, js, (int)(jn - js), E, kl, skip_ok, q, lane);
+            }
+            if (q.cnt > 0) {                               // the rest of the tile's queue
+                queue_flush(q, q.cnt, a, o, A, ab, lane);
+                q.cnt = 0;
+            }
         }
     }
 }
@@ -729,7 +737,7 @@ struct BpBufs {
     uint2* rec2;
     unsigned long long* rowkey;
     ChunkBox* boxes;
-    unsigned long long* d_nh;   // hits, candidates, smallest and largest alive cell key
+    unsigned long long* d_nh;   // hits, candidates, smallest and largest alive cell key, tile counter
     Hit* hits;
 };
 
@@ -804,6 +812,8 @@ int enqueue_pipeline(sss_ctx* ctx, const BpBufs& B, long long nn, long long capa
     ta.tp.hits = B.hits;
     ta.tp.cap = capacity;
     ta.tp.n_hits = B.d_nh;
+    ta.tile_ctr = B.d_nh + 4;
+    SSS_CUDA_TRY(ctx, cudaMemsetAsync(ta.tile_ctr, 0, sizeof(unsigned long long), s));
     k_tiles<<<(unsigned)(ctx->num_sms * 32), BP_NT, 0, s>>>(ta);
     SSS_LAUNCH_CHECK(ctx, "k_tiles");
     return SSS_OK;
@@ -845,7 +855,7 @@ extern "C" int sss_broadphase(sss_ctx* ctx, const float* x, const float* y, cons
     const size_t o_rec = take(2 * nn), o_rec2 = take(nn);      // float4 and uint2 per alive body
     const size_t o_rowkey = take(nn);                          // cell key per alive row
     const size_t o_box = take((nn + 31) / 32 * (sizeof(ChunkBox) / 8));
-    const size_t o_nh = take(4);                               // hits, candidates, smallest and largest cell key
+    const size_t o_nh = take(5);                               // hits, candidates, smallest and largest cell key, tile counter
     const size_t o_par = take(sizeof(BpParams) / 8 + 1);
     const size_t o_f5 = take((5 * nn + 1) / 2);                // staged x, y, vx, vy, rr (f32)
     const size_t o_u2 = take((2 * nn + 7) / 8);                // staged is_ast, vis (u8)
