@@ -41,8 +41,8 @@ FLOP_PER_PAIR = 20          # the reference's own convention (TODO.md:73-74)
 # nominal SIMT peaks of a B200 at 1965 MHz: 148 SMs x 64 DFMA / 128 FFMA lanes x 2 flops
 NOMINAL_FP64 = 148 * 64 * 2 * 1.965e9 / 1e12
 NOMINAL_FP32 = 148 * 128 * 2 * 1.965e9 / 1e12
-# DRAM bytes (read + write) of one k_force_mixed launch on this workload, from an
-# ncu capture of the full-size launch (profiles/k_force_mixed_dram_traffic_262k.md)
+# DRAM bytes (read + write) of one k_force_mixed launch on this workload, measured
+# by an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the full-size launch
 MIXED_DRAM_BYTES_PER_LAUNCH = 270_845_568
 METRIC = "G interactions/s (all-pairs self-gravity, mixed FP32-pair/FP64-accumulate, Yoshida-4)"
 UNIT = "G interactions/s"
