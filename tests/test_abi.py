@@ -42,3 +42,32 @@ def test_abi_version():
 def test_library_built_for_sm100a():
     # the build flags pin the architecture; nvcc refuses an unknown arch
     assert "arch=compute_100a,code=sm_100a" in " ".join(sss_build.ARCH_FLAGS)
+
+
+def test_c_host_compiles_links_and_calls_without_gpu(tmp_path):
+    """A plain C99 host (what a cgo or JNI binding compiles against) includes
+    include/sss.h, links libsss.so and calls entry points that need no GPU;
+    sss_create fails cleanly when no device is visible."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    sss_build.build()
+    src = tmp_path / "host.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "sss.h"\n'
+        "int main(void) {\n"
+        "    sss_ctx* ctx = 0;\n"
+        "    int rc = sss_create(0, &ctx);\n"
+        "    if (rc == SSS_OK) sss_destroy(ctx);\n"
+        '    printf("%d %d %s\\n", sss_abi_version(), rc == SSS_OK || rc == SSS_ERR_CUDA || rc == SSS_ERR_ARG,\n'
+        "           sss_last_error(0));\n"
+        "    return 0;\n}\n")
+    exe = tmp_path / "host"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-pedantic", f"-I{os.path.join(ROOT, 'include')}",
+                    str(src), f"-L{libdir}", "-lsss", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True, timeout=120).stdout.split()
+    assert out[0] == "1" and out[1] == "1" and " ".join(out[2:]) == "NULL context"
