@@ -373,7 +373,10 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": r / 1e9, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
 
     rows = None
-    if rank == 0 and not args.no_rows:
+    # the per-row measurements are single-GPU figures of the other paths; a
+    # multi-GPU run reports the headline alone (its other ranks would wait at
+    # the closing barrier while rank 0 measures them)
+    if rank == 0 and world == 1 and not args.no_rows:
         rows = {}
         for name, fn in (("frame_solar_system_belt", measure_frame), ("broadphase_asteroid_clouds",
                                                                        measure_broadphase),
