@@ -213,3 +213,29 @@ def test_deposit_in_a_plane_is_the_reference_2d_deposit(load_golden):
     plane = rho3[:, :, 0] * h ** 3
     assert np.abs(rho3[:, :, 1:]).max() == 0.0
     assert np.abs(plane - g["rho"]).max() <= 1e-12 * np.abs(g["rho"]).max()
+
+
+def test_gather_of_a_z_constant_field_is_the_reference_2d_gather(load_golden):
+    """A mesh whose planes are all equal reduces the 3-D trilinear stencil to
+    the 2-D bilinear one: the oracle's 3-D gather of the reference's 2-D force
+    field (pm_force_field of the reference's case, fixture pm2d_n2000_g128.npz,
+    which the 2-D oracle reproduces bit for bit) stacked along z, at the
+    bodies' positions in the same cells, is the reference's own gathered
+    acceleration (pm_kernel._cic_gather, pm_kernel.py:93-107), up to the order
+    of the eight weighted terms. The bodies sit inside the grid's margin, so
+    neither the 2-D clipping nor the periodic wrap acts."""
+    from oracle import pm as opm2
+    g = load_golden("pm2d_n2000_g128.npz")
+    n, h = int(g["grid_n"]), float(g["h"])
+    x0, y0 = float(g["x0"]), float(g["y0"])
+    fx, fy = opm2.pm_force_field(g["x"], g["y"], g["m"], n, x0, y0, h, float(g["eps2"]))
+    meshes = np.zeros((3, n, n, n))
+    meshes[0] = fx[:, :, None]
+    meshes[1] = fy[:, :, None]
+    for z in (0.0, 0.37 * h, 0.999 * h):            # on a plane and between two equal planes
+        pos = np.stack([g["x"] - x0, g["y"] - y0, np.full(len(g["x"]), 17 * h + z)], 1)
+        a = o.cic_gather(meshes, pos, L=n * h)
+        scale = max(np.abs(g["ax"]).max(), np.abs(g["ay"]).max())
+        assert np.abs(a[:, 0] - g["ax"]).max() <= 1e-12 * scale
+        assert np.abs(a[:, 1] - g["ay"]).max() <= 1e-12 * scale
+        assert np.abs(a[:, 2]).max() == 0.0
