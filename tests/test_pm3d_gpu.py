@@ -64,6 +64,34 @@ def test_deposit_in_a_plane_is_the_reference_2d_deposit(mods, load_golden):
     assert np.abs(rho[:, :, 0] * h ** 3 - g["rho"]).max() <= 2e-6 * np.abs(g["rho"]).max()
 
 
+def test_gather_of_a_z_constant_field_is_the_reference_2d_gather(mods, load_golden):
+    """k_gather3 on acceleration meshes whose planes all hold the reference's
+    2-D force field (pm_force_field of the reference's case, fixture
+    pm2d_n2000_g128.npz, reproduced bit for bit by the 2-D oracle) gives the
+    reference's own gathered accelerations (pm_kernel._cic_gather,
+    pm_kernel.py:93-107) to the f32 rounding of the mesh values; the z
+    component stays zero."""
+    _lib, pm3d, _, _ = mods
+    from oracle import pm as opm2
+    g = load_golden("pm2d_n2000_g128.npz")
+    n, h = int(g["grid_n"]), float(g["h"])
+    x0, y0 = float(g["x0"]), float(g["y0"])
+    fx, fy = opm2.pm_force_field(g["x"], g["y"], g["m"], n, x0, y0, h, float(g["eps2"]))
+    pm = pm3d.PMPeriodic3D(n, n * h, 1.0)
+    pos = np.stack([g["x"] - x0, g["y"] - y0, np.full(len(g["x"]), 17.37 * h)], 1)
+    st = pm.load_state(pos, np.zeros_like(pos), g["m"])
+    mesh = torch.zeros((3, n, n, n), dtype=torch.float32)
+    mesh[0] = torch.from_numpy(fx.astype(np.float32))[:, :, None]
+    mesh[1] = torch.from_numpy(fy.astype(np.float32))[:, :, None]
+    pm.acc_mesh.copy_(mesh.to(pm.acc_mesh.device))
+    pm.gather(st)
+    a = st["buf"][6:9].cpu().numpy().T
+    scale = max(np.abs(g["ax"]).max(), np.abs(g["ay"]).max())
+    assert np.abs(a[:, 0] - g["ax"]).max() <= 1e-6 * scale
+    assert np.abs(a[:, 1] - g["ay"]).max() <= 1e-6 * scale
+    assert np.abs(a[:, 2]).max() == 0.0
+
+
 @pytest.mark.parametrize("mesh,deconv,rs", [(32, 2, 0.6), (64, 2, 0.6), (32, 0, 0.0), (48, 1, 1.0)])
 def test_forces_match_oracle(mods, mesh, deconv, rs):
     _lib, pm3d, _, _ = mods
