@@ -42,9 +42,9 @@
 // issues the MMAs and commits them to mbarriers; every wait is bounded
 // (SSS_ERR_TIMEOUT).
 //
-// Measured on the 262,144-source benchmark state: 79.6 ms per force
-// evaluation (the SIMT mixed kernel: 75.8 ms), median relative force error
-// 1.4e-7 against f64.
+// Measured on the 262,144-source benchmark state: 79.0 ms per force
+// evaluation with the sorts and the tile prep (the SIMT mixed kernel:
+// 75.8 ms), median relative force error 1.4e-7 against f64.
 
 #include "allpairs.cuh"
 #include "devscan.cuh"
