@@ -32,6 +32,11 @@ namespace {
 constexpr int FR_NT = 256;
 constexpr int FR_WARPS = FR_NT / 32;
 constexpr int M_MAX = SSS_M_MAX;
+// A hot asteroid's fine loop runs on FG lanes, lane l taking the massive
+// bodies k = l, l + FG, ...; the CTA's hot asteroids are listed HOT_SPAN
+// asteroids at a time and handed to its FR_NT / FG lane groups on demand.
+constexpr int FG = 8;
+constexpr int HOT_SPAN = 2048;
 
 struct FrameArgs {
     double* ax[3];            // asteroid positions [n_ast] per dimension
@@ -73,6 +78,8 @@ struct FrameShared {
     double red[FR_WARPS];
     double dtH, rem;
     int done, guard, abort_;
+    int hl[HOT_SPAN];         // hot asteroids of the current span
+    int hn, hgrab;            // their count, the next one to hand out
     unsigned char mvis[M_MAX];
 };
 
@@ -150,22 +157,37 @@ __device__ __forceinline__ void massive_field_f32(const FrameShared& s, const do
     }
 }
 
-// Same, massive positions interpolated between mx0 and mx at fraction al.
-template <int D>
-__device__ __forceinline__ void interp_field(const FrameShared& s, int M, double G, double soft, double al,
-                                             const double* p, double* acc) {
+// massive_field on the FG lanes of a group (mask gmask, this lane gl): lane
+// gl forms the pair factor f m and the offset of bodies k = k0 + gl, then
+// every lane adds the terms in ascending k, so each lane holds the sum in the
+// serial order of massive_field. INTERP: the massive positions interpolated
+// between mx0 and mx at fraction al.
+template <int D, bool INTERP>
+__device__ __forceinline__ void field_grp(const FrameShared& s, int M, double G, double soft, double al,
+                                          const double* p, double* acc, int gl, unsigned gmask) {
     for (int c = 0; c < D; ++c) acc[c] = 0.0;
-    for (int k = 0; k < M; ++k) {
-        if (!s.mvis[k]) continue;
-        double dx[3], r2 = 0.0;
-        for (int c = 0; c < D; ++c) {
-            const double mi = s.mx0[c][k] + (s.mx[c][k] - s.mx0[c][k]) * al;
-            dx[c] = mi - p[c];
-            r2 += dx[c] * dx[c];
+    for (int k0 = 0; k0 < M; k0 += FG) {
+        const int k = k0 + gl;
+        double fm = 0.0, dx[3] = {0.0, 0.0, 0.0};
+        if (k < M && s.mvis[k]) {
+            double r2 = 0.0;
+            for (int c = 0; c < D; ++c) {
+                double mi;
+                if constexpr (INTERP) mi = s.mx0[c][k] + (s.mx[c][k] - s.mx0[c][k]) * al;
+                else mi = s.mx[c][k];
+                dx[c] = mi - p[c];
+                r2 += dx[c] * dx[c];
+            }
+            r2 += soft;
+            const double f = G / (r2 * sqrt(r2));
+            fm = f * s.mm[k];
         }
-        r2 += soft;
-        const double f = G / (r2 * sqrt(r2));
-        for (int c = 0; c < D; ++c) acc[c] += f * s.mm[k] * dx[c];
+        const int kn = min(FG, M - k0);
+        for (int j = 0; j < kn; ++j) {
+            if (!s.mvis[k0 + j]) continue;
+            const double fj = __shfl_sync(gmask, fm, j, FG);
+            for (int c = 0; c < D; ++c) acc[c] += fj * __shfl_sync(gmask, dx[c], j, FG);
+        }
     }
 }
 
@@ -274,41 +296,66 @@ __device__ double pair_dt(const FrameArgs& a, FrameShared& s) {
     return r;
 }
 
-// Hot asteroid: private adaptive Yoshida over [0, dtH] (nbody_kernel.py:416-535).
+// Hot asteroid i: private adaptive Yoshida over [0, dtH] (nbody_kernel.py:416-535)
+// on the FG lanes of a group. The massive bodies are spread over the lanes
+// (field_grp); the step size is the group minimum of the encounter times, a
+// contact the first body in k order (the ballot's lowest bit). Every lane
+// carries the same position, velocity and step, formed in the same order as
+// the serial loop; lane 0 writes.
 template <int D>
-__device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int ks, double dtH, double tSeg0) {
+__device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int ks, double dtH, double tSeg0,
+                          int gl, unsigned gmask) {
     const double wd[3] = {a.w1, a.w0, a.w1};
+    const int gbase = (threadIdx.x & 31) & ~(FG - 1);
     double p[3], v[3];
     for (int c = 0; c < D; ++c) { p[c] = a.ax[c][i]; v[c] = a.av[c][i]; }
     const double sgn = dtH >= 0.0 ? 1.0 : -1.0;
     const double span = fabs(dtH);
     const double subDt = a.m_sub > 0 ? a.dt_raster / a.m_sub : 0.0;
     const double rad = a.arad[i];
+    bool open = a.hit_t[i] < 0.0f;      // no contact time recorded yet
     double tau = 0.0;
     int guardF = 0;
     while (tau < span - 1e-15 && guardF++ < a.fine_guard) {
         const double al = tau / span;
         double dtF = a.max_sub_dt;
-        for (int k = 0; k < a.M; ++k) {
-            if (!s.mvis[k]) continue;
-            double d2 = 0.0, v2 = 0.0;
-            for (int c = 0; c < D; ++c) {
-                const double mi = s.mx0[c][k] + (s.mx[c][k] - s.mx0[c][k]) * al;
-                const double dx = mi - p[c], dv = s.mv[c][k] - v[c];
-                d2 += dx * dx;
-                v2 += dv * dv;
+        int first = -1, last = -1;      // bodies in contact, lowest and highest k
+        for (int k0 = 0; k0 < a.M; k0 += FG) {
+            const int k = k0 + gl;
+            bool touch = false;
+            if (k < a.M && s.mvis[k]) {
+                double d2 = 0.0, v2 = 0.0;
+                for (int c = 0; c < D; ++c) {
+                    const double mi = s.mx0[c][k] + (s.mx[c][k] - s.mx0[c][k]) * al;
+                    const double dx = mi - p[c], dv = s.mv[c][k] - v[c];
+                    d2 += dx * dx;
+                    v2 += dv * dv;
+                }
+                double dist = sqrt(d2);
+                if (dist < 1e-12) dist = 1e-12;
+                touch = dist <= s.mrad[k] + rad;
+                const double vrel = sqrt(v2);
+                if (vrel > 1e-9) {
+                    const double te = dist / vrel / 20.0;
+                    if (te < dtF) dtF = te;
+                }
             }
-            double dist = sqrt(d2);
-            if (dist < 1e-12) dist = 1e-12;
-            if (a.hit_t[i] < 0.0f && dist <= s.mrad[k] + rad) {
-                a.hit_t[i] = (float)(ks * a.dt_raster + tSeg0 + tau);
-                a.hit_m[i] = k;
+            const unsigned b = (__ballot_sync(gmask, touch) >> gbase) & ((1u << FG) - 1u);
+            if (b) {
+                if (first < 0) first = k0 + __ffs(b) - 1;
+                last = k0 + 31 - __clz(b);
             }
-            const double vrel = sqrt(v2);
-            if (vrel > 1e-9) {
-                const double te = dist / vrel / 20.0;
-                if (te < dtF) dtF = te;
+        }
+        for (int o = FG / 2; o > 0; o >>= 1) dtF = fmin(dtF, __shfl_xor_sync(gmask, dtF, o, FG));
+        if (open && first >= 0) {
+            // the serial test `hit_t < 0` per body: the first body in contact closes it,
+            // unless the recorded time is itself negative (then every later body overwrites)
+            const float h = (float)(ks * a.dt_raster + tSeg0 + tau);
+            if (gl == 0) {
+                a.hit_t[i] = h;
+                a.hit_m[i] = h < 0.0f ? last : first;
             }
+            open = h < 0.0f;
         }
         if (dtF < a.max_sub_dt / 1000.0) dtF = a.max_sub_dt / 1000.0;
         if (dtF > span - tau) dtF = span - tau;
@@ -324,14 +371,14 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
         for (int wf = 0; wf < 3; ++wf) {
             const double df = wd[wf] * dtF * sgn;
             double acc[3], ncc[3];
-            interp_field<D>(s, a.M, a.G, a.soft, tSub / span, p, acc);
+            field_grp<D, true>(s, a.M, a.G, a.soft, tSub / span, p, acc, gl, gmask);
             for (int c = 0; c < D; ++c) p[c] += v[c] * df + 0.5 * acc[c] * df * df;
             tSub += wd[wf] * dtF;
-            interp_field<D>(s, a.M, a.G, a.soft, tSub / span, p, ncc);
+            field_grp<D, true>(s, a.M, a.G, a.soft, tSub / span, p, ncc, gl, gmask);
             for (int c = 0; c < D; ++c) v[c] += 0.5 * (acc[c] + ncc[c]) * df;
         }
         tau += dtF;
-        if (a.m_sub > 0) {
+        if (a.m_sub > 0 && gl == 0) {
             const double q = (tSeg0 + tau) / subDt;
             const int j = (int)floor(q + 0.5);
             if (j >= 1 && j <= a.m_sub && fabs(q - j) < 1e-6) {
@@ -341,13 +388,40 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
             }
         }
     }
-    // the guard ran out before the interval was covered: the reference stops there silently
-    // (nbody_kernel.py:424); the state keeps it, the status word records it
-    if (tau < span - 1e-15) atomicCAS(a.status, SSS_OK, SSS_ERR_GUARD);
-    for (int c = 0; c < D; ++c) { a.ax[c][i] = p[c]; a.av[c][i] = v[c]; }
     double acc[3];
-    massive_field<D>(s, s.mx, a.M, a.G, a.soft, p, acc);
-    for (int c = 0; c < D; ++c) a.aacc[c][i] = acc[c];
+    field_grp<D, false>(s, a.M, a.G, a.soft, 0.0, p, acc, gl, gmask);
+    if (gl == 0) {
+        // the guard ran out before the interval was covered: the reference stops there silently
+        // (nbody_kernel.py:424); the state keeps it, the status word records it
+        if (tau < span - 1e-15) atomicCAS(a.status, SSS_OK, SSS_ERR_GUARD);
+        for (int c = 0; c < D; ++c) { a.ax[c][i] = p[c]; a.av[c][i] = v[c]; a.aacc[c][i] = acc[c]; }
+    }
+}
+
+// The fine loops of this CTA's hot visible asteroids in [lo, hi): listed
+// HOT_SPAN asteroids at a time, each taken by the next free lane group.
+template <int D>
+__device__ void hot_pass(const FrameArgs& a, FrameShared& s, int lo, int hi, int ks, double dtH, double tSeg0) {
+    const int gl = threadIdx.x & (FG - 1);
+    const unsigned gmask = ((1u << FG) - 1u) << ((threadIdx.x & 31) & ~(FG - 1));
+    for (int base = lo; base < hi; base += HOT_SPAN) {
+        const int end = min(hi, base + HOT_SPAN);
+        if (threadIdx.x == 0) { s.hn = 0; s.hgrab = 0; }
+        __syncthreads();
+        for (int i = base + (int)threadIdx.x; i < end; i += blockDim.x)
+            if (a.avis[i] && a.hot[i]) s.hl[atomicAdd(&s.hn, 1)] = i;
+        __syncthreads();
+        const int hn = s.hn;
+        for (;;) {
+            int j = 0;
+            if (gl == 0) j = atomicAdd(&s.hgrab, 1);
+            j = __shfl_sync(gmask, j, 0, FG);
+            if (j >= hn) break;
+            fine_loop<D>(a, s, s.hl[j], ks, dtH, tSeg0, gl, gmask);
+        }
+        __syncthreads();
+    }
+    __syncthreads();
 }
 
 // Back-reaction sums for the current asteroid positions into s.bk (all
@@ -489,10 +563,7 @@ __global__ void __launch_bounds__(FR_NT) k_frame(const FrameArgs a) {
                 __syncthreads();
             }
             // private fine loop of the hot asteroids (:416-535)
-            const double tSeg0 = a.dt_raster - s.rem - dtH;
-            for (int i = lo + tid; i < hi; i += blockDim.x)
-                if (a.avis[i] && a.hot[i]) fine_loop<D>(a, s, i, ks, dtH, tSeg0);
-            __syncthreads();
+            hot_pass<D>(a, s, lo, hi, ks, dtH, a.dt_raster - s.rem - dtH);
         }
         // snapshot of this raster sample, original body order (:540-557)
         float* row = a.snap + (int64_t)ks * 2 * D * a.n_total;
