@@ -132,23 +132,24 @@ def percentile_linear(sorted_vals, q: float) -> float:
     result NaN), with NumPy 2's arithmetic for f32 input, all of it in f32:
     q / 100, the virtual index (n - 1) * q, its fractional part t, and the
     interpolation a + (b - a) t, or b - (b - a)(1 - t) for t >= 1/2. Only the
-    two neighbours and the last value are read."""
+    two neighbours and the last value are read (one readback from a device
+    tensor)."""
     f32 = np.float32
     n = int(sorted_vals.shape[0])
     if n == 0:
         raise ValueError("percentile of an empty sample")
-
-    def at(i):
-        v = sorted_vals[i]
-        return f32(v.item() if isinstance(v, torch.Tensor) else v)
-
-    if np.isnan(at(n - 1)):
-        return float("nan")
     vi = f32(n - 1) * (f32(q) / f32(100))
-    if vi >= n - 1:
-        return float(at(n - 1))
     lo = np.floor(vi)
-    a, b = at(int(lo)), at(int(lo) + 1)
+    need = [n - 1] if vi >= n - 1 else [n - 1, int(lo), int(lo) + 1]
+    if isinstance(sorted_vals, torch.Tensor):
+        got = torch.stack([sorted_vals[i] for i in need]).cpu().numpy().astype(f32)
+    else:
+        got = np.asarray(sorted_vals)[need].astype(f32)
+    if np.isnan(got[0]):
+        return float("nan")
+    if vi >= n - 1:
+        return float(got[0])
+    a, b = got[1], got[2]
     t = vi - lo
     d = b - a
     if t >= 0.5:
@@ -163,9 +164,9 @@ def search_cell(gvx, gvy, alive, dt_y: float) -> float:
     rounded as the C library's hypotf rounds them (exact squares in f64, one
     square root), sorted on the device."""
     dev = alive.device
-    vx = _dev_f32(gvx, dev)[alive].double()
-    vy = _dev_f32(gvy, dev)[alive].double()
-    speed = torch.sqrt(vx * vx + vy * vy).float()
+    vx = _dev_f32(gvx, dev).double()
+    vy = _dev_f32(gvy, dev).double()
+    speed = torch.sqrt(vx * vx + vy * vy).float()[alive]
     v95 = percentile_linear(torch.sort(speed).values, 95)
     return max(1e-4, 2.0 * v95 * dt_y)
 

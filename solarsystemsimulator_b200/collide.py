@@ -193,8 +193,14 @@ class CollisionResponse:
         def finish(shatter):
             flush()
             self.changed = np.unique(np.asarray(changed, np.int64))
-            if np.any(self.is_ast[self.changed] & (self.vis[self.changed] == 0)):
-                self._free = None          # hidden asteroids are free slots now
+            c = self.changed
+            hid = c[self.is_ast[c] & (self.vis[c] == 0) & ~self.pending[c]]
+            if len(hid) and self._free is not None:
+                # hidden asteroids are free slots now: insert them into the ascending list
+                free = self._free
+                pos = np.searchsorted(free, hid)
+                there = free[np.minimum(pos, len(free) - 1)] == hid if len(free) else np.zeros(len(hid), bool)
+                self._free = np.insert(free, pos[~there], hid[~there])
             return events, shatter
 
         for mi, j, frac in pairs:
@@ -239,7 +245,23 @@ class CollisionResponse:
                 else:
                     sim.set_radius(st, a, float(rr[a]))
             events.append((int(a), int(b), float(m_ges), 0, float(frac), float(nx), float(ny)))
-        if runaways is not None:
+        if runaways is not None and (sim is None or batched):
+            # the loop below without its per-body simulation calls: the visible runaways in order
+            # (a repeated index acts once)
+            run = np.asarray(runaways, np.int64).ravel()
+            run = run[vis[run] != 0]
+            if len(run):
+                first = np.unique(run, return_index=True)[1]
+                if len(first) < len(run):
+                    run = run[np.sort(first)]
+                if sim is not None:
+                    removed.extend(run.tolist())
+                mass[run] = 0.0
+                vis[run] = 0
+                changed += run.tolist()
+                events += [(0xFFFFFFFF, j, 0.0, 2, 0.0, x, y)
+                           for j, x, y in zip(run.tolist(), sx[run].tolist(), sy[run].tolist())]
+        elif runaways is not None:
             for j in runaways:
                 j = int(j)
                 if not vis[j]:
@@ -342,8 +364,10 @@ class CollisionResponse:
             self.prev[1][p_idx] = torch.as_tensor(f01[:, 1].astype(np.float32)).to(self.dev)
         self.refresh(idx)
         fr = frags[:e]
-        events = [(int(a), int(b), float(q[0, 4]), 3, 0.0, float(q[:, 0].mean()), float(q[:, 1].mean()))
-                  for (a, b), q in zip(parents[:e], fr)]
+        # the event's place: the mean of its fragments' positions (summed in fragment order)
+        events = [(a, b, m, 3, 0.0, x, y) for (a, b), m, x, y in
+                  zip(parents[:e].tolist(), fr[:, 0, 4].tolist(), fr[:, :, 0].mean(axis=1).tolist(),
+                      fr[:, :, 1].mean(axis=1).tolist())]
         return events, slots.tolist(), skipped
 
     def activate_fragments(self, g0: torch.Tensor | None = None) -> np.ndarray:
