@@ -320,15 +320,21 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
         const double al = tau / span;
         double dtF = a.max_sub_dt;
         int first = -1, last = -1;      // bodies in contact, lowest and highest k
+        // one pass over the bodies at fraction al: the encounter times, the contacts and the
+        // first stage's acceleration (field_grp at tau, from the same offsets)
+        double acc[3];
+        for (int c = 0; c < D; ++c) acc[c] = 0.0;
         for (int k0 = 0; k0 < a.M; k0 += FG) {
             const int k = k0 + gl;
             bool touch = false;
+            double fm = 0.0, dx[3] = {0.0, 0.0, 0.0};
             if (k < a.M && s.mvis[k]) {
                 double d2 = 0.0, v2 = 0.0;
                 for (int c = 0; c < D; ++c) {
                     const double mi = s.mx0[c][k] + (s.mx[c][k] - s.mx0[c][k]) * al;
-                    const double dx = mi - p[c], dv = s.mv[c][k] - v[c];
-                    d2 += dx * dx;
+                    dx[c] = mi - p[c];
+                    const double dv = s.mv[c][k] - v[c];
+                    d2 += dx[c] * dx[c];
                     v2 += dv * dv;
                 }
                 double dist = sqrt(d2);
@@ -339,11 +345,20 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
                     const double te = dist / vrel / 20.0;
                     if (te < dtF) dtF = te;
                 }
+                const double r2 = d2 + a.soft;
+                const double f = a.G / (r2 * sqrt(r2));
+                fm = f * s.mm[k];
             }
             const unsigned b = (__ballot_sync(gmask, touch) >> gbase) & ((1u << FG) - 1u);
             if (b) {
                 if (first < 0) first = k0 + __ffs(b) - 1;
                 last = k0 + 31 - __clz(b);
+            }
+            const int kn = min(FG, a.M - k0);
+            for (int j = 0; j < kn; ++j) {
+                if (!s.mvis[k0 + j]) continue;
+                const double fj = __shfl_sync(gmask, fm, j, FG);
+                for (int c = 0; c < D; ++c) acc[c] += fj * __shfl_sync(gmask, dx[c], j, FG);
             }
         }
         for (int o = FG / 2; o > 0; o >>= 1) dtF = fmin(dtF, __shfl_xor_sync(gmask, dtF, o, FG));
@@ -367,15 +382,19 @@ __device__ void fine_loop(const FrameArgs& a, const FrameShared& s, int i, int k
                 if (rest > 0.0 && dtF > rest) dtF = rest;
             }
         }
+        // the three velocity-Verlet stages; a stage's closing acceleration (same time, same
+        // position) is the next stage's opening one
         double tSub = tau;
         for (int wf = 0; wf < 3; ++wf) {
             const double df = wd[wf] * dtF * sgn;
-            double acc[3], ncc[3];
-            field_grp<D, true>(s, a.M, a.G, a.soft, tSub / span, p, acc, gl, gmask);
+            double ncc[3];
             for (int c = 0; c < D; ++c) p[c] += v[c] * df + 0.5 * acc[c] * df * df;
             tSub += wd[wf] * dtF;
             field_grp<D, true>(s, a.M, a.G, a.soft, tSub / span, p, ncc, gl, gmask);
-            for (int c = 0; c < D; ++c) v[c] += 0.5 * (acc[c] + ncc[c]) * df;
+            for (int c = 0; c < D; ++c) {
+                v[c] += 0.5 * (acc[c] + ncc[c]) * df;
+                acc[c] = ncc[c];
+            }
         }
         tau += dtF;
         if (a.m_sub > 0 && gl == 0) {
