@@ -2,6 +2,7 @@
 percentile arithmetic of the search cell, against NumPy and the reference."""
 import numpy as np
 import pytest
+import torch
 
 from solarsystemsimulator_b200 import broadphase as bp
 
@@ -33,3 +34,6 @@ def test_percentile_matches_numpy_on_f32(seed):
             want = np.percentile(v, q)
             got = bp.percentile_linear(np.sort(v), q)
             assert (np.isnan(want) and np.isnan(got)) or got == float(want), (n, q, got, want)
+            # a tensor takes the one-readback path
+            got_t = bp.percentile_linear(torch.from_numpy(np.sort(v)), q)
+            assert (np.isnan(want) and np.isnan(got_t)) or got_t == float(want), (n, q, got_t, want)
