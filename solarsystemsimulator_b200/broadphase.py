@@ -37,6 +37,14 @@ def _dev_u8(a, device) -> torch.Tensor:
     return torch.as_tensor(np.ascontiguousarray(np.asarray(a) != 0, dtype=np.uint8)).to(device)
 
 
+def _dev_flags(a, device) -> torch.Tensor:
+    """Per-call flag bytes: a contiguous uint8 tensor on the device is passed
+    as it is (the kernels test a byte for nonzero), anything else as _dev_u8."""
+    if isinstance(a, torch.Tensor) and a.dtype == torch.uint8 and a.device == device and a.is_contiguous():
+        return a
+    return _dev_u8(a, device)
+
+
 def bounce_hits_device(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, rr, is_ast=None, vis=None,
                        lo: float = -np.inf, hi: float = np.inf, device: int = 0):
     """The hit list on the device, unsorted: (int32 (k, 3) tensor of
@@ -46,8 +54,8 @@ def bounce_hits_device(gx, gy, gvx, gvy, dt_y: float, h: float, halo: float, *, 
     x, y, vx, vy = (_dev_f32(a, dev) for a in (gx, gy, gvx, gvy))
     n = x.numel()
     r = _dev_f32(rr, dev)
-    ast = torch.ones(n, dtype=torch.uint8, device=dev) if is_ast is None else _dev_u8(is_ast, dev)
-    vv = torch.ones(n, dtype=torch.uint8, device=dev) if vis is None else _dev_u8(vis, dev)
+    ast = torch.ones(n, dtype=torch.uint8, device=dev) if is_ast is None else _dev_flags(is_ast, dev)
+    vv = torch.ones(n, dtype=torch.uint8, device=dev) if vis is None else _dev_flags(vis, dev)
     ctx = _lib.context(device)
     cap = max(4096, n)
     while True:

@@ -73,11 +73,16 @@ class CollisionResponse:
         idx = np.asarray(idx, np.int64).ravel()
         if len(idx) == 0:
             return
-        i_t = torch.as_tensor(idx).to(self.dev)
-        self.d_vis[i_t] = torch.as_tensor(self.vis[idx]).to(self.dev)
-        self.d_rr32[i_t] = torch.as_tensor(self.real_r[idx].astype(np.float32)).to(self.dev)
-        self.d_rr[i_t] = torch.as_tensor(self.real_r[idx]).to(self.dev)
-        self.d_mass[i_t] = torch.as_tensor(self.mass[idx]).to(self.dev)
+        # one transfer: index, vis, radius, mass as f64 rows (exact: indices < 2^53, vis 0/1);
+        # the f32 radius is the f64 one rounded to nearest on the device, as astype(float32)
+        pk = np.empty((4, len(idx)))
+        pk[0], pk[1], pk[2], pk[3] = idx, self.vis[idx], self.real_r[idx], self.mass[idx]
+        d = torch.as_tensor(pk).to(self.dev)
+        i_t = d[0].long()
+        self.d_vis[i_t] = d[1].to(torch.uint8)
+        self.d_rr32[i_t] = d[2].float()
+        self.d_rr[i_t] = d[2]
+        self.d_mass[i_t] = d[3]
 
     def _free_slots(self) -> np.ndarray:
         """Hidden asteroid slots not yet taken by a fragment, ascending."""
